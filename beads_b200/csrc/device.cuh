@@ -1,0 +1,189 @@
+// device.cuh -- data layout shared by the host engine and the kernels.
+//
+// Every per-particle array is indexed by SLOT.  Replicas are packed one after
+// another; replica r owns slots [atom_begin, atom_begin + n_pad), of which the
+// first n_atoms are real particles and the rest are inert padding that makes
+// every 128-thread block belong to exactly one replica.  Positions carry the
+// 0-based type in the .w lane (bit pattern of an int), velocities carry the
+// mass in .w, so one 16-byte load fetches what a pair or a kick needs.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bb {
+
+constexpr int kBlock = 128;          // threads per block of per-slot kernels
+constexpr int kGroup = 32;           // neighbour-list interleave width
+constexpr int kMaxTypes = 16;        // LJ type table held in shared memory
+constexpr double kFixScale = 268435456.0;  // 2^28: fixed-point totals
+constexpr double kFixLimit = 1.0e9;  // |per-slot value| above this -> status
+
+// status bits (ReplicaState::status)
+constexpr unsigned kStatusNeighborOverflow = 1u;
+constexpr unsigned kStatusNonFinite = 2u;
+constexpr unsigned kStatusFixedOverflow = 4u;
+constexpr unsigned kStatusCellClamp = 8u;
+
+// accumulator lanes (ReplicaState::acc)
+enum AccLane : int {
+  kAccPair = 0,
+  kAccBond = 1,
+  kAccAngle = 2,
+  kAccDihedral = 3,
+  kAccVirial = 4,
+  kAccKinetic = 5,
+  kAccLanes = 8
+};
+
+// Immutable per-replica parameters (uploaded once).
+struct ReplicaParams {
+  float lo[3];
+  float len[3];
+  float half[3];
+  float inv_len[3];
+  uint32_t atom_begin;       // first slot
+  uint32_t n_atoms;          // real particles
+  uint32_t n_pad;            // slots incl. padding (multiple of kBlock)
+  uint32_t block_begin;      // first block of this replica
+  uint32_t tag_base;         // global tag index of tag 1
+  uint32_t cell_begin;       // first cell (global cell numbering)
+  uint32_t start_base;       // first entry in cell_start (n_cells + 1 each)
+  uint32_t nc[3];            // cells per axis
+  uint32_t n_cells;
+  float inv_cell[3];
+  float search_cut_sq;       // (rc + skin)^2 in float, neighbour inclusion
+  float force_cut_sq;        // rc^2 in float, pair cutoff
+  float disp_thr_sq;         // (skin / 2)^2 in float
+  float skin;
+  uint32_t max_neighbors;    // overflow threshold of this replica
+  uint32_t check_every;
+  uint32_t sort_every;
+  uint32_t excl_degree;      // max exclusion partners (0 = none)
+  float dt;
+  int32_t thermostat;        // 0 none, 1 Berendsen
+  double kt_target;          // kB * T0
+  double tau;
+  double dof;                // 3N - 3 (>= 0)
+  double kb;
+  double press_scale;
+  double volume;
+  uint32_t lj_offset;        // first entry of this replica's LJ table
+  int32_t n_types;
+  uint32_t bond_type_base, angle_type_base, dihedral_type_base;
+};
+
+// Mutable per-replica device state.
+struct ReplicaState {
+  unsigned long long step;          // completed physical steps
+  unsigned long long builds;        // neighbour builds
+  unsigned long long dangerous;     // dangerous rebuilds
+  unsigned int need_rebuild;        // decision for the current step
+  unsigned int reorder_now;         // physical reorder during this rebuild
+  unsigned int exceeded;            // displacement flag (written by threads)
+  unsigned int checks_since_build;  // scheduled checks since the last build
+  unsigned int done_pre;            // last-block counters
+  unsigned int done_post;
+  unsigned int status;              // kStatus* bits
+  unsigned int pad0;
+  double lambda;                    // pending Berendsen velocity scale
+  long long acc[kAccLanes];         // fixed-point totals of the current eval
+};
+
+// Observables of the last evaluation of one replica (device copy).
+struct ReplicaObs {
+  unsigned long long step;
+  double pair_pe, bond_pe, angle_pe, dihedral_pe;
+  double virial;
+  double ke_pre;      // kinetic energy before the Berendsen scaling
+  double lambda;      // scale applied to that kinetic energy (KE = l^2 KE_pre)
+  unsigned long long builds, dangerous;
+  unsigned int status;
+  unsigned int pad;
+};
+
+// LJ coefficients of one type pair, packed as in the reference's
+// LjPairModel::DeviceCoeff (native/src/forcefield/pair/pair_lj.cu:171-192).
+struct LjCoeff {
+  float sigma2;
+  float eps4;
+  float eps24;
+  float shift;
+};
+
+// Harmonic term coefficients.
+struct BondCoeff { float k, r0; };
+struct AngleCoeff { float k, theta0; };
+struct DihedralCoeff { float k; int d; int n; int pad; };
+
+// Bonded-term membership of one particle: kind (2 bits), role (2 bits) and
+// term index (28 bits).  Stored per global tag.
+constexpr uint32_t kTermBond = 1u, kTermAngle = 2u, kTermDihedral = 3u;
+__host__ __device__ inline uint32_t term_pack(uint32_t kind, uint32_t role,
+                                              uint32_t index) {
+  return (kind << 30) | (role << 28) | index;
+}
+
+__host__ __device__ inline uint64_t nbr_index(uint32_t slot, uint32_t k,
+                                              uint32_t stride) {
+  return ((uint64_t)(slot >> 5) * stride + k) * kGroup + (slot & 31u);
+}
+
+struct DeviceView {
+  // particle arrays
+  float4* pos;
+  float4* vel;
+  float4* force;
+  int4* img;
+  uint32_t* tag;
+  uint32_t* mol;
+  float4* ref_pos;
+  int4* ref_img;
+  // reorder scratch
+  float4* pos2;
+  float4* vel2;
+  int4* img2;
+  uint32_t* tag2;
+  uint32_t* mol2;
+  uint32_t* cell2;
+  // cells
+  uint32_t* cell_of_slot;
+  uint32_t* cell_count;
+  uint32_t* cell_cursor;
+  uint32_t* cell_start;
+  uint32_t* cell_atoms;
+  // neighbour list
+  uint32_t* nbr_count;
+  uint32_t* nbr;
+  uint32_t nbr_stride;       // allocated capacity per slot
+  // identity
+  uint32_t* slot_of_tag;     // by global tag index
+  // exclusions
+  uint32_t* excl_slot;       // [slot * excl_cap + e]
+  uint32_t excl_cap;
+  const uint32_t* excl_off;  // by global tag index (+1)
+  const uint32_t* excl_tag;  // partner global tag indices
+  // bonded
+  const uint32_t* term_off;  // by global tag index (+1)
+  const uint32_t* term;      // packed memberships
+  const uint4* bonds;        // (tag_i, tag_j, type, 0) global tags, global type
+  const uint4* angles;       // (tag_i, tag_j, tag_k, type)
+  const uint4* dihedrals;    // (tag_i, tag_j, tag_k, tag_l)
+  const uint32_t* dihedral_type;
+  const BondCoeff* bond_coeff;
+  const AngleCoeff* angle_coeff;
+  const DihedralCoeff* dihedral_coeff;
+  // replicas
+  const ReplicaParams* rp;
+  ReplicaState* rs;
+  ReplicaObs* obs;
+  const uint32_t* block_replica;
+  const LjCoeff* lj;
+  uint32_t n_replicas;
+  uint32_t n_slots;
+  uint32_t n_blocks;
+  uint32_t total_cells;
+  int has_bonded;
+};
+
+}  // namespace bb

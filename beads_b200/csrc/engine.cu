@@ -1,0 +1,737 @@
+// engine.cu -- host side of the batched device engine: memory layout, static
+// tables, the captured step loop and host transfers.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+
+namespace bb {
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    throw CudaError(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+  }
+}
+
+namespace {
+
+constexpr uint32_t kChunkMax = 64;     // steps per captured graph
+constexpr double kKbNmKjMol = 0.00831446261815324;
+constexpr double kPressNmKjMol = 16.60539067;
+
+uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
+
+int exclusion_capacity(uint32_t degree) {
+  if (degree == 0) return 0;
+  for (int cap : {4, 8, 16, 32, 64}) {
+    if (degree <= static_cast<uint32_t>(cap)) return cap;
+  }
+  throw InvalidArgument(
+      "bonded exclusions with more than 64 partners per particle are not supported.");
+}
+
+}  // namespace
+
+template <typename T>
+T* Engine::dalloc(size_t count) {
+  void* p = nullptr;
+  const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  cuda_check(cudaMalloc(&p, bytes), "cudaMalloc");
+  allocations_.push_back(p);
+  cuda_check(cudaMemsetAsync(p, 0, bytes, stream_), "cudaMemset");
+  return static_cast<T*>(p);
+}
+
+Engine::Engine(uint32_t n, const beads_system_desc* systems,
+               const beads_forcefield_desc* ffs, const beads_neighbor_desc* nbrs,
+               const beads_dynamics_desc* dyns) {
+  if (n == 0) throw InvalidArgument("a batch needs at least one replica.");
+  for (uint32_t r = 0; r < n; ++r) validate_replica(systems[r], ffs[r], nbrs[r], dyns[r]);
+  cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream create");
+  try {
+    upload_static(n, systems, ffs, nbrs, dyns);
+  } catch (...) {
+    for (void* p : allocations_) cudaFree(p);
+    allocations_.clear();
+    if (h_obs_) cudaFreeHost(h_obs_);
+    if (h_state_) cudaFreeHost(h_state_);
+    cudaStreamDestroy(stream_);
+    throw;
+  }
+}
+
+Engine::~Engine() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto& kv : graphs_) {
+    cudaGraphExecDestroy(kv.second.second);
+    cudaGraphDestroy(kv.second.first);
+  }
+  for (void* p : allocations_) cudaFree(p);
+  if (h_obs_) cudaFreeHost(h_obs_);
+  if (h_state_) cudaFreeHost(h_state_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
+                           const beads_forcefield_desc* ffs,
+                           const beads_neighbor_desc* nbrs,
+                           const beads_dynamics_desc* dyns) {
+  rep_.resize(n);
+  uint64_t slots = 0, tags = 0, cells = 0, lj_entries = 0;
+  uint64_t bonds = 0, angles = 0, dihedrals = 0;
+  uint32_t bond_types = 0, angle_types = 0, dihedral_types = 0;
+  uint32_t stride = 0, max_cells = 0, max_atoms = 0, max_degree = 0;
+  bool any_bonded = false, any_thermostat = false;
+
+  // Exclusion partner lists per replica (global tag indices).
+  std::vector<std::vector<uint32_t>> excl_partners;  // by global tag
+  std::vector<ReplicaParams> rp(n);
+  for (uint32_t r = 0; r < n; ++r) {
+    const beads_system_desc& s = systems[r];
+    const beads_forcefield_desc& f = ffs[r];
+    ReplicaHost& h = rep_[r];
+    h.plan = make_plan(s.box_lo, s.box_hi, f.lj_cutoff, nbrs[r].cutoff_buffer);
+    h.n_atoms = s.n_particles;
+    h.atom_begin = static_cast<uint32_t>(slots);
+    h.n_pad = round_up(s.n_particles, kBlock);
+    h.tag_base = static_cast<uint32_t>(tags);
+    h.units = s.units;
+    std::memcpy(h.box_lo, s.box_lo, sizeof(h.box_lo));
+    std::memcpy(h.box_hi, s.box_hi, sizeof(h.box_hi));
+    h.max_neighbors = nbrs[r].max_neighbors;
+    h.n_bonds = s.n_bonds;
+    h.n_angles = s.n_angles;
+    h.n_dihedrals = s.n_dihedrals;
+    h.dt = dyns[r].dt;
+    h.thermostat = dyns[r].thermostat;
+    slots += h.n_pad;
+    tags += s.n_particles;
+    if (slots > 0xF0000000ull) throw OverflowError("total particle slots exceed index range.");
+    stride = std::max(stride, h.max_neighbors);
+    max_cells = std::max(max_cells, h.plan.n_cells);
+    max_atoms = std::max(max_atoms, h.n_atoms);
+    any_bonded |= (s.n_bonds + s.n_angles + s.n_dihedrals) > 0;
+    any_thermostat |= dyns[r].thermostat == 1;
+
+    ReplicaParams& p = rp[r];
+    std::memset(&p, 0, sizeof(p));
+    for (int a = 0; a < 3; ++a) {
+      p.lo[a] = s.box_lo[a];
+      p.len[a] = s.box_hi[a] - s.box_lo[a];
+      p.half[a] = 0.5f * p.len[a];
+      p.inv_len[a] = 1.0f / p.len[a];
+      p.nc[a] = h.plan.nc[a];
+      p.inv_cell[a] = h.plan.inv_cell[a];
+    }
+    p.atom_begin = h.atom_begin;
+    p.n_atoms = h.n_atoms;
+    p.n_pad = h.n_pad;
+    p.block_begin = h.atom_begin / kBlock;
+    p.tag_base = h.tag_base;
+    p.cell_begin = static_cast<uint32_t>(cells);
+    p.start_base = static_cast<uint32_t>(cells + r);
+    p.n_cells = h.plan.n_cells;
+    cells += h.plan.n_cells;
+    p.search_cut_sq = h.plan.search_cutoff_sq;
+    p.force_cut_sq = h.plan.force_cutoff_sq;
+    const float half_skin = 0.5f * h.plan.cutoff_buffer;
+    p.disp_thr_sq = half_skin * half_skin;
+    p.skin = h.plan.cutoff_buffer;
+    p.max_neighbors = h.max_neighbors;
+    p.check_every = static_cast<uint32_t>(std::min<uint64_t>(nbrs[r].rebuild_check_every, 0xFFFFFFFFull));
+    // The reference's direct path never reorders particles (neighbor_system.cpp:113-119).
+    p.sort_every = h.plan.path == kPathDirect
+                       ? 0u
+                       : static_cast<uint32_t>(std::min<uint64_t>(nbrs[r].sort_every_rebuild, 0xFFFFFFFFull));
+    p.dt = static_cast<float>(dyns[r].dt);
+    p.thermostat = dyns[r].thermostat;
+    p.kb = s.units == BEADS_UNITS_NM_KJMOL ? kKbNmKjMol : 1.0;
+    p.press_scale = s.units == BEADS_UNITS_NM_KJMOL ? kPressNmKjMol : 1.0;
+    p.kt_target = p.kb * static_cast<double>(static_cast<float>(dyns[r].temperature));
+    p.tau = static_cast<double>(static_cast<float>(dyns[r].tau));
+    const double dof = 3.0 * static_cast<double>(s.n_particles) - 3.0;
+    p.dof = dof > 0.0 ? dof : 0.0;
+    p.volume = static_cast<double>(p.len[0]) * p.len[1] * p.len[2];
+    p.lj_offset = static_cast<uint32_t>(lj_entries);
+    p.n_types = f.n_types;
+    lj_entries += static_cast<uint64_t>(f.n_types) * f.n_types;
+    p.bond_type_base = bond_types;
+    p.angle_type_base = angle_types;
+    p.dihedral_type_base = dihedral_types;
+    bond_types += f.n_bond_types;
+    angle_types += f.n_angle_types;
+    dihedral_types += f.n_dihedral_types;
+    bonds += s.n_bonds;
+    angles += s.n_angles;
+    dihedrals += s.n_dihedrals;
+  }
+  n_tags_ = tags;
+  const uint32_t S = static_cast<uint32_t>(slots);
+  const uint32_t T = static_cast<uint32_t>(tags);
+  const uint32_t C = static_cast<uint32_t>(cells);
+  const uint64_t list_entries = static_cast<uint64_t>(S) * stride;
+  if (list_entries > (1ull << 36)) throw OverflowError("NeighborList slot count overflows.");
+
+  // ---- exclusions (tag space) ----
+  std::vector<uint32_t> excl_off(T + 1, 0);
+  std::vector<uint32_t> excl_tag;
+  {
+    std::vector<std::vector<uint32_t>> partners(T);
+    for (uint32_t r = 0; r < n; ++r) {
+      const beads_system_desc& s = systems[r];
+      const int d = ffs[r].exclusion_distance;
+      if (d <= 0 || s.n_bonds == 0) continue;
+      const auto pairs = bond_graph_exclusions(s.n_particles, s.bonds, s.n_bonds, d);
+      rep_[r].excluded_pairs = pairs.size();
+      const uint32_t base = rep_[r].tag_base;
+      for (const auto& pr : pairs) {
+        partners[base + pr.first - 1].push_back(base + pr.second - 1);
+        partners[base + pr.second - 1].push_back(base + pr.first - 1);
+      }
+    }
+    for (uint32_t t = 0; t < T; ++t) {
+      std::sort(partners[t].begin(), partners[t].end());
+      max_degree = std::max<uint32_t>(max_degree, static_cast<uint32_t>(partners[t].size()));
+      excl_off[t + 1] = excl_off[t] + static_cast<uint32_t>(partners[t].size());
+    }
+    excl_tag.reserve(excl_off[T]);
+    for (uint32_t t = 0; t < T; ++t) {
+      excl_tag.insert(excl_tag.end(), partners[t].begin(), partners[t].end());
+    }
+  }
+  const int excl_cap = exclusion_capacity(max_degree);
+  for (uint32_t r = 0; r < n; ++r) rp[r].excl_degree = max_degree;
+
+  // ---- particles in input order ----
+  std::vector<float4> h_pos(S), h_vel(S);
+  std::vector<int4> h_img(S);
+  std::vector<uint32_t> h_tag(S, 0xffffffffu), h_mol(S, 0), slot_of_tag(T, 0);
+  std::vector<uint32_t> block_replica(S / kBlock);
+  for (uint32_t r = 0; r < n; ++r) {
+    const beads_system_desc& s = systems[r];
+    const ReplicaHost& h = rep_[r];
+    const std::vector<uint32_t> rt = row_tags(s);
+    for (uint32_t k = 0; k < h.n_pad; ++k) {
+      const uint32_t slot = h.atom_begin + k;
+      if (k < h.n_atoms) {
+        int ty = s.types[k] - 1;
+        float w;
+        std::memcpy(&w, &ty, sizeof(w));
+        h_pos[slot] = make_float4(s.positions[3 * k], s.positions[3 * k + 1],
+                                  s.positions[3 * k + 2], w);
+        const float m = s.masses ? s.masses[k] : 1.0f;
+        if (s.velocities) {
+          h_vel[slot] = make_float4(s.velocities[3 * k], s.velocities[3 * k + 1],
+                                    s.velocities[3 * k + 2], m);
+        } else {
+          h_vel[slot] = make_float4(0.f, 0.f, 0.f, m);
+        }
+        h_img[slot] = s.images ? make_int4(s.images[3 * k], s.images[3 * k + 1],
+                                           s.images[3 * k + 2], 0)
+                               : make_int4(0, 0, 0, 0);
+        const uint32_t gt = h.tag_base + rt[k] - 1;
+        h_tag[slot] = gt;
+        h_mol[slot] = s.molecule_ids ? s.molecule_ids[k] : 1u;
+        slot_of_tag[gt] = slot;
+      } else {
+        h_pos[slot] = make_float4(s.box_lo[0], s.box_lo[1], s.box_lo[2], 0.f);
+        h_vel[slot] = make_float4(0.f, 0.f, 0.f, 1.f);
+        h_img[slot] = make_int4(0, 0, 0, 0);
+      }
+    }
+    for (uint32_t b = 0; b < h.n_pad / kBlock; ++b) block_replica[h.atom_begin / kBlock + b] = r;
+  }
+
+  // ---- bonded tables (global tag indices, global type indices) ----
+  std::vector<uint4> h_bonds, h_angles, h_dihedrals;
+  std::vector<uint32_t> h_dih_type;
+  std::vector<BondCoeff> h_bc;
+  std::vector<AngleCoeff> h_ac;
+  std::vector<DihedralCoeff> h_dc;
+  std::vector<std::vector<uint32_t>> member(T);
+  for (uint32_t r = 0; r < n; ++r) {
+    const beads_system_desc& s = systems[r];
+    const beads_forcefield_desc& f = ffs[r];
+    const uint32_t base = rep_[r].tag_base;
+    for (int t = 0; t < f.n_bond_types; ++t) {
+      h_bc.push_back(BondCoeff{static_cast<float>(f.bond_k[t]), static_cast<float>(f.bond_r0[t])});
+    }
+    for (int t = 0; t < f.n_angle_types; ++t) {
+      const float theta0 = static_cast<float>(f.angle_theta0_deg[t]);
+      h_ac.push_back(AngleCoeff{static_cast<float>(f.angle_k[t]),
+                                theta0 * 3.14159265358979323846f / 180.0f});
+    }
+    for (int t = 0; t < f.n_dihedral_types; ++t) {
+      h_dc.push_back(DihedralCoeff{static_cast<float>(f.dihedral_k[t]), f.dihedral_d[t],
+                                   f.dihedral_n[t], 0});
+    }
+    for (uint32_t k = 0; k < s.n_bonds; ++k) {
+      const uint32_t* b = s.bonds + 3 * (size_t)k;
+      const uint32_t idx = static_cast<uint32_t>(h_bonds.size());
+      h_bonds.push_back(make_uint4(base + b[0] - 1, base + b[1] - 1,
+                                   rp[r].bond_type_base + b[2] - 1, 0));
+      member[base + b[0] - 1].push_back(term_pack(kTermBond, 0, idx));
+      member[base + b[1] - 1].push_back(term_pack(kTermBond, 1, idx));
+    }
+    for (uint32_t k = 0; k < s.n_angles; ++k) {
+      const uint32_t* a = s.angles + 4 * (size_t)k;
+      const uint32_t idx = static_cast<uint32_t>(h_angles.size());
+      h_angles.push_back(make_uint4(base + a[0] - 1, base + a[1] - 1, base + a[2] - 1,
+                                    rp[r].angle_type_base + a[3] - 1));
+      for (uint32_t m = 0; m < 3; ++m) member[base + a[m] - 1].push_back(term_pack(kTermAngle, m, idx));
+    }
+    for (uint32_t k = 0; k < s.n_dihedrals; ++k) {
+      const uint32_t* d = s.dihedrals + 5 * (size_t)k;
+      const uint32_t idx = static_cast<uint32_t>(h_dihedrals.size());
+      h_dihedrals.push_back(make_uint4(base + d[0] - 1, base + d[1] - 1, base + d[2] - 1,
+                                       base + d[3] - 1));
+      h_dih_type.push_back(rp[r].dihedral_type_base + d[4] - 1);
+      for (uint32_t m = 0; m < 4; ++m) member[base + d[m] - 1].push_back(term_pack(kTermDihedral, m, idx));
+    }
+  }
+  if (h_bonds.size() >= (1u << 28) || h_angles.size() >= (1u << 28) ||
+      h_dihedrals.size() >= (1u << 28)) {
+    throw OverflowError("bonded term count exceeds 2^28.");
+  }
+  std::vector<uint32_t> term_off(T + 1, 0), term;
+  for (uint32_t t = 0; t < T; ++t) {
+    term_off[t + 1] = term_off[t] + static_cast<uint32_t>(member[t].size());
+  }
+  term.reserve(term_off[T]);
+  for (uint32_t t = 0; t < T; ++t) term.insert(term.end(), member[t].begin(), member[t].end());
+
+  // ---- LJ tables ----
+  std::vector<LjCoeff> h_lj(lj_entries);
+  for (uint32_t r = 0; r < n; ++r) {
+    const beads_forcefield_desc& f = ffs[r];
+    const float rc = static_cast<float>(f.lj_cutoff);
+    for (int i = 0; i < f.n_types; ++i) {
+      for (int j = 0; j < f.n_types; ++j) {
+        const float eps = static_cast<float>(f.lj_epsilon[i * f.n_types + j]);
+        const float sig = static_cast<float>(f.lj_sigma[i * f.n_types + j]);
+        LjCoeff c;
+        c.sigma2 = sig * sig;
+        c.eps4 = 4.0f * eps;
+        c.eps24 = 6.0f * c.eps4;
+        c.shift = 0.0f;
+        if (f.lj_shift) {
+          const float sr2 = c.sigma2 / (rc * rc);
+          const float sr6 = sr2 * sr2 * sr2;
+          c.shift = c.eps4 * (sr6 * sr6 - sr6);
+        }
+        h_lj[rp[r].lj_offset + i * f.n_types + j] = c;
+      }
+    }
+  }
+
+  // ---- device allocation ----
+  DeviceView& v = v_;
+  v.n_replicas = n;
+  v.n_slots = S;
+  v.n_blocks = S / kBlock;
+  v.total_cells = C;
+  v.nbr_stride = stride;
+  v.excl_cap = static_cast<uint32_t>(excl_cap);
+  v.has_bonded = any_bonded ? 1 : 0;
+  v.pos = dalloc<float4>(S);
+  v.vel = dalloc<float4>(S);
+  v.force = dalloc<float4>(S);
+  v.img = dalloc<int4>(S);
+  v.tag = dalloc<uint32_t>(S);
+  v.mol = dalloc<uint32_t>(S);
+  v.ref_pos = dalloc<float4>(S);
+  v.ref_img = dalloc<int4>(S);
+  v.pos2 = dalloc<float4>(S);
+  v.vel2 = dalloc<float4>(S);
+  v.img2 = dalloc<int4>(S);
+  v.tag2 = dalloc<uint32_t>(S);
+  v.mol2 = dalloc<uint32_t>(S);
+  v.cell2 = dalloc<uint32_t>(S);
+  v.cell_of_slot = dalloc<uint32_t>(S);
+  v.cell_count = dalloc<uint32_t>(C);
+  v.cell_cursor = dalloc<uint32_t>(C);
+  v.cell_start = dalloc<uint32_t>(static_cast<size_t>(C) + n);
+  v.cell_atoms = dalloc<uint32_t>(S);
+  v.nbr_count = dalloc<uint32_t>(S);
+  v.nbr = dalloc<uint32_t>(list_entries);
+  v.slot_of_tag = dalloc<uint32_t>(T);
+  v.excl_slot = dalloc<uint32_t>(static_cast<size_t>(S) * std::max(1, excl_cap));
+  uint32_t* d_excl_off = dalloc<uint32_t>(T + 1);
+  uint32_t* d_excl_tag = dalloc<uint32_t>(excl_tag.size());
+  uint32_t* d_term_off = dalloc<uint32_t>(T + 1);
+  uint32_t* d_term = dalloc<uint32_t>(term.size());
+  uint4* d_bonds = dalloc<uint4>(h_bonds.size());
+  uint4* d_angles = dalloc<uint4>(h_angles.size());
+  uint4* d_dihedrals = dalloc<uint4>(h_dihedrals.size());
+  uint32_t* d_dih_type = dalloc<uint32_t>(h_dih_type.size());
+  BondCoeff* d_bc = dalloc<BondCoeff>(h_bc.size());
+  AngleCoeff* d_ac = dalloc<AngleCoeff>(h_ac.size());
+  DihedralCoeff* d_dc = dalloc<DihedralCoeff>(h_dc.size());
+  ReplicaParams* d_rp = dalloc<ReplicaParams>(n);
+  v.rs = dalloc<ReplicaState>(n);
+  v.obs = dalloc<ReplicaObs>(n);
+  uint32_t* d_block_replica = dalloc<uint32_t>(block_replica.size());
+  LjCoeff* d_lj = dalloc<LjCoeff>(h_lj.size());
+
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes) cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_), "upload");
+  };
+  up(v.pos, h_pos.data(), S * sizeof(float4));
+  up(v.vel, h_vel.data(), S * sizeof(float4));
+  up(v.img, h_img.data(), S * sizeof(int4));
+  up(v.tag, h_tag.data(), S * sizeof(uint32_t));
+  up(v.mol, h_mol.data(), S * sizeof(uint32_t));
+  up(v.slot_of_tag, slot_of_tag.data(), T * sizeof(uint32_t));
+  up(d_excl_off, excl_off.data(), excl_off.size() * sizeof(uint32_t));
+  up(d_excl_tag, excl_tag.data(), excl_tag.size() * sizeof(uint32_t));
+  up(d_term_off, term_off.data(), term_off.size() * sizeof(uint32_t));
+  up(d_term, term.data(), term.size() * sizeof(uint32_t));
+  up(d_bonds, h_bonds.data(), h_bonds.size() * sizeof(uint4));
+  up(d_angles, h_angles.data(), h_angles.size() * sizeof(uint4));
+  up(d_dihedrals, h_dihedrals.data(), h_dihedrals.size() * sizeof(uint4));
+  up(d_dih_type, h_dih_type.data(), h_dih_type.size() * sizeof(uint32_t));
+  up(d_bc, h_bc.data(), h_bc.size() * sizeof(BondCoeff));
+  up(d_ac, h_ac.data(), h_ac.size() * sizeof(AngleCoeff));
+  up(d_dc, h_dc.data(), h_dc.size() * sizeof(DihedralCoeff));
+  up(d_rp, rp.data(), n * sizeof(ReplicaParams));
+  up(d_block_replica, block_replica.data(), block_replica.size() * sizeof(uint32_t));
+  up(d_lj, h_lj.data(), h_lj.size() * sizeof(LjCoeff));
+  std::vector<ReplicaState> rs(n);
+  std::memset(rs.data(), 0, n * sizeof(ReplicaState));
+  for (auto& x : rs) x.lambda = 1.0;
+  up(v.rs, rs.data(), n * sizeof(ReplicaState));
+  v.excl_off = d_excl_off;
+  v.excl_tag = d_excl_tag;
+  v.term_off = d_term_off;
+  v.term = d_term;
+  v.bonds = d_bonds;
+  v.angles = d_angles;
+  v.dihedrals = d_dihedrals;
+  v.dihedral_type = d_dih_type;
+  v.bond_coeff = d_bc;
+  v.angle_coeff = d_ac;
+  v.dihedral_coeff = d_dc;
+  v.rp = d_rp;
+  v.block_replica = d_block_replica;
+  v.lj = d_lj;
+
+  cuda_check(cudaMallocHost(&h_obs_, n * sizeof(ReplicaObs)), "cudaMallocHost");
+  cuda_check(cudaMallocHost(&h_state_, n * sizeof(ReplicaState)), "cudaMallocHost");
+
+  launch_.v = v;
+  launch_.stream = stream_;
+  launch_.max_cells_per_replica = max_cells;
+  launch_.max_atoms_per_replica = max_atoms;
+  launch_.excl_cap = excl_cap;
+  launch_.need_kinetic = any_thermostat ? 1 : 0;
+  // Initial slot-space exclusion rows (slot order = input order).
+  launch_project_exclusions(launch_, true);
+  cuda_check(cudaStreamSynchronize(stream_), "setup");
+  host_row_tag_ = std::move(h_tag);
+}
+
+void Engine::sync() { cuda_check(cudaStreamSynchronize(stream_), "stream synchronize"); }
+
+void Engine::check_status() {
+  sync();
+  cuda_check(cudaMemcpy(h_state_, v_.rs, rep_.size() * sizeof(ReplicaState),
+                        cudaMemcpyDeviceToHost),
+             "status download");
+  for (uint32_t r = 0; r < rep_.size(); ++r) {
+    const unsigned s = h_state_[r].status;
+    if (s & kStatusNeighborOverflow) {
+      const ReplicaHost& h = rep_[r];
+      std::ostringstream m;
+      m << "NeighborList overflow"
+        << "\npath=" << path_name(h.plan.path) << "\nn_particles=" << h.n_atoms
+        << "\nmax_neighbors=" << h.max_neighbors << "\nforce_cutoff=" << h.plan.force_cutoff
+        << "\ncutoff_buffer=" << h.plan.cutoff_buffer
+        << "\nsearch_cutoff=" << h.plan.search_cutoff
+        << ". Increase max_neighbors before consuming this neighbor list.";
+      if (rep_.size() > 1) m << " (replica " << r << ")";
+      throw NeighborOverflow(m.str());
+    }
+    if (s & kStatusFixedOverflow) {
+      throw OverflowError("energy/virial total exceeds the fixed-point accumulator range.");
+    }
+    if (s & kStatusNonFinite) {
+      throw NonFinite("non-finite velocity after force evaluation (replica " +
+                      std::to_string(r) + ").");
+    }
+  }
+}
+
+void Engine::eval() {
+  launch_apply_lambda(launch_);
+  launch_rebuild(launch_, true);
+  launch_forces(launch_, true, false);
+  launch_post(launch_, false, true);
+  check_status();
+  initialized_ = true;
+}
+
+void Engine::record_step(bool observables) {
+  launch_pre(launch_, kPreVerlet);
+  launch_rebuild(launch_, false);
+  launch_forces(launch_, observables, false);
+  launch_post(launch_, true, observables);
+}
+
+cudaGraphExec_t Engine::graph_for(uint32_t steps, bool obs_last) {
+  const auto key = std::make_pair(steps, obs_last);
+  auto it = graphs_.find(key);
+  if (it != graphs_.end()) return it->second.second;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+  try {
+    for (uint32_t s = 0; s < steps; ++s) record_step(obs_last && s + 1 == steps);
+  } catch (...) {
+    cudaStreamEndCapture(stream_, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  cuda_check(cudaStreamEndCapture(stream_, &graph), "end capture");
+  cuda_check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+  graphs_[key] = std::make_pair(graph, exec);
+  return exec;
+}
+
+void Engine::launch_chunk(uint32_t steps, bool obs_last) {
+  if (use_graphs_) {
+    cuda_check(cudaGraphLaunch(graph_for(steps, obs_last), stream_), "graph launch");
+  } else {
+    for (uint32_t s = 0; s < steps; ++s) record_step(obs_last && s + 1 == steps);
+  }
+}
+
+bool Engine::run(uint64_t steps, uint64_t obs_every) {
+  if (!initialized_) eval();
+  bool last_obs = false;
+  uint64_t remaining = steps;
+  while (remaining > 0) {
+    uint64_t chunk = std::min<uint64_t>(remaining, kChunkMax);
+    bool obs = false;
+    if (obs_every > 0) {
+      const uint64_t next = (step_ / obs_every + 1) * obs_every;
+      if (next - step_ <= chunk) {
+        chunk = next - step_;
+        obs = true;
+      }
+    }
+    launch_chunk(static_cast<uint32_t>(chunk), obs);
+    step_ += chunk;
+    remaining -= chunk;
+    last_obs = obs;
+  }
+  check_status();
+  return last_obs;
+}
+
+void Engine::minimize(uint32_t iterations, float dmax, float fref) {
+  StepLaunch l = launch_;
+  l.sd_dmax = dmax;
+  l.sd_fref = fref;
+  launch_rebuild(l, true);
+  for (uint32_t it = 0; it < iterations; ++it) {
+    launch_forces(l, false, true);
+    launch_pre(l, kPreDescent);
+    launch_rebuild(l, false);
+  }
+  sync();
+  // The descent is set-up work: reset counters so a following run starts
+  // like a fresh one.
+  check_status();
+  for (uint32_t r = 0; r < rep_.size(); ++r) {
+    h_state_[r].builds = 0;
+    h_state_[r].dangerous = 0;
+    h_state_[r].checks_since_build = 0;
+    h_state_[r].need_rebuild = 0;
+    h_state_[r].reorder_now = 0;
+    h_state_[r].step = 0;
+    h_state_[r].lambda = 1.0;
+  }
+  cuda_check(cudaMemcpy(v_.rs, h_state_, rep_.size() * sizeof(ReplicaState),
+                        cudaMemcpyHostToDevice),
+             "state reset");
+  initialized_ = false;
+  step_ = 0;
+}
+
+void Engine::flush_lambda() { launch_apply_lambda(launch_); }
+
+void Engine::observables(std::vector<beads_observables>& out) {
+  sync();
+  cuda_check(cudaMemcpy(h_obs_, v_.obs, rep_.size() * sizeof(ReplicaObs), cudaMemcpyDeviceToHost),
+             "observables download");
+  out.resize(rep_.size());
+  for (uint32_t r = 0; r < rep_.size(); ++r) {
+    const ReplicaObs& o = h_obs_[r];
+    const ReplicaHost& h = rep_[r];
+    beads_observables& b = out[r];
+    b.step = o.step;
+    b.pair_pe = o.pair_pe;
+    b.bond_pe = o.bond_pe;
+    b.angle_pe = o.angle_pe;
+    b.dihedral_pe = o.dihedral_pe;
+    b.pe = o.pair_pe + o.bond_pe + o.angle_pe + o.dihedral_pe;
+    b.ke = o.lambda * o.lambda * o.ke_pre;
+    b.virial = o.virial;
+    const double kb = h.units == BEADS_UNITS_NM_KJMOL ? kKbNmKjMol : 1.0;
+    const double ps = h.units == BEADS_UNITS_NM_KJMOL ? kPressNmKjMol : 1.0;
+    const double dof = std::max(0.0, 3.0 * h.n_atoms - 3.0);
+    b.temp = (dof > 0.0) ? 2.0 * b.ke / (dof * kb) : 0.0;
+    const double vol = static_cast<double>(h.box_hi[0] - h.box_lo[0]) *
+                       static_cast<double>(h.box_hi[1] - h.box_lo[1]) *
+                       static_cast<double>(h.box_hi[2] - h.box_lo[2]);
+    b.press = vol > 0.0 ? ps * (2.0 * b.ke + b.virial) / (3.0 * vol) : 0.0;
+    b.neighbor_build_count = o.builds;
+    b.dangerous_rebuild_count = o.dangerous;
+  }
+}
+
+void Engine::slot_view(uint32_t r, SlotView& out) {
+  const ReplicaHost& h = rep_.at(r);
+  flush_lambda();
+  sync();
+  const size_t n = h.n_atoms;
+  out.pos.resize(n);
+  out.vel.resize(n);
+  out.force.resize(n);
+  out.img.resize(n);
+  out.tag.resize(n);
+  out.mol.resize(n);
+  const size_t b = h.atom_begin;
+  cuda_check(cudaMemcpy(out.pos.data(), v_.pos + b, n * sizeof(float4), cudaMemcpyDeviceToHost), "d2h");
+  cuda_check(cudaMemcpy(out.vel.data(), v_.vel + b, n * sizeof(float4), cudaMemcpyDeviceToHost), "d2h");
+  cuda_check(cudaMemcpy(out.force.data(), v_.force + b, n * sizeof(float4), cudaMemcpyDeviceToHost), "d2h");
+  cuda_check(cudaMemcpy(out.img.data(), v_.img + b, n * sizeof(int4), cudaMemcpyDeviceToHost), "d2h");
+  cuda_check(cudaMemcpy(out.tag.data(), v_.tag + b, n * sizeof(uint32_t), cudaMemcpyDeviceToHost), "d2h");
+  cuda_check(cudaMemcpy(out.mol.data(), v_.mol + b, n * sizeof(uint32_t), cudaMemcpyDeviceToHost), "d2h");
+  for (auto& t : out.tag) t = t - h.tag_base + 1;  // 1-based local tags
+}
+
+void Engine::state(uint32_t r, float* pos, float* vel, float* force, int32_t* img,
+                   uint32_t*, int32_t*) {
+  SlotView sv;
+  slot_view(r, sv);
+  for (size_t k = 0; k < sv.tag.size(); ++k) {
+    const size_t t = sv.tag[k] - 1;
+    if (pos) {
+      pos[3 * t] = sv.pos[k].x;
+      pos[3 * t + 1] = sv.pos[k].y;
+      pos[3 * t + 2] = sv.pos[k].z;
+    }
+    if (vel) {
+      vel[3 * t] = sv.vel[k].x;
+      vel[3 * t + 1] = sv.vel[k].y;
+      vel[3 * t + 2] = sv.vel[k].z;
+    }
+    if (force) {
+      force[3 * t] = sv.force[k].x;
+      force[3 * t + 1] = sv.force[k].y;
+      force[3 * t + 2] = sv.force[k].z;
+    }
+    if (img) {
+      img[3 * t] = sv.img[k].x;
+      img[3 * t + 1] = sv.img[k].y;
+      img[3 * t + 2] = sv.img[k].z;
+    }
+  }
+}
+
+void Engine::set_state(uint32_t r, const float* pos, const float* vel) {
+  const ReplicaHost& h = rep_.at(r);
+  if (pos) {
+    for (uint64_t k = 0; k < 3ull * h.n_atoms; ++k) {
+      const int a = static_cast<int>(k % 3);
+      if (!(pos[k] >= h.box_lo[a] && pos[k] < h.box_hi[a])) {
+        throw InvalidArgument("positions must be inside box_bound");
+      }
+    }
+  }
+  if (!d_xfer_pos_) {
+    d_xfer_pos_ = dalloc<float>(3 * n_tags_);
+    d_xfer_vel_ = dalloc<float>(3 * n_tags_);
+  }
+  flush_lambda();
+  const size_t off = 3ull * h.tag_base;
+  const size_t bytes = 3ull * h.n_atoms * sizeof(float);
+  // Stage this replica's rows and scatter only them: the kernel walks all
+  // tags, so the other replicas' rows are first refreshed from the device.
+  launch_gather_state(launch_, d_xfer_pos_, d_xfer_vel_, static_cast<uint32_t>(n_tags_));
+  if (pos) cuda_check(cudaMemcpyAsync(d_xfer_pos_ + off, pos, bytes, cudaMemcpyHostToDevice, stream_), "h2d");
+  if (vel) cuda_check(cudaMemcpyAsync(d_xfer_vel_ + off, vel, bytes, cudaMemcpyHostToDevice, stream_), "h2d");
+  launch_scatter_state(launch_, d_xfer_pos_, d_xfer_vel_, static_cast<uint32_t>(n_tags_));
+  sync();
+  initialized_ = false;
+}
+
+void Engine::upload_all(const float* pos, const float* vel) {
+  if (!d_xfer_pos_) {
+    d_xfer_pos_ = dalloc<float>(3 * n_tags_);
+    d_xfer_vel_ = dalloc<float>(3 * n_tags_);
+  }
+  const size_t bytes = 3ull * n_tags_ * sizeof(float);
+  flush_lambda();
+  if (pos) cuda_check(cudaMemcpyAsync(d_xfer_pos_, pos, bytes, cudaMemcpyHostToDevice, stream_), "h2d");
+  if (vel) cuda_check(cudaMemcpyAsync(d_xfer_vel_, vel, bytes, cudaMemcpyHostToDevice, stream_), "h2d");
+  launch_scatter_state(launch_, pos ? d_xfer_pos_ : nullptr, vel ? d_xfer_vel_ : nullptr,
+                       static_cast<uint32_t>(n_tags_));
+  initialized_ = false;
+}
+
+void Engine::download_all(float* pos, float* vel) {
+  if (!d_xfer_pos_) {
+    d_xfer_pos_ = dalloc<float>(3 * n_tags_);
+    d_xfer_vel_ = dalloc<float>(3 * n_tags_);
+  }
+  const size_t bytes = 3ull * n_tags_ * sizeof(float);
+  flush_lambda();
+  launch_gather_state(launch_, d_xfer_pos_, d_xfer_vel_, static_cast<uint32_t>(n_tags_));
+  if (pos) cuda_check(cudaMemcpyAsync(pos, d_xfer_pos_, bytes, cudaMemcpyDeviceToHost, stream_), "d2h");
+  if (vel) cuda_check(cudaMemcpyAsync(vel, d_xfer_vel_, bytes, cudaMemcpyDeviceToHost, stream_), "d2h");
+  sync();
+}
+
+void Engine::debug_cells(uint32_t r, uint32_t* cell_by_tag) {
+  const ReplicaHost& h = rep_.at(r);
+  sync();
+  std::vector<uint32_t> cell(h.n_atoms), tag(h.n_atoms);
+  cuda_check(cudaMemcpy(cell.data(), v_.cell_of_slot + h.atom_begin, h.n_atoms * 4, cudaMemcpyDeviceToHost), "d2h");
+  cuda_check(cudaMemcpy(tag.data(), v_.tag + h.atom_begin, h.n_atoms * 4, cudaMemcpyDeviceToHost), "d2h");
+  std::vector<ReplicaParams> rp(1);
+  cuda_check(cudaMemcpy(rp.data(), v_.rp + r, sizeof(ReplicaParams), cudaMemcpyDeviceToHost), "d2h");
+  for (uint32_t k = 0; k < h.n_atoms; ++k) {
+    cell_by_tag[tag[k] - h.tag_base] = cell[k] - rp[0].cell_begin;
+  }
+}
+
+void Engine::debug_neighbors(uint32_t r, uint32_t cap, uint32_t* counts, uint32_t* partners) {
+  const ReplicaHost& h = rep_.at(r);
+  sync();
+  const uint32_t S = v_.n_slots;
+  std::vector<uint32_t> cnt(S), tag(S);
+  cuda_check(cudaMemcpy(cnt.data(), v_.nbr_count, S * 4ull, cudaMemcpyDeviceToHost), "d2h");
+  cuda_check(cudaMemcpy(tag.data(), v_.tag, S * 4ull, cudaMemcpyDeviceToHost), "d2h");
+  // Only the groups of this replica's slots are copied.
+  const uint64_t g0 = h.atom_begin / kGroup, g1 = (h.atom_begin + h.n_pad) / kGroup;
+  const uint64_t per_group = static_cast<uint64_t>(v_.nbr_stride) * kGroup;
+  std::vector<uint32_t> list((g1 - g0) * per_group);
+  cuda_check(cudaMemcpy(list.data(), v_.nbr + g0 * per_group, list.size() * 4ull, cudaMemcpyDeviceToHost), "d2h");
+  for (uint32_t k = 0; k < h.n_atoms; ++k) {
+    const uint32_t slot = h.atom_begin + k;
+    const uint32_t t = tag[slot] - h.tag_base;  // 0-based local
+    const uint32_t c = cnt[slot];
+    counts[t] = c;
+    for (uint32_t q = 0; q < c && q < cap; ++q) {
+      const uint64_t at = nbr_index(slot, q, v_.nbr_stride) - g0 * per_group;
+      const uint32_t j = list[at];
+      partners[static_cast<uint64_t>(t) * cap + q] = tag[j] - h.tag_base + 1;
+    }
+  }
+}
+
+}  // namespace bb

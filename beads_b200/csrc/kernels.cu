@@ -1,0 +1,983 @@
+// kernels.cu -- sm_100a kernels of the BEADS per-step hot path.
+//
+// Reference behaviour followed (paths inside the reference project):
+//   cell id             native/src/simulation/neighbor/cell_list_build.cu:110-166
+//   neighbour inclusion native/src/simulation/neighbor/full/full_neighbor_path_common.cuh:49-94
+//   stencils            full/regular_cell_neighbor_builder.cu:40-113,
+//                       full/small_dimension_neighbor_builder.cu:56-142
+//   rebuild policy      native/src/simulation/neighbor/neighbor_system.cpp:79-216
+//   displacement check  native/src/simulation/neighbor/rebuild_tracker.cu:50-94
+//   LJ pair             native/src/forcefield/pair/pair_lj.cu:21-192
+//   harmonic bond       native/src/forcefield/bond/bond_harmonic.cu:24-99
+//   harmonic angle      native/src/forcefield/angle/angle_harmonic.cu:23-178
+//   harmonic dihedral   native/src/forcefield/dihedral/dihedral_harmonic.cu:22-227
+//   velocity Verlet     native/src/dynamics/integrator/velocity_verlet.cu:59-111
+//   Berendsen           native/src/dynamics/thermostat/berendsen_thermostat.cu:104-163
+//
+// Design (not a translation): every kernel runs over all replicas of a batch
+// at once; a block never straddles two replicas; the rebuild decision is taken
+// on the device so a captured step loop needs no host round trip; totals are
+// reduced in 64-bit fixed point so they do not depend on block scheduling;
+// bonded forces are gathered per particle (each thread evaluates the terms its
+// particle belongs to) so no force atomics exist anywhere.
+#include "kernels.cuh"
+
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+namespace bb {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ long long to_fixed(double v, unsigned* status) {
+  if (!(fabs(v) < kFixLimit)) {
+    atomicOr(status, kStatusFixedOverflow);
+    return 0;
+  }
+  return __double2ll_rn(v * kFixScale);
+}
+
+__device__ __forceinline__ double from_fixed(long long v) {
+  return (double)v / kFixScale;
+}
+
+// Warp + block sum of a 64-bit integer, one atomic per block.
+template <int kThreads>
+__device__ __forceinline__ void block_add_ll(long long v, long long* target) {
+  __shared__ long long partial[kThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) partial[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long s = 0;
+    for (int w = 0; w < kThreads / 32; ++w) s += partial[w];
+    if (s != 0) atomicAdd(reinterpret_cast<unsigned long long*>(target),
+                          static_cast<unsigned long long>(s));
+  }
+  __syncthreads();
+}
+
+// Minimum image exactly as the reference applies it to wrapped coordinates
+// (box_geometry_view.cuh:50-62): one subtraction, then one shift by L.
+__device__ __forceinline__ float ref_delta(float xi, float xj, float len,
+                                           float half) {
+  float d = __fsub_rn(xi, xj);
+  if (d > half) {
+    d = __fsub_rn(d, len);
+  } else if (d < -half) {
+    d = __fadd_rn(d, len);
+  }
+  return d;
+}
+
+// Minimum image rounded once from the exact difference.  When the pair spans
+// the periodic boundary the reference's form rounds xi - xj at the magnitude
+// of L before shifting; here the rounding error of xi - xj is recovered with
+// Knuth's TwoSum and added back after the (exact, by Sterbenz) shift by L.
+__device__ __forceinline__ float acc_delta(float xi, float xj, float len,
+                                           float half) {
+  float d = __fsub_rn(xi, xj);
+  if (fabsf(d) > half) {
+    const float nxj = -xj;
+    const float bp = __fsub_rn(d, xi);
+    const float ap = __fsub_rn(d, bp);
+    const float err = __fadd_rn(__fsub_rn(xi, ap), __fsub_rn(nxj, bp));
+    const float shifted = d > 0.0f ? __fsub_rn(d, len) : __fadd_rn(d, len);
+    d = __fadd_rn(shifted, err);
+  }
+  return d;
+}
+
+// |d|^2 with the contraction order fixed: fma(dz,dz, fma(dy,dy, dx*dx)).
+__device__ __forceinline__ float norm2(float dx, float dy, float dz) {
+  return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+}
+
+__device__ __forceinline__ uint32_t axis_cell(float x, float lo, float inv,
+                                              uint32_t n) {
+  const float scaled = __fmul_rn(__fsub_rn(x, lo), inv);
+  if (scaled <= 0.0f) return 0u;
+  if (scaled >= (float)n) return n - 1u;   // also catches NaN-free overflow
+  const uint32_t idx = (uint32_t)scaled;
+  return idx >= n ? n - 1u : idx;
+}
+
+// Cells visited along one axis around centre c (unique, so that one or two
+// cells per axis are not visited twice).  Same set rule as the reference's
+// unique_axis_cells (small_dimension_neighbor_builder.cu:56-76).
+__device__ __forceinline__ int axis_stencil(uint32_t c, uint32_t n,
+                                            uint32_t out[3]) {
+  if (n <= 1u) {
+    out[0] = 0u;
+    return 1;
+  }
+  if (n == 2u) {
+    out[0] = 0u;
+    out[1] = 1u;
+    return 2;
+  }
+  out[0] = c == 0u ? n - 1u : c - 1u;
+  out[1] = c;
+  out[2] = c + 1u == n ? 0u : c + 1u;
+  return 3;
+}
+
+// Last block of a replica to finish a kernel (threadfence-reduction pattern:
+// no waiting, the last arriving block does the per-replica epilogue).
+__device__ __forceinline__ bool arrive_last(unsigned int* counter,
+                                            unsigned int n_blocks) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned prev = atomicAdd(counter, 1u);
+    last = (prev + 1u == n_blocks);
+  }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// ---------------------------------------------------------------------------
+// pre: Berendsen lambda of the previous step, half-kick, drift, wrap, image
+// update, displacement check; the last block of each replica decides the
+// rebuild for this step (neighbor_system.cpp:79-105).
+template <int kMode>
+__global__ void __launch_bounds__(kBlock)
+k_pre(DeviceView v, float sd_dmax, float sd_fref) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const ReplicaParams& p = v.rp[r];
+  ReplicaState* st = &v.rs[r];
+  const uint32_t slot = b * kBlock + threadIdx.x;
+  const uint32_t local = slot - p.atom_begin;
+  const unsigned long long phys = st->step + 1ull;
+  const bool check_step = (kMode == kPreDescent) || p.skin == 0.0f ||
+                          (phys % (unsigned long long)p.check_every) == 0ull;
+  const float lam = (kMode == kPreVerlet) ? (float)st->lambda : 1.0f;
+
+  if (local < p.n_atoms) {
+    float4 x = v.pos[slot];
+    float4 vm = v.vel[slot];
+    const float4 f = v.force[slot];
+    if (kMode == kPreVerlet) {
+      if (lam != 1.0f) {
+        vm.x = __fmul_rn(vm.x, lam);
+        vm.y = __fmul_rn(vm.y, lam);
+        vm.z = __fmul_rn(vm.z, lam);
+      }
+      const float h = __fdiv_rn(__fmul_rn(0.5f, p.dt), vm.w);
+      vm.x = __fmaf_rn(h, f.x, vm.x);
+      vm.y = __fmaf_rn(h, f.y, vm.y);
+      vm.z = __fmaf_rn(h, f.z, vm.z);
+      x.x = __fmaf_rn(p.dt, vm.x, x.x);
+      x.y = __fmaf_rn(p.dt, vm.y, x.y);
+      x.z = __fmaf_rn(p.dt, vm.z, x.z);
+      v.vel[slot] = vm;
+    } else {
+      const float fn = sqrtf(norm2(f.x, f.y, f.z));
+      const float s = sd_dmax / fmaxf(fn, sd_fref);
+      if (isfinite(s) && isfinite(fn)) {
+        x.x = __fmaf_rn(s, f.x, x.x);
+        x.y = __fmaf_rn(s, f.y, x.y);
+        x.z = __fmaf_rn(s, f.z, x.z);
+      }
+    }
+    int4 im = v.img[slot];
+    {
+      const float cx = floorf(__fmul_rn(__fsub_rn(x.x, p.lo[0]), p.inv_len[0]));
+      const float cy = floorf(__fmul_rn(__fsub_rn(x.y, p.lo[1]), p.inv_len[1]));
+      const float cz = floorf(__fmul_rn(__fsub_rn(x.z, p.lo[2]), p.inv_len[2]));
+      x.x = __fmaf_rn(-cx, p.len[0], x.x);
+      x.y = __fmaf_rn(-cy, p.len[1], x.y);
+      x.z = __fmaf_rn(-cz, p.len[2], x.z);
+      im.x += (int)cx;
+      im.y += (int)cy;
+      im.z += (int)cz;
+    }
+    v.pos[slot] = x;
+    v.img[slot] = im;
+    if (check_step) {
+      const float4 rx = v.ref_pos[slot];
+      const int4 ri = v.ref_img[slot];
+      const float dx = __fmaf_rn((float)((long long)im.x - (long long)ri.x),
+                                 p.len[0], __fsub_rn(x.x, rx.x));
+      const float dy = __fmaf_rn((float)((long long)im.y - (long long)ri.y),
+                                 p.len[1], __fsub_rn(x.y, rx.y));
+      const float dz = __fmaf_rn((float)((long long)im.z - (long long)ri.z),
+                                 p.len[2], __fsub_rn(x.z, rx.z));
+      if (norm2(dx, dy, dz) > p.disp_thr_sq) atomicExch(&st->exceeded, 1u);
+    }
+  }
+
+  const uint32_t n_blocks = p.n_pad / kBlock;
+  if (arrive_last(&st->done_pre, n_blocks) && threadIdx.x == 0) {
+    const unsigned exceeded = atomicExch(&st->exceeded, 0u);
+    unsigned need = 0u;
+    if (kMode == kPreDescent || p.skin == 0.0f) {
+      need = (kMode == kPreDescent) ? exceeded : 1u;
+    } else if (check_step) {
+      const bool first = st->checks_since_build == 0u;
+      st->checks_since_build += 1u;
+      if (exceeded) {
+        need = 1u;
+        if (p.check_every > 1u && first) st->dangerous += 1ull;
+      }
+    }
+    if (need) {
+      st->builds += 1ull;
+      st->reorder_now =
+          (p.sort_every > 0u && (st->builds % p.sort_every) == 0ull) ? 1u : 0u;
+      st->checks_since_build = 0u;
+    } else {
+      st->reorder_now = 0u;
+    }
+    st->need_rebuild = need;
+    if (kMode == kPreVerlet) st->lambda = 1.0;
+    st->done_pre = 0u;
+  }
+}
+
+// Marks every replica for a rebuild (initial build / explicit eval).
+__global__ void k_force_rebuild_flags(DeviceView v, int count_build) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= v.n_replicas) return;
+  ReplicaState* st = &v.rs[r];
+  const ReplicaParams& p = v.rp[r];
+  st->need_rebuild = 1u;
+  if (count_build) {
+    st->builds += 1ull;
+    st->reorder_now =
+        (p.sort_every > 0u && (st->builds % p.sort_every) == 0ull) ? 1u : 0u;
+  } else {
+    st->reorder_now = 0u;
+  }
+  st->checks_since_build = 0u;
+}
+
+// ---------------------------------------------------------------------------
+// rebuild 1: cell id and per-cell count.
+__global__ void __launch_bounds__(kBlock) k_bin(DeviceView v) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  if (!v.rs[r].need_rebuild) return;
+  const ReplicaParams& p = v.rp[r];
+  const uint32_t slot = b * kBlock + threadIdx.x;
+  const uint32_t local = slot - p.atom_begin;
+  if (local >= p.n_atoms) return;
+  const float4 x = v.pos[slot];
+  const uint32_t ix = axis_cell(x.x, p.lo[0], p.inv_cell[0], p.nc[0]);
+  const uint32_t iy = axis_cell(x.y, p.lo[1], p.inv_cell[1], p.nc[1]);
+  const uint32_t iz = axis_cell(x.z, p.lo[2], p.inv_cell[2], p.nc[2]);
+  const uint32_t cell = p.cell_begin + ix + p.nc[0] * (iy + p.nc[1] * iz);
+  v.cell_of_slot[slot] = cell;
+  atomicAdd(&v.cell_count[cell], 1u);
+}
+
+// rebuild 2: exclusive scan of the counts of one replica (one block per
+// replica); resets the counts for the next build.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) k_scan(DeviceView v) {
+  const uint32_t r = blockIdx.x;
+  if (!v.rs[r].need_rebuild) return;
+  const ReplicaParams& p = v.rp[r];
+  __shared__ uint32_t sums[kScanThreads];
+  const uint32_t n = p.n_cells;
+  const uint32_t per = (n + kScanThreads - 1) / kScanThreads;
+  const uint32_t begin = min(n, threadIdx.x * per);
+  const uint32_t end = min(n, begin + per);
+  uint32_t local = 0;
+  for (uint32_t c = begin; c < end; ++c) local += v.cell_count[p.cell_begin + c];
+  sums[threadIdx.x] = local;
+  __syncthreads();
+  // Hillis-Steele inclusive scan over the thread sums.
+  for (int o = 1; o < kScanThreads; o <<= 1) {
+    const uint32_t add = threadIdx.x >= (uint32_t)o ? sums[threadIdx.x - o] : 0u;
+    __syncthreads();
+    sums[threadIdx.x] += add;
+    __syncthreads();
+  }
+  uint32_t run = p.atom_begin + (threadIdx.x > 0 ? sums[threadIdx.x - 1] : 0u);
+  for (uint32_t c = begin; c < end; ++c) {
+    const uint32_t g = p.cell_begin + c;
+    const uint32_t cnt = v.cell_count[g];
+    v.cell_start[p.start_base + c] = run;
+    v.cell_cursor[g] = run;
+    v.cell_count[g] = 0u;
+    run += cnt;
+  }
+  if (threadIdx.x == 0) v.cell_start[p.start_base + n] = p.atom_begin + p.n_atoms;
+}
+
+// rebuild 3: scatter slots into their cells (order inside a cell is fixed by
+// the next kernel).
+__global__ void __launch_bounds__(kBlock) k_scatter(DeviceView v) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  if (!v.rs[r].need_rebuild) return;
+  const ReplicaParams& p = v.rp[r];
+  const uint32_t slot = b * kBlock + threadIdx.x;
+  if (slot - p.atom_begin >= p.n_atoms) return;
+  const uint32_t at = atomicAdd(&v.cell_cursor[v.cell_of_slot[slot]], 1u);
+  v.cell_atoms[at] = slot;
+}
+
+// rebuild 4: sort each cell's slots ascending, which makes the counting sort
+// stable and the whole build deterministic.  One warp per cell; a bitonic
+// network in registers for <= 32 members, insertion sort otherwise.
+__global__ void __launch_bounds__(kBlock) k_cellsort(DeviceView v) {
+  const uint32_t r = blockIdx.y;
+  if (!v.rs[r].need_rebuild) return;
+  const ReplicaParams& p = v.rp[r];
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warps_per_block = kBlock / 32;
+  for (uint32_t c = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
+       c < p.n_cells; c += gridDim.x * warps_per_block) {
+    const uint32_t s0 = v.cell_start[p.start_base + c];
+    const uint32_t s1 = v.cell_start[p.start_base + c + 1];
+    const uint32_t n = s1 - s0;
+    if (n <= 1u) continue;
+    if (n <= 32u) {
+      uint32_t val = lane < n ? v.cell_atoms[s0 + lane] : 0xffffffffu;
+      for (uint32_t k = 2; k <= 32; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+          const uint32_t other = __shfl_xor_sync(kFull, val, j);
+          const bool up = (lane & k) == 0u;
+          const bool lower = (lane & j) == 0u;
+          val = (lower == up) ? min(val, other) : max(val, other);
+        }
+      }
+      if (lane < n) v.cell_atoms[s0 + lane] = val;
+    } else if (lane == 0) {
+      for (uint32_t a = s0 + 1; a < s1; ++a) {
+        const uint32_t key = v.cell_atoms[a];
+        uint32_t q = a;
+        while (q > s0 && v.cell_atoms[q - 1] > key) {
+          v.cell_atoms[q] = v.cell_atoms[q - 1];
+          --q;
+        }
+        v.cell_atoms[q] = key;
+      }
+    }
+  }
+}
+
+// rebuild 5/6: physical reorder into cell order (every sort_every builds).
+__global__ void __launch_bounds__(kBlock) k_reorder_gather(DeviceView v) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const ReplicaState& st = v.rs[r];
+  if (!st.need_rebuild || !st.reorder_now) return;
+  const ReplicaParams& p = v.rp[r];
+  const uint32_t k = b * kBlock + threadIdx.x;
+  if (k - p.atom_begin >= p.n_atoms) return;
+  const uint32_t old = v.cell_atoms[k];
+  v.pos2[k] = v.pos[old];
+  v.vel2[k] = v.vel[old];
+  v.img2[k] = v.img[old];
+  v.tag2[k] = v.tag[old];
+  v.mol2[k] = v.mol[old];
+  v.cell2[k] = v.cell_of_slot[old];
+}
+
+__global__ void __launch_bounds__(kBlock) k_reorder_commit(DeviceView v) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const ReplicaState& st = v.rs[r];
+  if (!st.need_rebuild || !st.reorder_now) return;
+  const ReplicaParams& p = v.rp[r];
+  const uint32_t k = b * kBlock + threadIdx.x;
+  if (k - p.atom_begin >= p.n_atoms) return;
+  v.pos[k] = v.pos2[k];
+  v.vel[k] = v.vel2[k];
+  v.img[k] = v.img2[k];
+  const uint32_t t = v.tag2[k];
+  v.tag[k] = t;
+  v.mol[k] = v.mol2[k];
+  v.cell_of_slot[k] = v.cell2[k];
+  v.cell_atoms[k] = k;
+  v.slot_of_tag[t] = k;
+}
+
+// Exclusion partners of every slot, projected from tag space to slot space
+// (the reference's SlotExclusionRuntime::rebuild_from_source,
+// exclusions.cu:337-460, here one fixed-width row per slot).
+__global__ void __launch_bounds__(kBlock)
+k_project_exclusions(DeviceView v, int force_all) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const ReplicaState& st = v.rs[r];
+  if (!force_all && (!st.need_rebuild || !st.reorder_now)) return;
+  const ReplicaParams& p = v.rp[r];
+  const uint32_t k = b * kBlock + threadIdx.x;
+  if (k - p.atom_begin >= p.n_atoms) return;
+  const uint32_t t = v.tag[k];
+  const uint32_t e0 = v.excl_off[t];
+  const uint32_t e1 = v.excl_off[t + 1];
+  uint32_t* row = v.excl_slot + (size_t)k * v.excl_cap;
+  for (uint32_t e = 0; e < v.excl_cap; ++e) {
+    row[e] = (e0 + e < e1) ? v.slot_of_tag[v.excl_tag[e0 + e]] : 0xffffffffu;
+  }
+}
+
+// rebuild 7: full neighbour list over the cell stencil, reference inclusion
+// rule: skip self and excluded partners, keep r^2 <= (rc+skin)^2, count
+// overflow past max_neighbors.  Also captures the displacement reference.
+template <int kCap>
+__global__ void __launch_bounds__(kBlock) k_build(DeviceView v) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  ReplicaState* st = &v.rs[r];
+  if (!st->need_rebuild) return;
+  const ReplicaParams& p = v.rp[r];
+  const uint32_t i = b * kBlock + threadIdx.x;
+  if (i - p.atom_begin >= p.n_atoms) return;
+
+  const float4 xi = v.pos[i];
+  uint32_t ex[kCap > 0 ? kCap : 1];
+  if (kCap > 0) {
+    const uint32_t* row = v.excl_slot + (size_t)i * v.excl_cap;
+#pragma unroll
+    for (int e = 0; e < kCap; ++e) ex[e] = row[e];
+  }
+  const uint32_t cell = v.cell_of_slot[i] - p.cell_begin;
+  const uint32_t cx = cell % p.nc[0];
+  const uint32_t cyz = cell / p.nc[0];
+  const uint32_t cy = cyz % p.nc[1];
+  const uint32_t cz = cyz / p.nc[1];
+  uint32_t sx[3], sy[3], sz[3];
+  const int nx = axis_stencil(cx, p.nc[0], sx);
+  const int ny = axis_stencil(cy, p.nc[1], sy);
+  const int nz = axis_stencil(cz, p.nc[2], sz);
+
+  uint32_t count = 0;
+  bool overflow = false;
+  const uint32_t cap = p.max_neighbors;
+  for (int a = 0; a < nz; ++a) {
+    for (int bb = 0; bb < ny; ++bb) {
+      const uint32_t rowcell = p.nc[0] * (sy[bb] + p.nc[1] * sz[a]);
+      for (int c = 0; c < nx; ++c) {
+        const uint32_t lc = sx[c] + rowcell;
+        const uint32_t s0 = v.cell_start[p.start_base + lc];
+        const uint32_t s1 = v.cell_start[p.start_base + lc + 1];
+        for (uint32_t q = s0; q < s1; ++q) {
+          const uint32_t j = v.cell_atoms[q];
+          if (j == i) continue;
+          bool excluded = false;
+#pragma unroll
+          for (int e = 0; e < kCap; ++e) excluded |= (ex[e] == j);
+          if (excluded) continue;
+          const float4 xj = v.pos[j];
+          const float dx = ref_delta(xi.x, xj.x, p.len[0], p.half[0]);
+          const float dy = ref_delta(xi.y, xj.y, p.len[1], p.half[1]);
+          const float dz = ref_delta(xi.z, xj.z, p.len[2], p.half[2]);
+          if (norm2(dx, dy, dz) > p.search_cut_sq) continue;
+          if (count < cap) {
+            v.nbr[nbr_index(i, count, v.nbr_stride)] = j;
+            ++count;
+          } else {
+            overflow = true;
+          }
+        }
+      }
+    }
+  }
+  v.nbr_count[i] = count;
+  v.ref_pos[i] = xi;
+  v.ref_img[i] = v.img[i];
+  if (overflow) atomicOr(&st->status, kStatusNeighborOverflow);
+}
+
+// ---------------------------------------------------------------------------
+// LJ pair forces over the full list (each pair evaluated from both ends, no
+// atomics).  FP32 pair arithmetic; per-slot energy and virial are converted to
+// fixed point once per slot and reduced per block.
+template <bool kObs, bool kClamp>
+__global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const ReplicaParams& p = v.rp[r];
+  __shared__ LjCoeff table[kMaxTypes * kMaxTypes];
+  const int nt = p.n_types;
+  for (int t = threadIdx.x; t < nt * nt; t += kBlock) table[t] = v.lj[p.lj_offset + t];
+  __syncthreads();
+
+  const uint32_t i = b * kBlock + threadIdx.x;
+  const bool real = (i - p.atom_begin) < p.n_atoms;
+  float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f, w = 0.f;
+  if (real) {
+    const float4 xi = v.pos[i];
+    const LjCoeff* row = table + __float_as_int(xi.w) * nt;
+    const uint32_t n = v.nbr_count[i];
+    const float rc2 = p.force_cut_sq;
+    const uint32_t* list = v.nbr + nbr_index(i, 0, v.nbr_stride);
+    for (uint32_t k = 0; k < n; ++k) {
+      const uint32_t j = list[(size_t)k * kGroup];
+      const float4 xj = v.pos[j];
+      const float dx = acc_delta(xi.x, xj.x, p.len[0], p.half[0]);
+      const float dy = acc_delta(xi.y, xj.y, p.len[1], p.half[1]);
+      const float dz = acc_delta(xi.z, xj.z, p.len[2], p.half[2]);
+      float r2 = norm2(dx, dy, dz);
+      if (!(r2 < rc2)) continue;
+      const LjCoeff c = row[__float_as_int(xj.w)];
+      if (kClamp) r2 = fmaxf(r2, 0.49f * c.sigma2);
+      const float inv_r2 = __frcp_rn(r2);
+      const float sr2 = c.sigma2 * inv_r2;
+      const float sr6 = sr2 * sr2 * sr2;
+      const float sr12 = sr6 * sr6;
+      const float fs = c.eps24 * inv_r2 * __fmaf_rn(2.0f, sr12, -sr6);
+      fx = __fmaf_rn(fs, dx, fx);
+      fy = __fmaf_rn(fs, dy, fy);
+      fz = __fmaf_rn(fs, dz, fz);
+      if (kObs) {
+        e += __fmaf_rn(c.eps4, sr12 - sr6, -c.shift);
+        w = __fmaf_rn(fs, r2, w);
+      }
+    }
+  }
+  v.force[i] = make_float4(fx, fy, fz, 0.f);
+  if (kObs) {
+    ReplicaState* st = &v.rs[r];
+    const long long ev = real ? to_fixed(0.5 * (double)e, &st->status) : 0ll;
+    const long long wv = real ? to_fixed(0.5 * (double)w, &st->status) : 0ll;
+    block_add_ll<kBlock>(ev, &st->acc[kAccPair]);
+    block_add_ll<kBlock>(wv, &st->acc[kAccVirial]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Bonded terms, gathered per particle.
+struct V3 {
+  float x, y, z;
+};
+__device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ float dot3(V3 a, V3 b) {
+  return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, __fmul_rn(a.x, b.x)));
+}
+__device__ __forceinline__ V3 cross3(V3 a, V3 b) {
+  return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ V3 axpy(float a, V3 x, V3 y) {
+  return v3(__fmaf_rn(a, x.x, y.x), __fmaf_rn(a, x.y, y.y), __fmaf_rn(a, x.z, y.z));
+}
+__device__ __forceinline__ V3 scal(float a, V3 x) { return v3(a * x.x, a * x.y, a * x.z); }
+
+__device__ __forceinline__ V3 arm(const DeviceView& v, const ReplicaParams& p,
+                                  uint32_t tag_a, uint32_t tag_b) {
+  const float4 a = v.pos[v.slot_of_tag[tag_a]];
+  const float4 b = v.pos[v.slot_of_tag[tag_b]];
+  return v3(acc_delta(a.x, b.x, p.len[0], p.half[0]),
+            acc_delta(a.y, b.y, p.len[1], p.half[1]),
+            acc_delta(a.z, b.z, p.len[2], p.half[2]));
+}
+
+// Force on member `role` of a harmonic bond; energy and virial of the whole
+// term.  U = 0.5 k (r - r0)^2.
+__device__ V3 bond_term(const DeviceView& v, const ReplicaParams& p,
+                        uint32_t idx, uint32_t role, float& energy,
+                        float& virial) {
+  const uint4 t = v.bonds[idx];
+  const BondCoeff c = v.bond_coeff[t.z];
+  const V3 d = arm(v, p, t.x, t.y);
+  const float r2 = dot3(d, d);
+  const float r = sqrtf(r2);
+  const float s = r - c.r0;
+  energy = 0.5f * c.k * s * s;
+  if (r == 0.0f) {
+    virial = 0.f;
+    return v3(0.f, 0.f, 0.f);
+  }
+  const float sc = -c.k * s / r;
+  virial = sc * r2;
+  const float sign = role == 0u ? 1.0f : -1.0f;
+  return scal(sc * sign, d);
+}
+
+// U = 0.5 k (theta - theta0)^2 with the reference's conventions: cosine
+// clamped to [-1, 1], sin(theta) floored at 1e-3, theta = 0 (energy only) on
+// a zero-length arm.
+__device__ V3 angle_term(const DeviceView& v, const ReplicaParams& p,
+                         uint32_t idx, uint32_t role, float& energy,
+                         float& virial) {
+  const uint4 t = v.angles[idx];
+  const AngleCoeff c = v.angle_coeff[t.w];
+  const V3 a1 = arm(v, p, t.x, t.y);   // i - j
+  const V3 a2 = arm(v, p, t.z, t.y);   // k - j
+  const float q1 = dot3(a1, a1);
+  const float q2 = dot3(a2, a2);
+  if (q1 == 0.0f || q2 == 0.0f) {
+    energy = 0.5f * c.k * c.theta0 * c.theta0;
+    virial = 0.f;
+    return v3(0.f, 0.f, 0.f);
+  }
+  const float r1 = sqrtf(q1);
+  const float r2 = sqrtf(q2);
+  float cs = dot3(a1, a2) / (r1 * r2);
+  cs = fminf(1.0f, fmaxf(-1.0f, cs));
+  const float theta = cs == 1.0f ? 0.0f : (cs == -1.0f ? 3.14159265358979323846f : acosf(cs));
+  const float dth = theta - c.theta0;
+  energy = 0.5f * c.k * dth * dth;
+  const float s2 = 1.0f - cs * cs;
+  const float sn = s2 <= 1.0e-6f ? 1.0e-3f : sqrtf(s2);
+  const float a = -c.k * dth / sn;
+  const float c11 = a * cs / q1;
+  const float c12 = -a / (r1 * r2);
+  const float c22 = a * cs / q2;
+  const V3 fi = axpy(c12, a2, scal(c11, a1));
+  const V3 fk = axpy(c12, a1, scal(c22, a2));
+  virial = dot3(a1, fi) + dot3(a2, fk);
+  if (role == 0u) return fi;
+  if (role == 2u) return fk;
+  return v3(-(fi.x + fk.x), -(fi.y + fk.y), -(fi.z + fk.z));
+}
+
+// U = k (1 + d cos(n phi)), signed phi; singular geometry contributes energy
+// only (k(1+d) if n == 0, else k).
+__device__ V3 dihedral_term(const DeviceView& v, const ReplicaParams& p,
+                            uint32_t idx, uint32_t role, float& energy,
+                            float& virial) {
+  const uint4 t = v.dihedrals[idx];
+  const DihedralCoeff c = v.dihedral_coeff[v.dihedral_type[idx]];
+  const V3 b0 = arm(v, p, t.x, t.y);   // i - j
+  const V3 b1 = arm(v, p, t.z, t.y);   // k - j
+  const V3 b2 = arm(v, p, t.z, t.w);   // k - l
+  const V3 m = cross3(b0, b1);
+  const V3 n = cross3(b1, b2);
+  const float q1 = dot3(b1, b1);
+  const float qm = dot3(m, m);
+  const float qn = dot3(n, n);
+  if (q1 == 0.0f || qm == 0.0f || qn == 0.0f) {
+    energy = c.n == 0 ? c.k * (1.0f + (float)c.d) : c.k;
+    virial = 0.f;
+    return v3(0.f, 0.f, 0.f);
+  }
+  float cs = dot3(m, n) * (1.0f / sqrtf(qm * qn));
+  cs = fminf(1.0f, fmaxf(-1.0f, cs));
+  float phi = cs == 1.0f ? 0.0f : (cs == -1.0f ? 3.14159265358979323846f : acosf(cs));
+  if (dot3(b0, n) < 0.0f) phi = -phi;
+  const float arg = (float)c.n * phi;
+  energy = c.k * (1.0f + (float)c.d * cosf(arg));
+  const float de = -c.k * (float)c.d * (float)c.n * sinf(arg);
+  const float l1 = sqrtf(q1);
+  const V3 fi = scal(-de * l1 / qm, m);
+  const V3 fl = scal(de * l1 / qn, n);
+  const float inv_q1 = 1.0f / q1;
+  const V3 s = v3(fi.x * (dot3(b0, b1) * inv_q1) - fl.x * (dot3(b2, b1) * inv_q1),
+                  fi.y * (dot3(b0, b1) * inv_q1) - fl.y * (dot3(b2, b1) * inv_q1),
+                  fi.z * (dot3(b0, b1) * inv_q1) - fl.z * (dot3(b2, b1) * inv_q1));
+  const V3 fj = v3(s.x - fi.x, s.y - fi.y, s.z - fi.z);
+  const V3 fk = v3(-(s.x + fl.x), -(s.y + fl.y), -(s.z + fl.z));
+  const V3 lj = v3(b1.x - b2.x, b1.y - b2.y, b1.z - b2.z);
+  virial = dot3(b0, fi) + dot3(b1, fk) + dot3(lj, fl);
+  switch (role) {
+    case 0u: return fi;
+    case 1u: return fj;
+    case 2u: return fk;
+    default: return fl;
+  }
+}
+
+template <bool kObs>
+__global__ void __launch_bounds__(kBlock) k_bonded(DeviceView v) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const ReplicaParams& p = v.rp[r];
+  const uint32_t i = b * kBlock + threadIdx.x;
+  const bool real = (i - p.atom_begin) < p.n_atoms;
+  float eb = 0.f, ea = 0.f, ed = 0.f, w = 0.f;
+  if (real) {
+    const uint32_t t = v.tag[i];
+    const uint32_t e0 = v.term_off[t];
+    const uint32_t e1 = v.term_off[t + 1];
+    if (e1 > e0) {
+      V3 f = v3(0.f, 0.f, 0.f);
+      for (uint32_t e = e0; e < e1; ++e) {
+        const uint32_t m = v.term[e];
+        const uint32_t kind = m >> 30;
+        const uint32_t role = (m >> 28) & 3u;
+        const uint32_t idx = m & 0x0fffffffu;
+        float en = 0.f, vir = 0.f;
+        V3 g;
+        if (kind == kTermBond) {
+          g = bond_term(v, p, idx, role, en, vir);
+          if (role == 0u) eb += en;
+        } else if (kind == kTermAngle) {
+          g = angle_term(v, p, idx, role, en, vir);
+          if (role == 0u) ea += en;
+        } else {
+          g = dihedral_term(v, p, idx, role, en, vir);
+          if (role == 0u) ed += en;
+        }
+        if (role == 0u) w += vir;
+        f.x += g.x;
+        f.y += g.y;
+        f.z += g.z;
+      }
+      float4 fo = v.force[i];
+      fo.x += f.x;
+      fo.y += f.y;
+      fo.z += f.z;
+      v.force[i] = fo;
+    }
+  }
+  if (kObs) {
+    ReplicaState* st = &v.rs[r];
+    block_add_ll<kBlock>(real ? to_fixed(eb, &st->status) : 0ll, &st->acc[kAccBond]);
+    block_add_ll<kBlock>(real ? to_fixed(ea, &st->status) : 0ll, &st->acc[kAccAngle]);
+    block_add_ll<kBlock>(real ? to_fixed(ed, &st->status) : 0ll, &st->acc[kAccDihedral]);
+    block_add_ll<kBlock>(real ? to_fixed(w, &st->status) : 0ll, &st->acc[kAccVirial]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// post: second half-kick, kinetic energy (FP64 per slot, fixed-point total),
+// and per replica (last block): observables, Berendsen lambda for the next
+// step (applied lazily by pre), step counter.
+template <bool kKick, bool kObs, bool kKinetic>
+__global__ void __launch_bounds__(kBlock) k_post(DeviceView v) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const ReplicaParams& p = v.rp[r];
+  ReplicaState* st = &v.rs[r];
+  const uint32_t i = b * kBlock + threadIdx.x;
+  const bool real = (i - p.atom_begin) < p.n_atoms;
+  double ke = 0.0;
+  if (real) {
+    float4 vm = v.vel[i];
+    if (kKick) {
+      const float4 f = v.force[i];
+      const float h = __fdiv_rn(__fmul_rn(0.5f, p.dt), vm.w);
+      vm.x = __fmaf_rn(h, f.x, vm.x);
+      vm.y = __fmaf_rn(h, f.y, vm.y);
+      vm.z = __fmaf_rn(h, f.z, vm.z);
+      v.vel[i] = vm;
+      if (!isfinite(vm.x + vm.y + vm.z)) atomicOr(&st->status, kStatusNonFinite);
+    }
+    if (kKinetic || kObs) {
+      const double vx = vm.x, vy = vm.y, vz = vm.z;
+      ke = 0.5 * (double)vm.w * (vx * vx + vy * vy + vz * vz);
+    }
+  }
+  if (kKinetic || kObs) {
+    block_add_ll<kBlock>(real ? to_fixed(ke, &st->status) : 0ll,
+                         &st->acc[kAccKinetic]);
+  }
+  const uint32_t n_blocks = p.n_pad / kBlock;
+  if (arrive_last(&st->done_post, n_blocks) && threadIdx.x == 0) {
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(st->acc);
+    const double kin = from_fixed((long long)atomicExch(&acc[kAccKinetic], 0ull));
+    double lam = 1.0;
+    if (kKick && p.thermostat == 1 && kin > 0.0 && p.dof > 0.0) {
+      const double current = 2.0 * kin / p.dof;
+      const double arg = 1.0 + ((double)p.dt / p.tau) * (p.kt_target / current - 1.0);
+      lam = sqrt(arg > 0.0 ? arg : 0.0);
+    }
+    if (kKick) {
+      st->lambda = lam;
+      st->step += 1ull;
+    }
+    if (kObs) {
+      ReplicaObs o;
+      o.step = st->step;
+      o.pair_pe = from_fixed((long long)atomicExch(&acc[kAccPair], 0ull));
+      o.bond_pe = from_fixed((long long)atomicExch(&acc[kAccBond], 0ull));
+      o.angle_pe = from_fixed((long long)atomicExch(&acc[kAccAngle], 0ull));
+      o.dihedral_pe = from_fixed((long long)atomicExch(&acc[kAccDihedral], 0ull));
+      o.virial = from_fixed((long long)atomicExch(&acc[kAccVirial], 0ull));
+      o.ke_pre = kin;
+      o.lambda = lam;
+      o.builds = st->builds;
+      o.dangerous = st->dangerous;
+      o.status = st->status;
+      o.pad = 0;
+      v.obs[r] = o;
+    }
+    st->done_post = 0u;
+  }
+}
+
+// Applies the pending Berendsen scale so host reads see the scaled velocities.
+__global__ void k_apply_lambda(DeviceView v) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const ReplicaParams& p = v.rp[r];
+  ReplicaState* st = &v.rs[r];
+  const uint32_t i = b * kBlock + threadIdx.x;
+  const float lam = (float)st->lambda;
+  if ((i - p.atom_begin) < p.n_atoms && lam != 1.0f) {
+    float4 u = v.vel[i];
+    u.x = __fmul_rn(u.x, lam);
+    u.y = __fmul_rn(u.y, lam);
+    u.z = __fmul_rn(u.z, lam);
+    v.vel[i] = u;
+  }
+  if (arrive_last(&st->done_pre, p.n_pad / kBlock) && threadIdx.x == 0) {
+    st->lambda = 1.0;
+    st->done_pre = 0u;
+  }
+}
+
+__global__ void k_scatter_state(DeviceView v, const float* pos_tag,
+                                const float* vel_tag, uint32_t n_tags) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_tags) return;
+  const uint32_t s = v.slot_of_tag[t];
+  if (pos_tag) {
+    float4 x = v.pos[s];
+    x.x = pos_tag[3 * (size_t)t];
+    x.y = pos_tag[3 * (size_t)t + 1];
+    x.z = pos_tag[3 * (size_t)t + 2];
+    v.pos[s] = x;
+  }
+  if (vel_tag) {
+    float4 u = v.vel[s];
+    u.x = vel_tag[3 * (size_t)t];
+    u.y = vel_tag[3 * (size_t)t + 1];
+    u.z = vel_tag[3 * (size_t)t + 2];
+    v.vel[s] = u;
+  }
+}
+
+__global__ void k_gather_state(DeviceView v, float* pos_tag, float* vel_tag,
+                               uint32_t n_tags) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_tags) return;
+  const uint32_t s = v.slot_of_tag[t];
+  if (pos_tag) {
+    const float4 x = v.pos[s];
+    pos_tag[3 * (size_t)t] = x.x;
+    pos_tag[3 * (size_t)t + 1] = x.y;
+    pos_tag[3 * (size_t)t + 2] = x.z;
+  }
+  if (vel_tag) {
+    const float4 u = v.vel[s];
+    vel_tag[3 * (size_t)t] = u.x;
+    vel_tag[3 * (size_t)t + 1] = u.y;
+    vel_tag[3 * (size_t)t + 2] = u.z;
+  }
+}
+
+void check_launch(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    throw std::runtime_error(std::string("CUDA launch of ") + what +
+                             " failed: " + cudaGetErrorString(e));
+  }
+}
+
+uint32_t cell_grid_x(uint32_t max_cells) {
+  const uint32_t warps = kBlock / 32;
+  uint32_t g = (max_cells + warps - 1) / warps;
+  if (g > 1184u) g = 1184u;  // 8 blocks per SM on 148 SMs, grid-stride beyond
+  return g < 1u ? 1u : g;
+}
+
+}  // namespace
+
+void launch_pre(const StepLaunch& l, int mode) {
+  if (mode == kPreDescent) {
+    k_pre<kPreDescent><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, l.sd_dmax, l.sd_fref);
+  } else {
+    k_pre<kPreVerlet><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, 0.f, 0.f);
+  }
+  check_launch("pre");
+}
+
+void launch_project_exclusions(const StepLaunch& l, bool force_all) {
+  if (l.excl_cap == 0) return;
+  k_project_exclusions<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, force_all ? 1 : 0);
+  check_launch("project_exclusions");
+}
+
+void launch_rebuild(const StepLaunch& l, bool force_all) {
+  if (force_all) {
+    k_force_rebuild_flags<<<(l.v.n_replicas + 127) / 128, 128, 0, l.stream>>>(l.v, 1);
+    check_launch("force_rebuild_flags");
+  }
+  k_bin<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  check_launch("bin");
+  k_scan<<<l.v.n_replicas, kScanThreads, 0, l.stream>>>(l.v);
+  check_launch("scan");
+  k_scatter<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  check_launch("scatter");
+  const dim3 cg(cell_grid_x(l.max_cells_per_replica), l.v.n_replicas);
+  k_cellsort<<<cg, kBlock, 0, l.stream>>>(l.v);
+  check_launch("cellsort");
+  k_reorder_gather<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  check_launch("reorder_gather");
+  k_reorder_commit<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  check_launch("reorder_commit");
+  if (l.excl_cap > 0) {
+    k_project_exclusions<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, 0);
+    check_launch("project_exclusions");
+  }
+  switch (l.excl_cap) {
+    case 0: k_build<0><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); break;
+    case 4: k_build<4><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); break;
+    case 8: k_build<8><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); break;
+    case 16: k_build<16><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); break;
+    case 32: k_build<32><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); break;
+    case 64: k_build<64><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); break;
+    default: throw std::runtime_error("unsupported exclusion capacity");
+  }
+  check_launch("build");
+}
+
+void launch_forces(const StepLaunch& l, bool observables, bool clamp) {
+  if (clamp) {
+    k_lj<false, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  } else if (observables) {
+    k_lj<true, false><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  } else {
+    k_lj<false, false><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  }
+  check_launch("lj");
+  if (l.v.has_bonded) {
+    if (observables) {
+      k_bonded<true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+    } else {
+      k_bonded<false><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+    }
+    check_launch("bonded");
+  }
+}
+
+void launch_post(const StepLaunch& l, bool kick, bool observables) {
+  const bool kin = l.need_kinetic != 0;
+  if (kick) {
+    if (observables) {
+      k_post<true, true, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+    } else if (kin) {
+      k_post<true, false, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+    } else {
+      k_post<true, false, false><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+    }
+  } else {
+    k_post<false, true, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  }
+  check_launch("post");
+}
+
+void launch_apply_lambda(const StepLaunch& l) {
+  k_apply_lambda<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  check_launch("apply_lambda");
+}
+
+void launch_scatter_state(const StepLaunch& l, const float* pos_tag,
+                          const float* vel_tag, uint32_t n_tags_total) {
+  k_scatter_state<<<(n_tags_total + 255) / 256, 256, 0, l.stream>>>(
+      l.v, pos_tag, vel_tag, n_tags_total);
+  check_launch("scatter_state");
+}
+
+void launch_gather_state(const StepLaunch& l, float* pos_tag, float* vel_tag,
+                         uint32_t n_tags_total) {
+  k_gather_state<<<(n_tags_total + 255) / 256, 256, 0, l.stream>>>(
+      l.v, pos_tag, vel_tag, n_tags_total);
+  check_launch("gather_state");
+}
+
+}  // namespace bb

@@ -1,0 +1,37 @@
+// kernels.cuh -- launch interface of the per-step kernels.
+#pragma once
+
+#include "device.cuh"
+
+namespace bb {
+
+// One MD step is: pre (Berendsen lambda of the previous step, half-kick,
+// drift, wrap, displacement check, rebuild decision) -> rebuild chain (each
+// kernel returns at once for replicas that do not rebuild) -> pair forces ->
+// bonded forces -> post (half-kick, kinetic energy, observables, next lambda).
+enum PreMode : int { kPreVerlet = 0, kPreDescent = 1 };
+
+struct StepLaunch {
+  DeviceView v;
+  cudaStream_t stream;
+  uint32_t max_cells_per_replica;
+  uint32_t max_atoms_per_replica;
+  int excl_cap;           // 0, 4, 8, 16, 32 or 64
+  int need_kinetic;       // a thermostat is active in some replica
+  float sd_dmax;          // descent: displacement cap
+  float sd_fref;          // descent: force floor
+};
+
+void launch_pre(const StepLaunch& l, int mode);
+void launch_rebuild(const StepLaunch& l, bool force_all);
+void launch_forces(const StepLaunch& l, bool observables, bool clamp);
+void launch_post(const StepLaunch& l, bool kick, bool observables);
+void launch_project_exclusions(const StepLaunch& l, bool force_all);
+void launch_apply_lambda(const StepLaunch& l);
+// Scatter a tag-ordered host copy (already on the device) into slots.
+void launch_scatter_state(const StepLaunch& l, const float* pos_tag,
+                          const float* vel_tag, uint32_t n_tags_total);
+void launch_gather_state(const StepLaunch& l, float* pos_tag, float* vel_tag,
+                         uint32_t n_tags_total);
+
+}  // namespace bb

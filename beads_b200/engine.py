@@ -1,0 +1,237 @@
+"""Engine contexts over the C ABI: one or many replicas in one device batch.
+
+``Engine`` is the in-process handle used by the benchmark, the tests and the
+autograd wrapper; the public drop-in surface (``System`` / ``Simulation``)
+goes through ``beads_b200._native.execute_simulation`` instead.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+
+
+@dataclass
+class ReplicaSpec:
+    """Everything one replica needs, as plain arrays and numbers.
+
+    Bonded records use 1-based tags; ``epsilon``/``sigma`` are full symmetric
+    ``n_types x n_types`` tables; ``thermostat`` is ``None`` or a
+    ``(temperature, tau)`` pair in public units.
+    """
+
+    positions: np.ndarray
+    types: np.ndarray
+    box_bound: np.ndarray
+    epsilon: np.ndarray
+    sigma: np.ndarray
+    cutoff: float
+    dt: float
+    units: str = "reduced"
+    velocities: np.ndarray | None = None
+    masses: np.ndarray | None = None
+    tags: np.ndarray | None = None
+    molecule_ids: np.ndarray | None = None
+    images: np.ndarray | None = None
+    shift: bool = False
+    bonds: np.ndarray | None = None
+    angles: np.ndarray | None = None
+    dihedrals: np.ndarray | None = None
+    bond_k: Sequence[float] | None = None
+    bond_r0: Sequence[float] | None = None
+    angle_k: Sequence[float] | None = None
+    angle_theta0: Sequence[float] | None = None
+    dihedral_k: Sequence[float] | None = None
+    dihedral_d: Sequence[int] | None = None
+    dihedral_n: Sequence[int] | None = None
+    exclusion_distance: int = 0
+    cutoff_buffer: float = 0.3
+    rebuild_check_every: int = 1
+    sort_every_rebuild: int = 10
+    max_neighbors: int = 512
+    thermostat: tuple[float, float] | None = None
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return int(np.asarray(self.positions).shape[0])
+
+
+def _descriptors(spec: ReplicaSpec, keep: _lib.Keep):
+    sd = _lib.SystemDesc()
+    n = spec.n
+    sd.n_particles = n
+    sd.units = _lib.UNITS[spec.units]
+    bb = np.asarray(spec.box_bound, dtype=np.float32).reshape(2, 3)
+    sd.box_lo[:] = [float(x) for x in bb[0]]
+    sd.box_hi[:] = [float(x) for x in bb[1]]
+    sd.positions = keep.ptr(spec.positions, np.float32, ctypes.c_float)
+    sd.velocities = keep.ptr(spec.velocities, np.float32, ctypes.c_float)
+    sd.masses = keep.ptr(spec.masses, np.float32, ctypes.c_float)
+    sd.types = keep.ptr(spec.types, np.int32, ctypes.c_int32)
+    sd.tags = keep.ptr(spec.tags, np.uint32, ctypes.c_uint32)
+    sd.molecule_ids = keep.ptr(spec.molecule_ids, np.uint32, ctypes.c_uint32)
+    sd.images = keep.ptr(spec.images, np.int32, ctypes.c_int32)
+    for name, width in (("bonds", 3), ("angles", 4), ("dihedrals", 5)):
+        rec = getattr(spec, name)
+        count = 0 if rec is None else int(np.asarray(rec).reshape(-1, width).shape[0])
+        setattr(sd, "n_" + name, count)
+        setattr(sd, name, keep.ptr(None if count == 0 else rec, np.uint32, ctypes.c_uint32))
+
+    fd = _lib.ForceFieldDesc()
+    eps = np.asarray(spec.epsilon, dtype=np.float64)
+    fd.n_types = int(round(np.sqrt(eps.size)))
+    fd.lj_epsilon = keep.ptr(eps, np.float64, ctypes.c_double)
+    fd.lj_sigma = keep.ptr(spec.sigma, np.float64, ctypes.c_double)
+    fd.lj_cutoff = float(spec.cutoff)
+    fd.lj_shift = int(bool(spec.shift))
+    fd.n_bond_types = 0 if spec.bond_k is None else len(spec.bond_k)
+    fd.bond_k = keep.ptr(spec.bond_k, np.float64, ctypes.c_double)
+    fd.bond_r0 = keep.ptr(spec.bond_r0, np.float64, ctypes.c_double)
+    fd.n_angle_types = 0 if spec.angle_k is None else len(spec.angle_k)
+    fd.angle_k = keep.ptr(spec.angle_k, np.float64, ctypes.c_double)
+    fd.angle_theta0_deg = keep.ptr(spec.angle_theta0, np.float64, ctypes.c_double)
+    fd.n_dihedral_types = 0 if spec.dihedral_k is None else len(spec.dihedral_k)
+    fd.dihedral_k = keep.ptr(spec.dihedral_k, np.float64, ctypes.c_double)
+    fd.dihedral_d = keep.ptr(spec.dihedral_d, np.int32, ctypes.c_int32)
+    fd.dihedral_n = keep.ptr(spec.dihedral_n, np.int32, ctypes.c_int32)
+    fd.exclusion_distance = int(spec.exclusion_distance)
+
+    nd = _lib.NeighborDesc()
+    nd.cutoff_buffer = float(spec.cutoff_buffer)
+    nd.rebuild_check_every = int(spec.rebuild_check_every)
+    nd.sort_every_rebuild = int(spec.sort_every_rebuild)
+    nd.max_neighbors = int(spec.max_neighbors)
+
+    dd = _lib.DynamicsDesc()
+    dd.dt = float(spec.dt)
+    if spec.thermostat is None:
+        dd.thermostat = 0
+    else:
+        dd.thermostat = 1
+        dd.temperature = float(spec.thermostat[0])
+        dd.tau = float(spec.thermostat[1])
+    return sd, fd, nd, dd
+
+
+class Engine:
+    """A device batch of replicas (one replica = one simulation)."""
+
+    def __init__(self, replicas: ReplicaSpec | Sequence[ReplicaSpec]):
+        if isinstance(replicas, ReplicaSpec):
+            replicas = [replicas]
+        self.replicas = list(replicas)
+        L = _lib.load()
+        keep = _lib.Keep()
+        n = len(self.replicas)
+        systems = (_lib.SystemDesc * n)()
+        ffs = (_lib.ForceFieldDesc * n)()
+        nbrs = (_lib.NeighborDesc * n)()
+        dyns = (_lib.DynamicsDesc * n)()
+        for r, spec in enumerate(self.replicas):
+            systems[r], ffs[r], nbrs[r], dyns[r] = _descriptors(spec, keep)
+        handle = ctypes.c_void_p()
+        _lib.check(L.beads_batch_create(n, systems, ffs, nbrs, dyns, ctypes.byref(handle)))
+        self._h = handle
+        self._lib = L
+        self.sizes = [spec.n for spec in self.replicas]
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
+        self.step = 0
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.beads_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- stepping ---------------------------------------------------------
+    def eval(self) -> list[dict]:
+        out = (_lib.Observables * len(self.replicas))()
+        _lib.check(self._lib.beads_eval(self._h, out))
+        return [o.as_dict() for o in out]
+
+    def run(self, steps: int, obs_every: int = 0) -> list[dict] | None:
+        out = (_lib.Observables * len(self.replicas))()
+        _lib.check(self._lib.beads_run(self._h, int(steps), int(obs_every), out))
+        self.step += int(steps)
+        if obs_every and steps and self.step % int(obs_every) == 0:
+            return [o.as_dict() for o in out]
+        return None
+
+    def minimize(self, iterations: int, dmax: float, fref: float) -> None:
+        _lib.check(self._lib.beads_minimize(self._h, int(iterations), float(dmax), float(fref)))
+        self.step = 0
+
+    # -- state --------------------------------------------------------------
+    def state(self, replica: int = 0) -> dict:
+        n = self.sizes[replica]
+        pos = np.zeros((n, 3), np.float32)
+        vel = np.zeros((n, 3), np.float32)
+        force = np.zeros((n, 3), np.float32)
+        img = np.zeros((n, 3), np.int32)
+        _lib.check(self._lib.beads_get_state(self._h, replica, pos.ctypes.data, vel.ctypes.data,
+                                             force.ctypes.data, img.ctypes.data))
+        return {"positions": pos, "velocities": vel, "forces": force, "images": img}
+
+    def set_state(self, replica: int, positions=None, velocities=None) -> None:
+        p = None if positions is None else np.ascontiguousarray(positions, np.float32)
+        v = None if velocities is None else np.ascontiguousarray(velocities, np.float32)
+        _lib.check(self._lib.beads_set_state(self._h, replica,
+                                             None if p is None else p.ctypes.data,
+                                             None if v is None else v.ctypes.data))
+
+    def upload_all(self, positions=None, velocities=None) -> None:
+        p = None if positions is None else np.ascontiguousarray(positions, np.float32)
+        v = None if velocities is None else np.ascontiguousarray(velocities, np.float32)
+        _lib.check(self._lib.beads_upload_all(self._h, None if p is None else p.ctypes.data,
+                                              None if v is None else v.ctypes.data))
+
+    def download_all(self, positions: np.ndarray, velocities: np.ndarray | None = None) -> None:
+        _lib.check(self._lib.beads_download_all(
+            self._h, positions.ctypes.data, None if velocities is None else velocities.ctypes.data))
+
+    def info(self) -> dict:
+        nr = ctypes.c_uint32()
+        nt = ctypes.c_uint64()
+        st = ctypes.c_void_p()
+        _lib.check(self._lib.beads_ctx_info(self._h, ctypes.byref(nr), ctypes.byref(nt),
+                                            ctypes.byref(st)))
+        return {"n_replicas": nr.value, "n_particles": nt.value, "stream": st.value or 0}
+
+    # -- parity views ----------------------------------------------------------
+    def debug_cells(self, replica: int = 0) -> np.ndarray:
+        out = np.zeros(self.sizes[replica], np.uint32)
+        _lib.check(self._lib.beads_debug_cells(self._h, replica, out.ctypes.data))
+        return out
+
+    def debug_neighbors(self, replica: int = 0, cap: int | None = None):
+        cap = cap or int(self.replicas[replica].max_neighbors)
+        n = self.sizes[replica]
+        counts = np.zeros(n, np.uint32)
+        partners = np.zeros((n, cap), np.uint32)
+        _lib.check(self._lib.beads_debug_neighbors(self._h, replica, cap, counts.ctypes.data,
+                                                   partners.ctypes.data))
+        return counts, partners
+
+    def debug_plan(self, replica: int = 0) -> dict:
+        path = ctypes.c_int32()
+        nc = np.zeros(3, np.uint32)
+        _lib.check(self._lib.beads_debug_plan(self._h, replica, ctypes.byref(path), nc.ctypes.data))
+        return {"path": ("direct", "regular_cell", "small_dimension")[path.value], "nc": nc}

@@ -1,0 +1,210 @@
+"""Seeded synthetic inputs with the shapes of the benchmark configurations.
+
+No dataset is involved anywhere: every configuration is generated here from
+fixed seeds.
+
+* ``lj_lattice``      4,096-bead single-type LJ fluid on a jittered simple-cubic
+                      lattice, reduced units (rho 0.8442, rc 2.5, skin 0.3).
+* ``lj_mixture``      binary LJ mixture in nm_kjmol units (80/20 types, mass
+                      39.95 u, rho 20.37 nm^-3), uniform random start that the
+                      caller relaxes with ``Engine.minimize``.
+* ``polymer_melt``    bead-spring chains (seeded random walks, step 0.97,
+                      rejection radius 0.8) with harmonic bonds, angles and
+                      dihedrals, reduced units, rho 0.85.
+* ``replica_batch``   many independent single-type LJ boxes of uneven size.
+
+Each function returns ``ReplicaSpec`` objects for ``beads_b200.engine.Engine``.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .engine import ReplicaSpec
+
+KB_NM_KJMOL = 0.00831446261815324
+
+
+def _gaussian_velocities(rng, n, masses, kt):
+    v = rng.standard_normal((n, 3)) * np.sqrt(kt / masses)[:, None]
+    p = (v * masses[:, None]).sum(axis=0) / masses.sum()
+    return (v - p).astype(np.float32)
+
+
+def _inside(pos, lo, hi):
+    """Wrap into [lo, hi) in float32 (guards the rounding edge x == hi)."""
+    length = hi - lo
+    pos = lo + np.mod(pos - lo, length)
+    pos = pos.astype(np.float32)
+    for a in range(3):
+        over = pos[:, a] >= np.float32(hi[a])
+        pos[over, a] = np.nextafter(np.float32(hi[a]), np.float32(lo[a]))
+        under = pos[:, a] < np.float32(lo[a])
+        pos[under, a] = np.float32(lo[a])
+    return pos
+
+
+def lj_lattice(n_side: int = 16, density: float = 0.8442, jitter: float = 0.05,
+               temperature: float = 1.0, seed_pos: int = 1, seed_vel: int = 2,
+               cutoff: float = 2.5, skin: float = 0.3, check_every: int = 10,
+               dt: float = 0.005, max_neighbors: int = 512,
+               sort_every_rebuild: int = 10) -> ReplicaSpec:
+    a = (1.0 / density) ** (1.0 / 3.0)
+    length = n_side * a
+    g = np.indices((n_side,) * 3).reshape(3, -1).T.astype(np.float64)
+    rng = np.random.default_rng(seed_pos)
+    pos = (g + 0.5) * a + rng.uniform(-jitter, jitter, size=g.shape)
+    lo = np.zeros(3)
+    hi = np.full(3, length)
+    pos = _inside(pos, lo, hi)
+    n = pos.shape[0]
+    masses = np.ones(n, np.float64)
+    vel = _gaussian_velocities(np.random.default_rng(seed_vel), n, masses, temperature)
+    return ReplicaSpec(
+        positions=pos, types=np.ones(n, np.int32),
+        box_bound=np.array([lo, hi], np.float32), epsilon=np.array([[1.0]]),
+        sigma=np.array([[1.0]]), cutoff=cutoff, dt=dt, units="reduced", velocities=vel,
+        masses=masses.astype(np.float32), shift=False, cutoff_buffer=skin,
+        rebuild_check_every=check_every, max_neighbors=max_neighbors,
+        sort_every_rebuild=sort_every_rebuild)
+
+
+MIXTURE_EPS = np.array([[1.0, 0.7], [0.7, 0.5]])
+MIXTURE_SIG = np.array([[0.34, 0.32], [0.32, 0.30]])
+
+
+def lj_mixture(n: int = 1_048_576, box: float | None = 37.2, density: float | None = None,
+               seed: int = 3, temperature: float = 120.0, tau: float = 0.1, dt: float = 0.002,
+               skin: float = 0.1, max_neighbors: int = 128, sort_every_rebuild: int = 1,
+               check_every: int = 1) -> ReplicaSpec:
+    """Binary mixture (nm_kjmol).  ``box`` wins over ``density`` when given."""
+    if box is None:
+        box = (n / density) ** (1.0 / 3.0)
+    rng = np.random.default_rng(seed)
+    lo = np.zeros(3)
+    hi = np.full(3, box)
+    pos = _inside(rng.uniform(0.0, box, size=(n, 3)), lo, hi)
+    types = np.ones(n, np.int32)
+    types[rng.permutation(n)[: int(round(0.2 * n))]] = 2
+    masses = np.full(n, 39.95)
+    vel = _gaussian_velocities(np.random.default_rng(seed + 1), n, masses,
+                               KB_NM_KJMOL * temperature)
+    return ReplicaSpec(
+        positions=pos, types=types, box_bound=np.array([lo, hi], np.float32),
+        epsilon=MIXTURE_EPS, sigma=MIXTURE_SIG, cutoff=0.9, dt=dt, units="nm_kjmol",
+        velocities=vel, masses=masses.astype(np.float32), shift=True, cutoff_buffer=skin,
+        rebuild_check_every=check_every, max_neighbors=max_neighbors,
+        sort_every_rebuild=sort_every_rebuild, thermostat=(temperature, tau))
+
+
+def polymer_melt(n_chains: int = 2000, beads: int = 200, density: float = 0.85, seed: int = 5,
+                 step: float = 0.97, reject: float = 0.8, temperature: float = 1.0,
+                 tau: float = 1.0, dt: float = 0.005, skin: float = 0.3,
+                 exclusion_distance: int = 2, dihedrals: bool = True,
+                 max_neighbors: int = 128) -> ReplicaSpec:
+    """Bead-spring melt from seeded self-avoiding random walks."""
+    n = n_chains * beads
+    length = (n / density) ** (1.0 / 3.0)
+    rng = np.random.default_rng(seed)
+    cell = reject
+    ncell = max(1, int(length // cell))
+    grid: dict[tuple[int, int, int], list[int]] = {}
+    pos = np.zeros((n, 3))
+
+    def key(p):
+        return tuple(int(c) % ncell for c in np.floor(p / (length / ncell)))
+
+    def clash(p):
+        kx, ky, kz = key(p)
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for j in grid.get(((kx + dx) % ncell, (ky + dy) % ncell, (kz + dz) % ncell), ()):
+                        d = p - pos[j]
+                        d -= length * np.round(d / length)
+                        if d @ d < reject * reject:
+                            return True
+        return False
+
+    idx = 0
+    for _ in range(n_chains):
+        while True:
+            p = rng.uniform(0.0, length, 3)
+            if not clash(p):
+                break
+        for b in range(beads):
+            if b > 0:
+                for _attempt in range(200):
+                    u = rng.standard_normal(3)
+                    u /= np.linalg.norm(u)
+                    cand = np.mod(pos[idx - 1] + step * u, length)
+                    if not clash(cand):
+                        p = cand
+                        break
+                else:
+                    p = np.mod(pos[idx - 1] + step * u, length)
+            pos[idx] = p
+            grid.setdefault(key(p), []).append(idx)
+            idx += 1
+    lo = np.zeros(3)
+    hi = np.full(3, length)
+    posf = _inside(pos, lo, hi)
+    tags = np.arange(1, n + 1, dtype=np.uint32)
+    bonds, angles, dihs = [], [], []
+    for c in range(n_chains):
+        first = c * beads + 1
+        for b in range(beads - 1):
+            bonds.append((first + b, first + b + 1, 1))
+        for b in range(beads - 2):
+            angles.append((first + b, first + b + 1, first + b + 2, 1))
+        if dihedrals:
+            for b in range(beads - 3):
+                dihs.append((first + b, first + b + 1, first + b + 2, first + b + 3, 1))
+    masses = np.ones(n)
+    vel = _gaussian_velocities(np.random.default_rng(seed + 1), n, masses, temperature)
+    mol = np.repeat(np.arange(1, n_chains + 1, dtype=np.uint32), beads)
+    return ReplicaSpec(
+        positions=posf, types=np.ones(n, np.int32), box_bound=np.array([lo, hi], np.float32),
+        epsilon=np.array([[1.0]]), sigma=np.array([[1.0]]), cutoff=2.0 ** (1.0 / 6.0), dt=dt,
+        units="reduced", velocities=vel, masses=masses.astype(np.float32), tags=tags,
+        molecule_ids=mol, shift=True, bonds=np.array(bonds, np.uint32),
+        angles=np.array(angles, np.uint32),
+        dihedrals=np.array(dihs, np.uint32) if dihedrals else None,
+        bond_k=[500.0], bond_r0=[0.97], angle_k=[5.0], angle_theta0=[150.0],
+        dihedral_k=[1.0] if dihedrals else None, dihedral_d=[1] if dihedrals else None,
+        dihedral_n=[1] if dihedrals else None, exclusion_distance=exclusion_distance,
+        cutoff_buffer=skin, max_neighbors=max_neighbors, thermostat=(temperature, tau))
+
+
+def replica_batch(n_replicas: int = 512, n_min: int = 256, n_max: int = 32768, seed: int = 7,
+                  cutoff: float = 2.5, skin: float = 0.3, dt: float = 0.005,
+                  max_neighbors: int = 160) -> list[ReplicaSpec]:
+    """Uneven single-type LJ replicas: log-uniform sizes, rho ~ U[0.7, 0.9],
+    Berendsen target T ~ U[0.8, 1.5] (tau 1), jittered lattices."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for r in range(n_replicas):
+        n_target = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+        rho = rng.uniform(0.7, 0.9)
+        t_target = rng.uniform(0.8, 1.5)
+        n = n_target
+        side = int(math.ceil(n ** (1.0 / 3.0)))
+        length = (n / rho) ** (1.0 / 3.0)
+        length = max(length, 2.0 * (cutoff + skin) + 1e-3)
+        a = length / side
+        rr = np.random.default_rng(seed * 100003 + r)
+        g = np.indices((side,) * 3).reshape(3, -1).T.astype(np.float64)
+        g = g[np.sort(rr.permutation(g.shape[0])[:n])]
+        pos = _inside((g + 0.5) * a + rr.uniform(-0.05, 0.05, g.shape), np.zeros(3),
+                      np.full(3, length))
+        masses = np.ones(n)
+        vel = _gaussian_velocities(rr, n, masses, t_target)
+        out.append(ReplicaSpec(
+            positions=pos, types=np.ones(n, np.int32),
+            box_bound=np.array([np.zeros(3), np.full(3, length)], np.float32),
+            epsilon=np.array([[1.0]]), sigma=np.array([[1.0]]), cutoff=cutoff, dt=dt,
+            units="reduced", velocities=vel, masses=masses.astype(np.float32),
+            cutoff_buffer=skin, max_neighbors=max_neighbors, thermostat=(t_target, 1.0)))
+    return out

@@ -1,0 +1,279 @@
+/*
+ * beads_b200.h -- C ABI of the B200-native BEADS molecular-dynamics engine.
+ *
+ * The reference binds its engine through one pybind11 module, `beads._native`,
+ * with two functions (native/src/bindings/module.cpp:15-55):
+ *   build_info()             -> dict of dtype names
+ *   execute_simulation(spec) -> None, results go to files
+ * This header is the plain-C boundary underneath a drop-in replacement for that
+ * module.  Every entry point takes plain pointers and sizes; no C++ or torch
+ * type crosses it.  All functions return 0 (BEADS_OK) on success or a negative
+ * status; the message of the last failure on the calling thread is available
+ * through beads_last_error().  Status codes map onto the Python exception types
+ * the reference raises (ValueError / RuntimeError / OverflowError).
+ *
+ * Terms:
+ *   replica  -- one independent periodic system (box, particles, topology).
+ *               A single simulation is a batch of one replica.
+ *   slot     -- the device storage position of a particle; slots are permuted
+ *               by the cell sort.  Every host-facing array in this header is in
+ *               TAG order (index = tag - 1) unless it says otherwise.
+ *   real     -- float (IEEE binary32): positions, velocities, masses and forces
+ *               are float, as in the reference's default single-precision build
+ *               (native/include/beads/core/types.hpp:12-20).
+ */
+#ifndef BEADS_B200_H
+#define BEADS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define BEADS_API __attribute__((visibility("default")))
+#else
+#define BEADS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define BEADS_OK 0
+#define BEADS_ERR_INVALID (-1)   /* bad argument / spec  -> ValueError       */
+#define BEADS_ERR_RUNTIME (-2)   /* runtime failure      -> RuntimeError     */
+#define BEADS_ERR_OVERFLOW (-3)  /* size / range overflow-> OverflowError    */
+#define BEADS_ERR_CUDA (-4)      /* CUDA error           -> RuntimeError     */
+#define BEADS_ERR_NEIGHBOR_OVERFLOW (-5) /* list overflow -> RuntimeError    */
+#define BEADS_ERR_NONFINITE (-6) /* non-finite force/energy -> RuntimeError  */
+#define BEADS_ERR_INTERRUPTED (-7) /* interrupt callback asked to stop       */
+
+/* ---- units (native/src/system/units/unit_system.cpp:9-12) --------------- */
+#define BEADS_UNITS_REDUCED 0
+#define BEADS_UNITS_NM_KJMOL 1
+
+/* ---- trajectory field mask (native/src/simulation/output/trajectory/
+ *      trajectory_output.cu:38-45) ---------------------------------------- */
+#define BEADS_FIELD_TAG (1u << 0)
+#define BEADS_FIELD_TYPE (1u << 1)
+#define BEADS_FIELD_POSITION (1u << 2)
+#define BEADS_FIELD_IMAGE (1u << 3)
+#define BEADS_FIELD_VELOCITY (1u << 4)
+#define BEADS_FIELD_FORCE (1u << 5)
+
+/* ---- log echo modes (native/src/simulation/output/log/log_output.cpp) --- */
+#define BEADS_ECHO_NONE 0
+#define BEADS_ECHO_SCREEN 1
+#define BEADS_ECHO_LOG 2
+#define BEADS_ECHO_BOTH 3
+
+/* One replica's particles, box and topology.  Replaces input::SystemSpec
+ * (native/src/input/native_spec.hpp:51-62).  Arrays are in the caller's
+ * order; `tags` gives each row's tag (a permutation of 1..n), NULL = 1..n. */
+typedef struct beads_system_desc {
+  uint32_t n_particles;
+  int32_t units;                 /* BEADS_UNITS_*                              */
+  float box_lo[3];
+  float box_hi[3];
+  const float* positions;        /* [n][3], inside [lo, hi)                    */
+  const float* velocities;       /* [n][3] or NULL (zero)                      */
+  const float* masses;           /* [n] or NULL (one)                          */
+  const int32_t* types;          /* [n], dense 1-based                         */
+  const uint32_t* tags;          /* [n] or NULL                                */
+  const uint32_t* molecule_ids;  /* [n] or NULL (one)                          */
+  const int32_t* images;         /* [n][3] or NULL (zero)                      */
+  uint32_t n_bonds;
+  const uint32_t* bonds;         /* [n_bonds][3]: tag_i, tag_j, type           */
+  uint32_t n_angles;
+  const uint32_t* angles;        /* [n_angles][4]: tag_i, tag_j, tag_k, type   */
+  uint32_t n_dihedrals;
+  const uint32_t* dihedrals;     /* [n][5]: tag_i..tag_l, type                 */
+} beads_system_desc;
+
+/* Force field of one replica.  Replaces input::ForceFieldSpec
+ * (native_spec.hpp:114-125) after the reference's per-style parameter readers
+ * (pair/pair_lj.cu:197-231, bond/bond_harmonic.cu, angle/angle_harmonic.cu:
+ * 236-253, dihedral/dihedral_harmonic.cu:293-320).  Tables are indexed by
+ * 0-based type id; the LJ tables are full symmetric n_types x n_types. */
+typedef struct beads_forcefield_desc {
+  int32_t n_types;
+  const double* lj_epsilon;      /* [n_types * n_types]                        */
+  const double* lj_sigma;        /* [n_types * n_types]                        */
+  double lj_cutoff;              /* one global cutoff (pair_lj.cu:201-212)     */
+  int32_t lj_shift;              /* subtract U(rc)                             */
+  int32_t n_bond_types;
+  const double* bond_k;          /* U = 0.5 k (r - r0)^2                       */
+  const double* bond_r0;
+  int32_t n_angle_types;
+  const double* angle_k;         /* U = 0.5 k (theta - theta0)^2               */
+  const double* angle_theta0_deg;
+  int32_t n_dihedral_types;
+  const double* dihedral_k;      /* U = k (1 + d cos(n phi))                   */
+  const int32_t* dihedral_d;     /* +1 or -1                                   */
+  const int32_t* dihedral_n;     /* >= 0                                       */
+  int32_t exclusion_distance;    /* 0 = none, else bond-graph distance 1..3    */
+} beads_forcefield_desc;
+
+/* Replaces input::NeighborSpec (native_spec.hpp:139-144). */
+typedef struct beads_neighbor_desc {
+  double cutoff_buffer;          /* skin                                       */
+  uint64_t rebuild_check_every;
+  uint64_t sort_every_rebuild;
+  uint32_t max_neighbors;
+} beads_neighbor_desc;
+
+/* Replaces input::DynamicsSpec (native_spec.hpp:133-137). */
+typedef struct beads_dynamics_desc {
+  double dt;
+  int32_t thermostat;            /* 0 none, 1 berendsen                        */
+  double temperature;            /* public units (K in nm_kjmol)               */
+  double tau;
+} beads_dynamics_desc;
+
+/* Observables of the most recent force evaluation of one replica, the values
+ * of one thermo row (native/src/simulation/output/thermo/thermo_output.cu:
+ * 437-470).  Totals are reduced in 64-bit fixed point on the device. */
+typedef struct beads_observables {
+  uint64_t step;
+  double pair_pe;
+  double bond_pe;
+  double angle_pe;
+  double dihedral_pe;
+  double pe;                     /* sum of the four                            */
+  double ke;                     /* after the Berendsen scaling of that step   */
+  double virial;                 /* global scalar virial  sum r.F              */
+  double temp;                   /* 2 KE / (dof kB), dof = 3N - 3              */
+  double press;                  /* s (2 KE + W) / (3 V)                       */
+  uint64_t neighbor_build_count;
+  uint64_t dangerous_rebuild_count;
+} beads_observables;
+
+typedef struct beads_ctx beads_ctx;
+
+/* Interrupt hook: called from the run loop every `every` steps (the
+ * reference polls PyErr_CheckSignals every max(1, 100000/N) steps,
+ * simulation_run.cpp:92); return non-zero to stop with
+ * BEADS_ERR_INTERRUPTED. */
+typedef int (*beads_interrupt_fn)(void* user);
+
+/* Whole-run description used by beads_execute(); replaces
+ * input::SimulationSpec (native_spec.hpp:169-176) together with its
+ * OutputSpec (native_spec.hpp:146-167). */
+typedef struct beads_run_desc {
+  const beads_system_desc* system;
+  const beads_forcefield_desc* forcefield;
+  const beads_neighbor_desc* neighbor;
+  const beads_dynamics_desc* dynamics;
+  uint64_t runsteps;
+  uint64_t thermo_every;         /* 0 = no thermo output                       */
+  const char* thermo_prefix;
+  uint64_t trajectory_every;     /* 0 = no trajectory output                   */
+  const char* trajectory_prefix;
+  uint32_t trajectory_fields;    /* BEADS_FIELD_* mask, tag always set         */
+  const char* final_state_prefix;/* NULL = no final state                      */
+  int32_t log_echo;              /* BEADS_ECHO_*                               */
+  const char* log_prefix;        /* required for LOG / BOTH                    */
+  const char* thermostat_name;   /* "none" or "berendsen" (log only)           */
+  const char* exclusion_policy;  /* "none" / "default" / "explicit" (log only) */
+  beads_interrupt_fn interrupt;  /* may be NULL                                */
+  void* interrupt_user;
+} beads_run_desc;
+
+/* ---- build information ---------------------------------------------------
+ * Replaces _native.build_info() (native/src/bindings/module.cpp:15-27).
+ * Writes a JSON object with the keys real_precision, real_dtype, type_dtype,
+ * index_dtype, image_dtype, runstep_dtype into buf (NUL-terminated). */
+BEADS_API int beads_build_info(char* buf, size_t buf_size);
+
+/* Message of the last failure on this thread (NUL-terminated, truncated). */
+BEADS_API int beads_last_error(char* buf, size_t buf_size);
+
+/* ---- whole simulation with file outputs ----------------------------------
+ * Replaces _native.execute_simulation(spec) (module.cpp:36-44 ->
+ * SimulationRun(spec).execute(), simulation_run.cpp:237-244): validates,
+ * runs `runsteps` velocity-Verlet steps (or a zero-step evaluation), and
+ * writes the thermo CSV, binary trajectory, final-state snapshot and log in
+ * the reference's formats. */
+BEADS_API int beads_execute(const beads_run_desc* run);
+
+/* ---- engine contexts ------------------------------------------------------
+ * A context owns the device state of n_replicas independent replicas packed
+ * into one set of arrays; every kernel runs over all replicas at once.
+ * beads_ctx_create is the one-replica case of beads_batch_create.  Replaces the
+ * construction in SimulationRun::SimulationRun (simulation_run.cpp:60-98). */
+BEADS_API int beads_ctx_create(const beads_system_desc* system,
+                     const beads_forcefield_desc* forcefield,
+                     const beads_neighbor_desc* neighbor,
+                     const beads_dynamics_desc* dynamics,
+                     beads_ctx** out);
+BEADS_API int beads_batch_create(uint32_t n_replicas,
+                       const beads_system_desc* systems,
+                       const beads_forcefield_desc* forcefields,
+                       const beads_neighbor_desc* neighbors,
+                       const beads_dynamics_desc* dynamics,
+                       beads_ctx** out);
+BEADS_API void beads_ctx_destroy(beads_ctx* ctx);
+
+/* Neighbour build + force/energy/virial evaluation at the current positions
+ * (the reference's initialize_force_state, simulation_run.cpp:113-119, and
+ * its zero-step run, :158-172).  Fills one beads_observables per replica. */
+BEADS_API int beads_eval(beads_ctx* ctx, beads_observables* out);
+
+/* Advance every replica by `steps` velocity-Verlet steps (the reference's
+ * advance_dynamics_step loop, simulation_run.cpp:189-235).  If
+ * obs_every > 0, observables are evaluated on steps that are multiples of
+ * obs_every; `out` (may be NULL) receives the observables of the last step if
+ * it was such a step.  The step loop between output steps is replayed as a
+ * CUDA graph; neighbour rebuilds are decided on the device. */
+BEADS_API int beads_run(beads_ctx* ctx, uint64_t steps, uint64_t obs_every,
+              beads_observables* out);
+
+/* Copy the state of one replica to host arrays in TAG order.  Any pointer may
+ * be NULL.  forces are those of the last evaluation. */
+BEADS_API int beads_get_state(beads_ctx* ctx, uint32_t replica, float* positions,
+                    float* velocities, float* forces, int32_t* images);
+/* Overwrite positions/velocities (TAG order, may be NULL) of one replica;
+ * positions must be inside the box.  The next step rebuilds the list. */
+BEADS_API int beads_set_state(beads_ctx* ctx, uint32_t replica, const float* positions,
+                    const float* velocities);
+
+/* Whole-batch host transfers in TAG order, replica after replica (replica r's
+ * block starts at the sum of the previous replicas' particle counts).  These
+ * are one H2D / D2H copy each plus a device scatter/gather, used by callers
+ * that stream the state every call.  Any pointer may be NULL. */
+BEADS_API int beads_upload_all(beads_ctx* ctx, const float* positions,
+                     const float* velocities);
+BEADS_API int beads_download_all(beads_ctx* ctx, float* positions, float* velocities);
+
+/* Device-resident views for in-process callers (the autograd wrapper, the
+ * benchmark): number of replicas / particles, and the CUDA stream the engine
+ * launches on. */
+BEADS_API int beads_ctx_info(beads_ctx* ctx, uint32_t* n_replicas,
+                   uint64_t* n_particles_total, void** stream);
+
+/* Steepest descent with a per-particle displacement cap, used to relax
+ * random initial configurations: x += dmax * F / max(|F|, fref), with the LJ
+ * force evaluated on r^2 clamped to >= (0.7 sigma)^2 so overlaps stay finite.
+ * Not a reference feature (the reference has no minimiser). */
+BEADS_API int beads_minimize(beads_ctx* ctx, uint32_t iterations, float dmax,
+                   float fref);
+
+/* ---- parity / debugging views (TAG order) --------------------------------
+ * Cell id of every particle from the last neighbour build (the reference's
+ * particle_cell, cell_list_build.cu:135-166). */
+BEADS_API int beads_debug_cells(beads_ctx* ctx, uint32_t replica, uint32_t* cell_by_tag);
+/* Full neighbour list of the last build: counts[tag-1] and the partner tags
+ * in partners[(tag-1) * cap + k].  Replaces the reference's NeighborList
+ * storage (neighbor_list.cuh:12-71) as a host view. */
+BEADS_API int beads_debug_neighbors(beads_ctx* ctx, uint32_t replica, uint32_t cap,
+                          uint32_t* counts, uint32_t* partners);
+/* Neighbour-build path of a replica: 0 direct, 1 regular_cell,
+ * 2 small_dimension (neighbor_plan.cpp:107-128) and its cell grid. */
+BEADS_API int beads_debug_plan(beads_ctx* ctx, uint32_t replica, int32_t* path,
+                     uint32_t* ncells3);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEADS_B200_H */
