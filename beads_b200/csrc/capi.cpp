@@ -355,6 +355,20 @@ int beads_minimize(beads_ctx* ctx, uint32_t iterations, float dmax, float fref) 
   });
 }
 
+int beads_profile(beads_ctx* ctx, int32_t stage, uint32_t reps, double* avg_ms) {
+  return guarded([&] {
+    require(ctx && ctx->engine && avg_ms, "NULL argument.");
+    *avg_ms = ctx->engine->profile(stage, reps);
+  });
+}
+
+int beads_list_stats(beads_ctx* ctx, uint64_t* total_entries, uint32_t* max_count) {
+  return guarded([&] {
+    require(ctx && ctx->engine, "NULL context.");
+    ctx->engine->list_stats(total_entries, max_count);
+  });
+}
+
 int beads_debug_cells(beads_ctx* ctx, uint32_t replica, uint32_t* cell_by_tag) {
   return guarded([&] {
     require(ctx && ctx->engine && cell_by_tag, "NULL argument.");

@@ -562,6 +562,56 @@ void Engine::minimize(uint32_t iterations, float dmax, float fref) {
 
 void Engine::flush_lambda() { launch_apply_lambda(launch_); }
 
+double Engine::profile(int stage, uint32_t reps) {
+  if (!initialized_) eval();
+  if (reps == 0) reps = 1;
+  cudaEvent_t start = nullptr, stop = nullptr;
+  cuda_check(cudaEventCreate(&start), "event create");
+  cuda_check(cudaEventCreate(&stop), "event create");
+  float ms = 0.f;
+  try {
+    sync();
+    cuda_check(cudaEventRecord(start, stream_), "event record");
+    for (uint32_t k = 0; k < reps; ++k) {
+      if (stage == 0) {
+        launch_forces(launch_, false, false);
+      } else if (stage == 1) {
+        launch_chunk(1, false);
+        step_ += 1;
+      } else if (stage == 2) {
+        launch_rebuild(launch_, true);
+      } else {
+        throw InvalidArgument("unknown profile stage");
+      }
+    }
+    cuda_check(cudaEventRecord(stop, stream_), "event record");
+    cuda_check(cudaEventSynchronize(stop), "event sync");
+    cuda_check(cudaEventElapsedTime(&ms, start, stop), "event elapsed");
+  } catch (...) {
+    cudaEventDestroy(start);
+    cudaEventDestroy(stop);
+    throw;
+  }
+  cudaEventDestroy(start);
+  cudaEventDestroy(stop);
+  check_status();
+  return static_cast<double>(ms) / reps;
+}
+
+void Engine::list_stats(uint64_t* total, uint32_t* max_count) {
+  sync();
+  std::vector<uint32_t> cnt(v_.n_slots);
+  cuda_check(cudaMemcpy(cnt.data(), v_.nbr_count, cnt.size() * 4ull, cudaMemcpyDeviceToHost), "d2h");
+  uint64_t t = 0;
+  uint32_t m = 0;
+  for (uint32_t c : cnt) {
+    t += c;
+    m = std::max(m, c);
+  }
+  if (total) *total = t;
+  if (max_count) *max_count = m;
+}
+
 void Engine::observables(std::vector<beads_observables>& out) {
   sync();
   cuda_check(cudaMemcpy(h_obs_, v_.obs, rep_.size() * sizeof(ReplicaObs), cudaMemcpyDeviceToHost),

@@ -83,6 +83,8 @@ class Engine {
   bool initialized() const { return initialized_; }
   // Applies a pending Berendsen scale to the velocities (state reads).
   void flush_lambda();
+  double profile(int stage, uint32_t reps);
+  void list_stats(uint64_t* total, uint32_t* max_count);
   void check_status();
 
  private:

@@ -215,6 +215,21 @@ class Engine:
                                             ctypes.byref(st)))
         return {"n_replicas": nr.value, "n_particles": nt.value, "stream": st.value or 0}
 
+    def profile(self, stage: str, reps: int) -> float:
+        """Mean milliseconds per launch of 'forces', 'step' or 'rebuild'."""
+        code = {"forces": 0, "step": 1, "rebuild": 2}[stage]
+        out = ctypes.c_double()
+        _lib.check(self._lib.beads_profile(self._h, code, int(reps), ctypes.byref(out)))
+        if code == 1:
+            self.step += int(reps)
+        return out.value
+
+    def list_stats(self) -> dict:
+        total = ctypes.c_uint64()
+        mx = ctypes.c_uint32()
+        _lib.check(self._lib.beads_list_stats(self._h, ctypes.byref(total), ctypes.byref(mx)))
+        return {"entries": total.value, "max": mx.value}
+
     # -- parity views ----------------------------------------------------------
     def debug_cells(self, replica: int = 0) -> np.ndarray:
         out = np.zeros(self.sizes[replica], np.uint32)

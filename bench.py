@@ -1,0 +1,422 @@
+"""Benchmark: atom-steps/s of the BEADS per-step MD hot path on B200.
+
+Workload (one replica per GPU, "replicas only" scaling): the 1,048,576-bead
+binary LJ mixture in nm_kjmol units (80/20 types, mass 39.95 u, cubic box
+37.2 nm, eps 1.0/0.5/0.7, sigma 0.34/0.30/0.32, rc 0.9 shifted, skin 0.1,
+max_neighbors 128, Berendsen 120 K / tau 0.1, dt 0.002), seeded uniform start
+relaxed by 500 capped steepest-descent steps.  Synthetic data; no dataset.
+
+One bench "step" is one velocity-Verlet MD step of the whole system (pre
+half-kick/drift/wrap/rebuild decision, device-decided neighbour rebuild,
+LJ forces, post half-kick + Berendsen).  The neighbour list (~360 MB) and the
+particle state (~100 MB) exceed the 126 MB L2, so consecutive steps cannot
+serve each other from L2.
+
+Arms:
+  default            the CUDA engine through its C ABI.
+  --impl reference   the reference's algorithm on the host cores (the CPU
+                     oracle port: the reference has no CPU implementation of
+                     this path), bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "atom-steps/s on 1 B200 (1M-bead binary LJ mixture, FP32 pair math, fixed-point totals)"
+UNIT = "atom-steps/s"
+N_BEADS = 1_048_576
+E2E_STEPS = 100  # MD steps per end-to-end call
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_from_profile():
+    """DRAM bytes per launch of the force kernel from the committed ncu summary
+    (profiles/lj_force_mixture_1m.txt), or None."""
+    path = ROOT / "profiles" / "lj_force_mixture_1m.txt"
+    if not path.exists():
+        return None
+    m = re.search(r"dram_bytes_per_launch_full:\s*([0-9.eE+]+)", path.read_text())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows: list[list[str]] = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def _prepare_engine(local_rank: int, n_beads: int = N_BEADS):
+    from beads_b200 import workloads
+    from beads_b200.engine import Engine
+
+    box = 37.2 * (n_beads / N_BEADS) ** (1 / 3)
+    spec = workloads.lj_mixture(n=n_beads, box=box, seed=3 + local_rank)
+    # The uniform start has Poisson density fluctuations that overflow the
+    # production list capacity (128); relax with a roomier list first.
+    capacity = spec.max_neighbors
+    spec.max_neighbors = 256
+    with Engine(spec) as relax:
+        relax.minimize(500, 0.004, 200.0)
+        # A wrapped float coordinate can round to the upper bound itself;
+        # nudge those onto the last float inside [lo, hi) for the new engine.
+        spec.positions = workloads._inside(relax.state()["positions"].astype(np.float64),
+                                           np.zeros(3), np.full(3, box))
+    spec.max_neighbors = capacity
+    eng = Engine(spec)
+    eng.run(200)  # settle the list / sort order before timing
+    return spec, eng
+
+
+def _cpu_sim(spec, positions, n_sample: int):
+    """CPU oracle state for a bounded sample: the first n_sample beads of a
+    cubic sub-box at the workload's density and composition."""
+    from oracle import oracle as O
+
+    ff = O.ForceField(epsilon=spec.epsilon.ravel(), sigma=spec.sigma.ravel(), cutoff=spec.cutoff,
+                      shift=spec.shift)
+    n_all = spec.n
+    if n_sample >= n_all:
+        pos = np.asarray(positions, np.float32)
+        box = spec.box_bound
+        sel = np.arange(n_all)
+    else:
+        side = float(spec.box_bound[1][0] - spec.box_bound[0][0]) * (n_sample / n_all) ** (1 / 3)
+        sel = np.nonzero(np.all(np.asarray(positions) < side, axis=1))[0]
+        pos = np.asarray(positions, np.float32)[sel]
+        box = np.array([[0, 0, 0], [side] * 3], np.float32)
+    sim = O.Sim(pos, np.asarray(spec.velocities, np.float64)[sel], np.asarray(spec.masses)[sel],
+                np.asarray(spec.types)[sel], box, ff, dt=spec.dt, skin=spec.cutoff_buffer,
+                check_every=spec.rebuild_check_every, thermostat=True,
+                kt_target=0.00831446261815324 * spec.thermostat[0], tau=spec.thermostat[1])
+    return sim, len(sel)
+
+
+def _cpu_rate(sim, n, steps: int) -> tuple[float, float]:
+    t0 = time.perf_counter()
+    sim.step(steps)
+    wall = time.perf_counter() - t0
+    return n * steps / wall, wall
+
+
+def _cpu_baseline(positions, spec, budget_s: float):
+    """Times the CPU oracle port (OpenMP, FP64) on the full system for a
+    bounded number of MD steps (about budget_s of host work)."""
+    from oracle import oracle as O
+
+    sim, n = _cpu_sim(spec, positions, spec.n)
+    rate, wall = _cpu_rate(sim, n, 1)
+    steps = max(1, int(budget_s / max(wall, 1e-3)))
+    rate, wall = _cpu_rate(sim, n, steps)
+    sim.close()
+    return {"value": rate, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+            "sample": f"{steps} MD steps of the full {n}-bead system (after one untimed step), "
+                      f"{wall:.1f} s of host work, FP64 oracle with OpenMP"}
+
+
+def _lattice_mixture(n_side: int):
+    """The workload's mixture (same density, composition, parameters) on a
+    jittered n_side^3 simple-cubic lattice: no overlaps, so the CPU arm needs
+    no relaxation (its cost is set by pair counts, not by overlaps)."""
+    from beads_b200 import workloads
+
+    n = n_side ** 3
+    box = (n / (N_BEADS / 37.2 ** 3)) ** (1 / 3)
+    spec = workloads.lj_mixture(n=n, box=box, seed=3)
+    a = box / n_side
+    g = np.indices((n_side,) * 3).reshape(3, -1).T.astype(np.float64)
+    rng = np.random.default_rng(3)
+    pos = (((g + 0.5) * a + rng.uniform(-0.02, 0.02, g.shape)) % box).astype(np.float32)
+    spec.positions = pos
+    return spec
+
+
+def run_reference(args) -> None:
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    # Each bench step is one MD step (with the reference's rebuild policy) of
+    # a lattice-started copy of the workload, sized so warm-up + steps take
+    # about args.ref_budget seconds of host work.
+    probe_spec = _lattice_mixture(40)
+    probe, n_probe = _cpu_sim(probe_spec, probe_spec.positions, probe_spec.n)
+    probe.step(1)
+    rate, _ = _cpu_rate(probe, n_probe, 2)
+    probe.close()
+    per_step = args.ref_budget / (args.steps + args.warmup)
+    n_target = min(N_BEADS, max(8192, rate * per_step))
+    spec = _lattice_mixture(max(20, int(round(n_target ** (1 / 3)))))
+    sim, n = _cpu_sim(spec, spec.positions, spec.n)
+    for _ in range(args.warmup):
+        sim.step(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.step(1)
+    total = time.perf_counter() - t0
+    sim.close()
+    value = n * args.steps / total
+    cores = O.num_threads()
+    sample = (f"{n}-bead copy of the mixture (same density and parameters, jittered-lattice "
+              f"start), one MD step per bench step")
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "binary LJ mixture, 1,048,576 beads, nm_kjmol, rc 0.9, skin 0.1, "
+                               "Berendsen 120 K", "sampled_beads": n},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args) -> None:
+    import torch
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from beads_b200.engine import Engine  # noqa: F401
+
+    spec, eng = _prepare_engine(local, args.beads)
+    stream = torch.cuda.ExternalStream(eng.info()["stream"], device=torch.device("cuda", local))
+
+    # L2 flush buffer (not needed: the working set is > L2, kept for hygiene of
+    # the kernel-level timing below).
+    for _ in range(max(3, args.warmup)):
+        eng.run(1)
+    stats = eng.list_stats()
+    mean_nbr = stats["entries"] / spec.n
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    eng.run(args.steps)
+    stop.record(stream)
+    stop.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    elapsed_ms = start.elapsed_time(stop)
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    value = world * spec.n * args.steps / (elapsed_ms / 1e3)
+
+    # Dominant kernel: LJ pair forces, timed alone on the engine stream.
+    force_ms = eng.profile("forces", 50)
+    step_ms_alone = elapsed_ms / args.steps
+    bytes_per_atom = 4.0 * mean_nbr + 36.0  # list + own pos + count + force write
+    achieved = spec.n * bytes_per_atom / (force_ms / 1e3) / 1e9
+    peak, peak_kind = _peaks()
+    traffic = _traffic_from_profile()
+
+    # End-to-end through the C ABI with host buffers: upload positions and
+    # velocities, run E2E_STEPS steps (the call rebuilds the list and forces
+    # first, as a fresh run does), download both.
+    e2e_value = None
+    if args.no_e2e:
+        e2e_calls = 0
+    pin_pos = torch.empty((spec.n, 3), dtype=torch.float32, pin_memory=True)
+    pin_vel = torch.empty((spec.n, 3), dtype=torch.float32, pin_memory=True)
+    eng.download_all(pin_pos.numpy(), pin_vel.numpy())
+    if not args.no_e2e:
+        e2e_calls = max(2, args.steps // (4 * E2E_STEPS))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_calls):
+        eng.upload_all(pin_pos.numpy(), pin_vel.numpy())
+        eng.run(E2E_STEPS)
+        eng.download_all(pin_pos.numpy(), pin_vel.numpy())
+    barrier()
+    e2e_wall = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_wall], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_wall = float(t.item())
+    if e2e_calls:
+        e2e_value = world * spec.n * E2E_STEPS * e2e_calls / e2e_wall
+    h2d = 2 * spec.n * 3 * 4
+    d2h = 2 * spec.n * 3 * 4
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        st = eng.state()
+        cpu = _cpu_baseline(st["positions"], spec, args.cpu_budget)
+
+    launches_per_step = 10  # pre, 7 rebuild-chain kernels, forces, post
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": step_ms_alone,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": "binary LJ mixture, 1,048,576 beads per GPU, nm_kjmol, rc 0.9 (shifted), "
+                        "skin 0.1, max_neighbors 128, Berendsen 120 K tau 0.1, dt 0.002",
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (list ~4*mean_nbr*N bytes + state)",
+            "mean_neighbors": round(mean_nbr, 2),
+            "max_neighbors_seen": stats["max"],
+        },
+        "roofline": {
+            "bound": "hbm",
+            "kernel": "k_lj (pair forces)",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": traffic,
+            "peak_kind": peak_kind,
+            "bytes_per_atom": bytes_per_atom,
+            "kernel_ms": force_ms,
+        },
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "md_steps_per_call": E2E_STEPS},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clocks,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line))
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser(description=__doc__)
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=2000)
+    parser.add_argument("--warmup", type=int, default=20)
+    parser.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    parser.add_argument("--cpu-budget", type=float, default=15.0,
+                        help="seconds of host work for the cpu_baseline sample")
+    parser.add_argument("--ref-budget", type=float, default=90.0,
+                        help="seconds of host work for the whole reference arm")
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    parser.add_argument("--beads", type=int, default=N_BEADS,
+                        help="system size (same density); profiling of small cases only")
+    args = parser.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

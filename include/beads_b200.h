@@ -251,6 +251,18 @@ BEADS_API int beads_download_all(beads_ctx* ctx, float* positions, float* veloci
 BEADS_API int beads_ctx_info(beads_ctx* ctx, uint32_t* n_replicas,
                    uint64_t* n_particles_total, void** stream);
 
+/* Times `reps` back-to-back launches of one stage on the engine's stream
+ * with CUDA events (synchronized on both sides) and returns the mean duration
+ * per launch in milliseconds.  stage 0: pair + bonded forces on the current
+ * list (no observables); 1: one full MD step; 2: one forced neighbour
+ * rebuild.  Stages 1 and 2 advance or rebuild the state they time. */
+BEADS_API int beads_profile(beads_ctx* ctx, int32_t stage, uint32_t reps,
+                            double* avg_ms);
+/* Neighbour-list statistics of the last build over all replicas: total list
+ * entries and the largest per-particle count. */
+BEADS_API int beads_list_stats(beads_ctx* ctx, uint64_t* total_entries,
+                               uint32_t* max_count);
+
 /* Steepest descent with a per-particle displacement cap, used to relax
  * random initial configurations: x += dmax * F / max(|F|, fref), with the LJ
  * force evaluated on r^2 clamped to >= (0.7 sigma)^2 so overlaps stay finite.

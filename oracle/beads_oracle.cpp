@@ -484,56 +484,48 @@ int orc_forces(uint32_t n, const float* pos, const int32_t* types, const float l
   return 0;
 }
 
-// Velocity-Verlet + Berendsen trajectory in double, with the reference's
-// rebuild policy driving a float-rule neighbour list (positions are rounded
-// to float for list building and force evaluation so that the pair sets
-// follow the engine's rules).  pos/vel are updated in place (double, [n][3]);
-// thermo[k] rows (every obs_every steps, incl. step 0): step, pe_pair,
-// pe_bond, pe_angle, pe_dihedral, ke, virial.  Returns the number of rows.
-int64_t orc_md(uint32_t n, double* pos, double* vel, const double* mass, int32_t* img,
-               const int32_t* types, const float lo[3], const float hi[3], int ntypes,
-               const double* eps, const double* sig, double rc, int shift, double skin,
-               uint64_t check_every, int excl_distance, uint32_t nb, const uint32_t* bonds,
-               const double* bond_k, const double* bond_r0, uint32_t na, const uint32_t* angles,
-               const double* angle_k, const double* angle_theta0_deg, uint32_t nd,
-               const uint32_t* dihedrals, const double* dihedral_k, const int32_t* dihedral_d,
-               const int32_t* dihedral_n, double dt, int thermostat, double kt_target,
-               double tau, uint64_t steps, uint64_t obs_every, double* thermo,
-               uint64_t* builds_out) {
-  Plan p;
-  if (make_plan(lo, hi, rc, skin, &p) != 0) return -1;
-  const Box b = make_box(lo, hi);
-  FF ff{ntypes, eps, sig, rc, shift, nb, bonds, bond_k, bond_r0, na, angles, angle_k,
-        angle_theta0_deg, nd, dihedrals, dihedral_k, dihedral_d, dihedral_n};
+// Velocity-Verlet + Berendsen state in double, advanced step by step with the
+// reference's step order and rebuild policy (simulation_run.cpp:212-235,
+// neighbor_system.cpp:79-105).  The neighbour list is built from the state
+// rounded to float so that pair sets follow the engine's float rules; forces,
+// energies and the integration are double.
+struct OracleSim {
+  uint32_t n = 0;
+  std::vector<double> pos, vel, mass, f, ref;
+  std::vector<int32_t> img, ref_img, types;
+  std::vector<float> fpos;
+  std::vector<uint32_t> bonds_v, angles_v, dihedrals_v;
+  std::vector<double> eps_v, sig_v, bk, br0, ak, at0, dk;
+  std::vector<int32_t> dd, dn;
+  Plan plan{};
+  Box box{};
+  FF ff{};
   std::vector<uint32_t> ex_off, ex_idx;
-  if (excl_distance > 0 && nb > 0) exclusion_csr(n, ff, excl_distance, &ex_off, &ex_idx);
-  std::vector<float> fpos(3 * n);
-  std::vector<double> f(3 * n, 0.0), ref(3 * n);
-  std::vector<int32_t> ref_img(3 * n);
   std::vector<std::vector<uint32_t>> nbr;
-  uint64_t builds = 0;
-  int64_t rows = 0;
-  const double dof = std::max(0.0, 3.0 * n - 3.0);
-  const double thr = 0.25 * static_cast<double>(static_cast<float>(skin)) *
-                     static_cast<double>(static_cast<float>(skin));
-  auto to_float = [&]() {
+  double dt = 0, skin = 0, kt = 0, tau = 1, dof = 0, thr = 0;
+  int thermostat = 0;
+  uint64_t check_every = 1, builds = 0, step = 0;
+  Out last;
+
+  void to_float() {
     for (uint64_t k = 0; k < 3ull * n; ++k) fpos[k] = static_cast<float>(pos[k]);
-  };
-  auto rebuild = [&]() {
+  }
+  void rebuild() {
     to_float();
-    neighbors_f(n, fpos.data(), b, p, ex_off.empty() ? nullptr : ex_off.data(),
+    neighbors_f(n, fpos.data(), box, plan, ex_off.empty() ? nullptr : ex_off.data(),
                 ex_idx.empty() ? nullptr : ex_idx.data(), &nbr);
-    std::memcpy(ref.data(), pos, sizeof(double) * 3 * n);
-    std::memcpy(ref_img.data(), img, sizeof(int32_t) * 3 * n);
+    ref = pos;
+    ref_img = img;
     ++builds;
-  };
-  auto forces = [&](Out* out) {
+  }
+  void forces() {
     to_float();
     std::fill(f.begin(), f.end(), 0.0);
-    pair_forces(n, fpos.data(), types, b, ff, nbr, f.data(), out);
-    bonded_forces(fpos.data(), b, ff, f.data(), out);
-  };
-  auto kinetic = [&]() {
+    last = Out();
+    pair_forces(n, fpos.data(), types.data(), box, ff, nbr, f.data(), &last);
+    bonded_forces(fpos.data(), box, ff, f.data(), &last);
+  }
+  double kinetic() const {
     double ke = 0;
 #pragma omp parallel for reduction(+ : ke)
     for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
@@ -541,23 +533,9 @@ int64_t orc_md(uint32_t n, double* pos, double* vel, const double* mass, int32_t
                              vel[3 * i + 2] * vel[3 * i + 2]);
     }
     return ke;
-  };
-  auto record = [&](uint64_t step, const Out& o) {
-    double* row = thermo + 7 * rows;
-    row[0] = static_cast<double>(step);
-    row[1] = o.pair;
-    row[2] = o.bond;
-    row[3] = o.angle;
-    row[4] = o.dihedral;
-    row[5] = kinetic();
-    row[6] = o.virial;
-    ++rows;
-  };
-  rebuild();
-  Out o0;
-  forces(&o0);
-  if (obs_every > 0 && thermo) record(0, o0);
-  for (uint64_t s = 1; s <= steps; ++s) {
+  }
+  void advance() {
+    ++step;
 #pragma omp parallel for
     for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
       const double h = 0.5 * dt / mass[i];
@@ -566,26 +544,28 @@ int64_t orc_md(uint32_t n, double* pos, double* vel, const double* mass, int32_t
         double& x = pos[3 * i + a];
         v += h * f[3 * i + a];
         x += dt * v;
-        const double c = std::floor((x - b.lo[a]) / b.len[a]);
-        x -= c * b.len[a];
+        const double c = std::floor((x - box.lo[a]) / box.len[a]);
+        x -= c * box.len[a];
         img[3 * i + a] += static_cast<int32_t>(c);
       }
     }
     bool need = skin == 0.0;
-    if (!need && s % check_every == 0) {
-      for (uint32_t i = 0; i < n && !need; ++i) {
+    if (!need && step % check_every == 0) {
+      int exceeded = 0;
+#pragma omp parallel for reduction(| : exceeded)
+      for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
         double d2 = 0;
         for (int a = 0; a < 3; ++a) {
           const double d = pos[3 * i + a] - ref[3 * i + a] +
-                           static_cast<double>(img[3 * i + a] - ref_img[3 * i + a]) * b.len[a];
+                           static_cast<double>(img[3 * i + a] - ref_img[3 * i + a]) * box.len[a];
           d2 += d * d;
         }
-        need = d2 > thr;
+        exceeded |= d2 > thr ? 1 : 0;
       }
+      need = exceeded != 0;
     }
     if (need) rebuild();
-    Out o;
-    forces(&o);
+    forces();
 #pragma omp parallel for
     for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
       const double h = 0.5 * dt / mass[i];
@@ -595,15 +575,107 @@ int64_t orc_md(uint32_t n, double* pos, double* vel, const double* mass, int32_t
       const double ke = kinetic();
       double lam = 1.0;
       if (ke > 0.0 && dof > 0.0) {
-        const double arg = 1.0 + dt / tau * (kt_target / (2.0 * ke / dof) - 1.0);
+        const double arg = 1.0 + dt / tau * (kt / (2.0 * ke / dof) - 1.0);
         lam = std::sqrt(std::max(0.0, arg));
       }
       for (uint64_t k = 0; k < 3ull * n; ++k) vel[k] *= lam;
     }
-    if (obs_every > 0 && thermo && s % obs_every == 0) record(s, o);
   }
-  if (builds_out) *builds_out = builds;
-  return rows;
+};
+
+}  // extern "C"
+
+template <typename T>
+static std::vector<T> copy_of(const T* p, size_t count) {
+  return p ? std::vector<T>(p, p + count) : std::vector<T>();
+}
+
+extern "C" {
+
+// Creates a simulation state (initial list + forces computed).
+void* orc_sim_create(uint32_t n, const double* pos, const double* vel, const double* mass,
+                     const int32_t* img, const int32_t* types, const float lo[3],
+                     const float hi[3], int ntypes, const double* eps, const double* sig,
+                     double rc, int shift, double skin, uint64_t check_every, int excl_distance,
+                     uint32_t nb, const uint32_t* bonds, const double* bond_k,
+                     const double* bond_r0, uint32_t na, const uint32_t* angles,
+                     const double* angle_k, const double* angle_theta0_deg, uint32_t nd,
+                     const uint32_t* dihedrals, const double* dihedral_k,
+                     const int32_t* dihedral_d, const int32_t* dihedral_n, double dt,
+                     int thermostat, double kt_target, double tau) {
+  auto* s = new OracleSim;
+  if (make_plan(lo, hi, rc, skin, &s->plan) != 0) {
+    delete s;
+    return nullptr;
+  }
+  s->n = n;
+  s->box = make_box(lo, hi);
+  s->pos.assign(pos, pos + 3ull * n);
+  s->vel.assign(vel, vel + 3ull * n);
+  s->mass.assign(mass, mass + n);
+  s->img = img ? std::vector<int32_t>(img, img + 3ull * n) : std::vector<int32_t>(3ull * n, 0);
+  s->types.assign(types, types + n);
+  s->fpos.resize(3ull * n);
+  s->f.assign(3ull * n, 0.0);
+  s->eps_v.assign(eps, eps + ntypes * ntypes);
+  s->sig_v.assign(sig, sig + ntypes * ntypes);
+  s->bonds_v = copy_of(bonds, 3ull * nb);
+  s->angles_v = copy_of(angles, 4ull * na);
+  s->dihedrals_v = copy_of(dihedrals, 5ull * nd);
+  int nbt = 0, nat = 0, ndt = 0;
+  for (uint32_t k = 0; k < nb; ++k) nbt = std::max<int>(nbt, bonds[3 * k + 2]);
+  for (uint32_t k = 0; k < na; ++k) nat = std::max<int>(nat, angles[4 * k + 3]);
+  for (uint32_t k = 0; k < nd; ++k) ndt = std::max<int>(ndt, dihedrals[5 * k + 4]);
+  s->bk = copy_of(bond_k, nbt);
+  s->br0 = copy_of(bond_r0, nbt);
+  s->ak = copy_of(angle_k, nat);
+  s->at0 = copy_of(angle_theta0_deg, nat);
+  s->dk = copy_of(dihedral_k, ndt);
+  s->dd = copy_of(dihedral_d, ndt);
+  s->dn = copy_of(dihedral_n, ndt);
+  s->ff = FF{ntypes, s->eps_v.data(), s->sig_v.data(), rc, shift,
+             nb, s->bonds_v.data(), s->bk.data(), s->br0.data(),
+             na, s->angles_v.data(), s->ak.data(), s->at0.data(),
+             nd, s->dihedrals_v.data(), s->dk.data(), s->dd.data(), s->dn.data()};
+  if (excl_distance > 0 && nb > 0) exclusion_csr(n, s->ff, excl_distance, &s->ex_off, &s->ex_idx);
+  s->dt = dt;
+  s->skin = skin;
+  s->check_every = check_every;
+  s->thermostat = thermostat;
+  s->kt = kt_target;
+  s->tau = tau;
+  s->dof = std::max(0.0, 3.0 * n - 3.0);
+  const double sk = static_cast<double>(static_cast<float>(skin));
+  s->thr = 0.25 * sk * sk;
+  s->rebuild();
+  s->forces();
+  return s;
+}
+
+void orc_sim_destroy(void* sim) { delete static_cast<OracleSim*>(sim); }
+
+// Advances `steps`; writes the observables of the last force evaluation:
+// [step, pair, bond, angle, dihedral, ke, virial] (ke after Berendsen).
+void orc_sim_step(void* sim, uint64_t steps, double* obs) {
+  auto* s = static_cast<OracleSim*>(sim);
+  for (uint64_t k = 0; k < steps; ++k) s->advance();
+  if (obs) {
+    obs[0] = static_cast<double>(s->step);
+    obs[1] = s->last.pair;
+    obs[2] = s->last.bond;
+    obs[3] = s->last.angle;
+    obs[4] = s->last.dihedral;
+    obs[5] = s->kinetic();
+    obs[6] = s->last.virial;
+  }
+}
+
+void orc_sim_state(void* sim, double* pos, double* vel, int32_t* img, uint64_t* builds) {
+  auto* s = static_cast<OracleSim*>(sim);
+  if (pos) std::memcpy(pos, s->pos.data(), sizeof(double) * 3 * s->n);
+  if (vel) std::memcpy(vel, s->vel.data(), sizeof(double) * 3 * s->n);
+  if (img) std::memcpy(img, s->img.data(), sizeof(int32_t) * 3 * s->n);
+  if (builds) *builds = s->builds;
 }
 
 int orc_num_threads() {

@@ -64,11 +64,17 @@ def _declare(L) -> None:
                              c.c_double, c.c_int, c.c_double, c.c_int, *bonded,
                              _f64p, _f64p, c.POINTER(c.c_double)]
     L.orc_forces.restype = c.c_int
-    L.orc_md.argtypes = [c.c_uint32, _f64p, _f64p, _f64p, _i32p, _i32p, _f32p, _f32p, c.c_int,
-                         _f64p, _f64p, c.c_double, c.c_int, c.c_double, c.c_uint64, c.c_int,
-                         *bonded, c.c_double, c.c_int, c.c_double, c.c_double, c.c_uint64,
-                         c.c_uint64, c.c_void_p, c.POINTER(c.c_uint64)]
-    L.orc_md.restype = c.c_int64
+    L.orc_sim_create.argtypes = [c.c_uint32, _f64p, _f64p, _f64p, c.c_void_p, _i32p, _f32p,
+                                 _f32p, c.c_int, _f64p, _f64p, c.c_double, c.c_int,
+                                 c.c_double, c.c_uint64, c.c_int, *bonded, c.c_double, c.c_int,
+                                 c.c_double, c.c_double]
+    L.orc_sim_create.restype = c.c_void_p
+    L.orc_sim_destroy.argtypes = [c.c_void_p]
+    L.orc_sim_destroy.restype = None
+    L.orc_sim_step.argtypes = [c.c_void_p, c.c_uint64, _f64p]
+    L.orc_sim_step.restype = None
+    L.orc_sim_state.argtypes = [c.c_void_p, _f64p, _f64p, _i32p, c.POINTER(c.c_uint64)]
+    L.orc_sim_state.restype = None
     L.orc_num_threads.argtypes = []
     L.orc_num_threads.restype = c.c_int
 
@@ -218,35 +224,82 @@ def forces(positions, types, box_bound, ff: ForceField, *, skin: float = 0.0, bo
     return f.reshape(n, 3), e, w.value
 
 
+class Sim:
+    """Persistent FP64 velocity-Verlet (+ Berendsen) state with the reference's
+    step order and rebuild policy; ``step(k)`` advances k MD steps."""
+
+    def __init__(self, positions, velocities, masses, types, box_bound, ff: ForceField, *,
+                 dt: float, skin: float = 0.3, check_every: int = 1, images=None, bonds=None,
+                 angles=None, dihedrals=None, thermostat: bool = False, kt_target: float = 0.0,
+                 tau: float = 1.0):
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1)
+        vel = np.ascontiguousarray(velocities, dtype=np.float64).reshape(-1)
+        self.n = pos.size // 3
+        mass = np.ascontiguousarray(masses, dtype=np.float64)
+        img = (None if images is None
+               else np.ascontiguousarray(images, dtype=np.int32).reshape(-1))
+        ty = np.ascontiguousarray(types, dtype=np.int32)
+        lo, hi = _box(box_bound)
+        args, keep = _bonded_args(ff, bonds, angles, dihedrals)
+        self._keep = keep
+        self._h = lib().orc_sim_create(self.n, pos, vel, mass, _ptr(img), ty, lo, hi, ff.ntypes,
+                                       ff.epsilon, ff.sigma, ff.cutoff, int(ff.shift), skin,
+                                       check_every, ff.exclusion_distance, *args, dt,
+                                       int(thermostat), kt_target, tau)
+        if not self._h:
+            raise ValueError("neighbor search_cutoff must not exceed half shortest box length.")
+
+    def step(self, steps: int) -> np.ndarray:
+        """Advance; returns [step, pair, bond, angle, dihedral, ke, virial]."""
+        obs = np.zeros(7, np.float64)
+        lib().orc_sim_step(self._h, int(steps), obs)
+        return obs
+
+    def state(self):
+        pos = np.zeros(3 * self.n, np.float64)
+        vel = np.zeros(3 * self.n, np.float64)
+        img = np.zeros(3 * self.n, np.int32)
+        builds = ctypes.c_uint64()
+        lib().orc_sim_state(self._h, pos, vel, img, ctypes.byref(builds))
+        return pos.reshape(-1, 3), vel.reshape(-1, 3), img.reshape(-1, 3), int(builds.value)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().orc_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def md(positions, velocities, masses, types, box_bound, ff: ForceField, *, dt: float,
        steps: int, skin: float = 0.3, check_every: int = 1, images=None, bonds=None,
        angles=None, dihedrals=None, thermostat: bool = False, kt_target: float = 0.0,
        tau: float = 1.0, obs_every: int = 0):
-    """FP64 velocity-Verlet (+ Berendsen) trajectory.
-
-    Returns (positions, velocities, images, thermo rows [step, pair, bond,
-    angle, dihedral, ke, virial], build count).
-    """
-    pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1).copy()
-    vel = np.ascontiguousarray(velocities, dtype=np.float64).reshape(-1).copy()
-    n = pos.size // 3
-    mass = np.ascontiguousarray(masses, dtype=np.float64)
-    img = (np.zeros(3 * n, np.int32) if images is None
-           else np.ascontiguousarray(images, dtype=np.int32).reshape(-1).copy())
-    ty = np.ascontiguousarray(types, dtype=np.int32)
-    lo, hi = _box(box_bound)
-    rows = (steps // obs_every + 1) if obs_every else 0
-    thermo = np.zeros((max(rows, 1), 7), np.float64)
-    builds = ctypes.c_uint64()
-    args, _keep = _bonded_args(ff, bonds, angles, dihedrals)
-    got = lib().orc_md(n, pos, vel, mass, img, ty, lo, hi, ff.ntypes, ff.epsilon, ff.sigma,
-                       ff.cutoff, int(ff.shift), skin, check_every, ff.exclusion_distance,
-                       *args, dt, int(thermostat), kt_target, tau, steps, obs_every,
-                       _ptr(thermo), ctypes.byref(builds))
-    if got < 0:
-        raise ValueError("neighbor search_cutoff must not exceed half shortest box length.")
-    return (pos.reshape(n, 3), vel.reshape(n, 3), img.reshape(n, 3), thermo[:got],
-            int(builds.value))
+    """FP64 trajectory.  Returns (positions, velocities, images, thermo rows
+    [step, pair, bond, angle, dihedral, ke, virial] every obs_every steps from
+    step 0, build count)."""
+    sim = Sim(positions, velocities, masses, types, box_bound, ff, dt=dt, skin=skin,
+              check_every=check_every, images=images, bonds=bonds, angles=angles,
+              dihedrals=dihedrals, thermostat=thermostat, kt_target=kt_target, tau=tau)
+    rows = []
+    if obs_every:
+        rows.append(sim.step(0))
+        done = 0
+        while done < steps:
+            k = min(obs_every, steps - done)
+            obs = sim.step(k)
+            done += k
+            if done % obs_every == 0:
+                rows.append(obs)
+    else:
+        sim.step(steps)
+    pos, vel, img, builds = sim.state()
+    sim.close()
+    return pos, vel, img, np.array(rows).reshape(-1, 7), builds
 
 
 def num_threads() -> int:

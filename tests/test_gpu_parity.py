@@ -141,12 +141,15 @@ def test_short_md_tracks_fp64_oracle(oracle):
 
 
 def test_energy_conservation_nve():
+    # Shifted LJ keeps U continuous at rc, so the total energy only moves by
+    # integration error (plus the small force step at rc).
     spec = workloads.lj_lattice()
+    spec.shift = True
     with Engine(spec) as eng:
-        e0 = eng.eval()[0]
+        eng.run(500)  # melt the lattice first
         rows = [eng.run(100, 100)[0] for _ in range(10)]
     etot = np.array([r["pe"] + r["ke"] for r in rows])
-    drift = abs(etot[-1] - (e0["pe"] + e0["ke"])) / spec.n
+    drift = np.ptp(etot) / spec.n
     assert drift < 2e-3, drift
 
 
