@@ -225,6 +225,10 @@ void execute_run(const beads_run_desc& run) {
 
 }  // namespace
 
+namespace bb {
+void set_last_error(const char* message) { g_last_error = message; }
+}  // namespace bb
+
 extern "C" {
 
 int beads_build_info(char* buf, size_t buf_size) {

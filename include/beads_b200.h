@@ -270,6 +270,32 @@ BEADS_API int beads_list_stats(beads_ctx* ctx, uint64_t* total_entries,
 BEADS_API int beads_minimize(beads_ctx* ctx, uint32_t iterations, float dmax,
                    float fref);
 
+/* ---- allocation-free cell sort ------------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * host codes that own all device memory through their own pool, and step
+ * loops that must not synchronize the device (cudaMalloc/cudaFree do).  Bins
+ * n particles (device positions [n][3], float) into the cell grid the
+ * neighbour build uses for this box and rc + skin (same plan and cell-id
+ * rules), then sorts them stably by cell: d_cell_of[i] = cell of particle i,
+ * d_order = particle indices grouped by cell (ascending inside a cell),
+ * d_cell_start[c] = first entry of cell c in d_order (n_cells + 1 entries;
+ * *n_cells_out receives n_cells).  All device buffers are the caller's; the
+ * per-cell counters live in a static device array of BEADS_STATIC_MAX_CELLS
+ * cells that every GPU loading the library holds until exit, so grids with
+ * more cells are rejected with BEADS_ERR_INVALID.  Work is enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) and is complete
+ * when that stream is.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  All calls share the array, so calls that overlap on the GPU
+ * (different streams or host threads without ordering) race. */
+#define BEADS_STATIC_MAX_CELLS 65536u
+BEADS_API int beads_cell_sort_static(const float* d_positions, uint32_t n,
+                                     const float box_lo[3], const float box_hi[3],
+                                     double cutoff, double skin, uint32_t* d_cell_of,
+                                     uint32_t* d_order, uint32_t* d_cell_start,
+                                     uint32_t cell_start_capacity,
+                                     uint32_t* n_cells_out, void* stream);
+
 /* ---- parity / debugging views (TAG order) --------------------------------
  * Cell id of every particle from the last neighbour build (the reference's
  * particle_cell, cell_list_build.cu:135-166). */
