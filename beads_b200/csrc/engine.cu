@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <sstream>
 
@@ -48,6 +49,9 @@ Engine::Engine(uint32_t n, const beads_system_desc* systems,
                const beads_forcefield_desc* ffs, const beads_neighbor_desc* nbrs,
                const beads_dynamics_desc* dyns) {
   if (n == 0) throw InvalidArgument("a batch needs at least one replica.");
+  // BEADS_GRAPHS=0 launches every kernel directly (same kernels, no graph):
+  // profilers that cannot see kernels inside conditional graphs need it.
+  if (const char* g = std::getenv("BEADS_GRAPHS")) use_graphs_ = std::string(g) != "0";
   for (uint32_t r = 0; r < n; ++r) validate_replica(systems[r], ffs[r], nbrs[r], dyns[r]);
   cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream create");
   try {
@@ -71,6 +75,7 @@ Engine::~Engine() {
   for (void* p : allocations_) cudaFree(p);
   if (h_obs_) cudaFreeHost(h_obs_);
   if (h_state_) cudaFreeHost(h_state_);
+  if (side_stream_) cudaStreamDestroy(side_stream_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -479,22 +484,92 @@ void Engine::record_step(bool observables) {
   launch_post(launch_, true, observables);
 }
 
+// One step inside a stream capture, with the rebuild chain as the body of an
+// IF conditional node that the pre kernel switches on (CUDA 12.4+ graphs).
+// Steps without a rebuild then launch only pre, forces and post.
+void Engine::record_step_conditional(bool observables) {
+  cudaStreamCaptureStatus status;
+  cudaGraph_t graph = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t n_deps = 0;
+  cuda_check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &graph, &deps, &n_deps),
+             "capture info");
+  cudaGraphConditionalHandle handle;
+  cuda_check(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault),
+             "conditional handle");
+  launch_pre(launch_, kPreVerlet, handle, true);
+  cuda_check(cudaStreamGetCaptureInfo(stream_, &status, nullptr, &graph, &deps, &n_deps),
+             "capture info");
+  cudaGraphNodeParams params = {};
+  params.type = cudaGraphNodeTypeConditional;
+  params.conditional.handle = handle;
+  params.conditional.type = cudaGraphCondTypeIf;
+  params.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  cuda_check(cudaGraphAddNode(&node, graph, deps, n_deps, &params), "conditional node");
+  cudaGraph_t body = params.conditional.phGraph_out[0];
+  cuda_check(cudaStreamUpdateCaptureDependencies(stream_, &node, 1,
+                                                 cudaStreamSetCaptureDependencies),
+             "capture dependencies");
+  if (!side_stream_) {
+    cuda_check(cudaStreamCreateWithFlags(&side_stream_, cudaStreamNonBlocking), "stream create");
+  }
+  StepLaunch side = launch_;
+  side.stream = side_stream_;
+  cuda_check(cudaStreamBeginCaptureToGraph(side_stream_, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal),
+             "body capture");
+  try {
+    launch_rebuild(side, false);
+  } catch (...) {
+    cudaGraph_t discard = nullptr;
+    cudaStreamEndCapture(side_stream_, &discard);
+    throw;
+  }
+  cuda_check(cudaStreamEndCapture(side_stream_, &body), "body capture end");
+  launch_forces(launch_, observables, false);
+  launch_post(launch_, true, observables);
+}
+
 cudaGraphExec_t Engine::graph_for(uint32_t steps, bool obs_last) {
   const auto key = std::make_pair(steps, obs_last);
   auto it = graphs_.find(key);
   if (it != graphs_.end()) return it->second.second;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
-  try {
-    for (uint32_t s = 0; s < steps; ++s) record_step(obs_last && s + 1 == steps);
-  } catch (...) {
-    cudaStreamEndCapture(stream_, &graph);
-    if (graph) cudaGraphDestroy(graph);
-    throw;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    const bool conditional = use_conditional_;
+    cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+      for (uint32_t s = 0; s < steps; ++s) {
+        const bool obs = obs_last && s + 1 == steps;
+        if (conditional) {
+          record_step_conditional(obs);
+        } else {
+          record_step(obs);
+        }
+      }
+      cuda_check(cudaStreamEndCapture(stream_, &graph), "end capture");
+      cuda_check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+      break;
+    } catch (const CudaError&) {
+      cudaGraph_t discard = nullptr;
+      cudaStreamEndCapture(stream_, &discard);
+      if (discard) cudaGraphDestroy(discard);
+      if (graph) cudaGraphDestroy(graph);
+      graph = nullptr;
+      cudaGetLastError();
+      // Conditional nodes refused (older driver): capture the same step with
+      // the rebuild kernels returning early instead.
+      if (!conditional) throw;
+      use_conditional_ = false;
+    } catch (...) {
+      cudaGraph_t discard = nullptr;
+      cudaStreamEndCapture(stream_, &discard);
+      if (discard) cudaGraphDestroy(discard);
+      throw;
+    }
   }
-  cuda_check(cudaStreamEndCapture(stream_, &graph), "end capture");
-  cuda_check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
   graphs_[key] = std::make_pair(graph, exec);
   return exec;
 }

@@ -95,6 +95,7 @@ class Engine {
                      const beads_neighbor_desc* nbrs,
                      const beads_dynamics_desc* dyns);
   void record_step(bool observables);
+  void record_step_conditional(bool observables);
   cudaGraphExec_t graph_for(uint32_t steps, bool obs_last);
   void launch_chunk(uint32_t steps, bool obs_last);
   void sync();
@@ -108,6 +109,8 @@ class Engine {
   uint64_t step_ = 0;
   bool initialized_ = false;
   bool use_graphs_ = true;
+  bool use_conditional_ = true;
+  cudaStream_t side_stream_ = nullptr;
   std::map<std::pair<uint32_t, bool>, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs_;
   ReplicaObs* h_obs_ = nullptr;        // pinned
   ReplicaState* h_state_ = nullptr;    // pinned

@@ -105,24 +105,15 @@ __device__ __forceinline__ uint32_t axis_cell(float x, float lo, float inv,
   return idx >= n ? n - 1u : idx;
 }
 
-// Cells visited along one axis around centre c (unique, so that one or two
-// cells per axis are not visited twice).  Same set rule as the reference's
-// unique_axis_cells (small_dimension_neighbor_builder.cu:56-76).
-__device__ __forceinline__ int axis_stencil(uint32_t c, uint32_t n,
-                                            uint32_t out[3]) {
-  if (n <= 1u) {
-    out[0] = 0u;
-    return 1;
-  }
-  if (n == 2u) {
-    out[0] = 0u;
-    out[1] = 1u;
-    return 2;
-  }
-  out[0] = c == 0u ? n - 1u : c - 1u;
-  out[1] = c;
-  out[2] = c + 1u == n ? 0u : c + 1u;
-  return 3;
+// Cells visited along one axis around centre c, unique so that one or two
+// cells per axis are not visited twice (same set rule as the reference's
+// unique_axis_cells, small_dimension_neighbor_builder.cu:56-76): the k-th of
+// min(n, 3) cells, computed without an indexed array so the hot loop's state
+// stays in registers.
+__device__ __forceinline__ uint32_t stencil_cell(uint32_t c, uint32_t n, uint32_t k) {
+  if (n < 3u) return k;
+  const uint32_t t = c + k + n - 1u;  // c - 1 + k, wrapped
+  return t >= n ? (t >= 2u * n ? t - 2u * n : t - n) : t;
 }
 
 // Last block of a replica to finish a kernel (threadfence-reduction pattern:
@@ -147,7 +138,8 @@ __device__ __forceinline__ bool arrive_last(unsigned int* counter,
 // rebuild for this step (neighbor_system.cpp:79-105).
 template <int kMode>
 __global__ void __launch_bounds__(kBlock)
-k_pre(DeviceView v, float sd_dmax, float sd_fref) {
+k_pre(DeviceView v, float sd_dmax, float sd_fref, cudaGraphConditionalHandle cond,
+      int use_cond) {
   const uint32_t b = blockIdx.x;
   const uint32_t r = v.block_replica[b];
   const ReplicaParams& p = v.rp[r];
@@ -236,6 +228,9 @@ k_pre(DeviceView v, float sd_dmax, float sd_fref) {
       st->reorder_now = 0u;
     }
     st->need_rebuild = need;
+    // Inside a captured step the rebuild chain is the body of a conditional
+    // graph node: any replica that rebuilds switches it on for this step.
+    if (need && use_cond) cudaGraphSetConditional(cond, 1u);
     if (kMode == kPreVerlet) st->lambda = 1.0;
     st->done_pre = 0u;
   }
@@ -448,38 +443,46 @@ __global__ void __launch_bounds__(kBlock) k_build(DeviceView v) {
   const uint32_t cyz = cell / p.nc[0];
   const uint32_t cy = cyz % p.nc[1];
   const uint32_t cz = cyz / p.nc[1];
-  uint32_t sx[3], sy[3], sz[3];
-  const int nx = axis_stencil(cx, p.nc[0], sx);
-  const int ny = axis_stencil(cy, p.nc[1], sy);
-  const int nz = axis_stencil(cz, p.nc[2], sz);
+  const uint32_t nx = min(p.nc[0], 3u), ny = min(p.nc[1], 3u), nz = min(p.nc[2], 3u);
 
   uint32_t count = 0;
   bool overflow = false;
   const uint32_t cap = p.max_neighbors;
-  for (int a = 0; a < nz; ++a) {
-    for (int bb = 0; bb < ny; ++bb) {
-      const uint32_t rowcell = p.nc[0] * (sy[bb] + p.nc[1] * sz[a]);
-      for (int c = 0; c < nx; ++c) {
-        const uint32_t lc = sx[c] + rowcell;
+  for (uint32_t a = 0; a < nz; ++a) {
+    const uint32_t zc = stencil_cell(cz, p.nc[2], a);
+    for (uint32_t bb = 0; bb < ny; ++bb) {
+      const uint32_t rowcell = p.nc[0] * (stencil_cell(cy, p.nc[1], bb) + p.nc[1] * zc);
+      for (uint32_t c = 0; c < nx; ++c) {
+        const uint32_t lc = stencil_cell(cx, p.nc[0], c) + rowcell;
         const uint32_t s0 = v.cell_start[p.start_base + lc];
         const uint32_t s1 = v.cell_start[p.start_base + lc + 1];
-        for (uint32_t q = s0; q < s1; ++q) {
-          const uint32_t j = v.cell_atoms[q];
-          if (j == i) continue;
-          bool excluded = false;
+        // Candidates in batches of 8 (slots first, then positions) so the
+        // dependent loads of a batch overlap; insertion order is unchanged.
+        for (uint32_t q0 = s0; q0 < s1; q0 += 8u) {
+          uint32_t jj[8];
 #pragma unroll
-          for (int e = 0; e < kCap; ++e) excluded |= (ex[e] == j);
-          if (excluded) continue;
-          const float4 xj = v.pos[j];
-          const float dx = ref_delta(xi.x, xj.x, p.len[0], p.half[0]);
-          const float dy = ref_delta(xi.y, xj.y, p.len[1], p.half[1]);
-          const float dz = ref_delta(xi.z, xj.z, p.len[2], p.half[2]);
-          if (norm2(dx, dy, dz) > p.search_cut_sq) continue;
-          if (count < cap) {
-            v.nbr[nbr_index(i, count, v.nbr_stride)] = j;
-            ++count;
-          } else {
-            overflow = true;
+          for (uint32_t u = 0; u < 8u; ++u) jj[u] = (q0 + u < s1) ? v.cell_atoms[q0 + u] : i;
+          float4 xj[8];
+#pragma unroll
+          for (uint32_t u = 0; u < 8u; ++u) xj[u] = __ldg(&v.pos[jj[u]]);
+#pragma unroll
+          for (uint32_t u = 0; u < 8u; ++u) {
+            const uint32_t j = jj[u];
+            if (j == i) continue;  // self, or a lane past the end of the cell
+            bool excluded = false;
+#pragma unroll
+            for (int e = 0; e < kCap; ++e) excluded |= (ex[e] == j);
+            if (excluded) continue;
+            const float dx = ref_delta(xi.x, xj[u].x, p.len[0], p.half[0]);
+            const float dy = ref_delta(xi.y, xj[u].y, p.len[1], p.half[1]);
+            const float dz = ref_delta(xi.z, xj[u].z, p.len[2], p.half[2]);
+            if (norm2(dx, dy, dz) > p.search_cut_sq) continue;
+            if (count < cap) {
+              v.nbr[nbr_index(i, count, v.nbr_stride)] = j;
+              ++count;
+            } else {
+              overflow = true;
+            }
           }
         }
       }
@@ -508,33 +511,65 @@ __global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
   const uint32_t i = b * kBlock + threadIdx.x;
   const bool real = (i - p.atom_begin) < p.n_atoms;
   float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f, w = 0.f;
-  if (real) {
+  {
+    // Every lane of the warp (padding lanes included, with n = 0) runs the
+    // same number of batches, so the warp votes below are convergent.
     const float4 xi = v.pos[i];
     const LjCoeff* row = table + __float_as_int(xi.w) * nt;
-    const uint32_t n = v.nbr_count[i];
+    const uint32_t n = real ? v.nbr_count[i] : 0u;
+    const uint32_t n_warp = __reduce_max_sync(kFull, n);
     const float rc2 = p.force_cut_sq;
+    const float hmin = fminf(p.half[0], fminf(p.half[1], p.half[2]));
+    const float half_min_sq = hmin * hmin;
     const uint32_t* list = v.nbr + nbr_index(i, 0, v.nbr_stride);
-    for (uint32_t k = 0; k < n; ++k) {
-      const uint32_t j = list[(size_t)k * kGroup];
-      const float4 xj = v.pos[j];
-      const float dx = acc_delta(xi.x, xj.x, p.len[0], p.half[0]);
-      const float dy = acc_delta(xi.y, xj.y, p.len[1], p.half[1]);
-      const float dz = acc_delta(xi.z, xj.z, p.len[2], p.half[2]);
-      float r2 = norm2(dx, dy, dz);
-      if (!(r2 < rc2)) continue;
-      const LjCoeff c = row[__float_as_int(xj.w)];
-      if (kClamp) r2 = fmaxf(r2, 0.49f * c.sigma2);
-      const float inv_r2 = __frcp_rn(r2);
-      const float sr2 = c.sigma2 * inv_r2;
-      const float sr6 = sr2 * sr2 * sr2;
-      const float sr12 = sr6 * sr6;
-      const float fs = c.eps24 * inv_r2 * __fmaf_rn(2.0f, sr12, -sr6);
-      fx = __fmaf_rn(fs, dx, fx);
-      fy = __fmaf_rn(fs, dy, fy);
-      fz = __fmaf_rn(fs, dz, fz);
-      if (kObs) {
-        e += __fmaf_rn(c.eps4, sr12 - sr6, -c.shift);
-        w = __fmaf_rn(fs, r2, w);
+    // Software-pipelined over batches of kUnroll pairs: all list loads of a
+    // batch are issued, then all position gathers, then the arithmetic, so a
+    // warp keeps kUnroll independent misses in flight instead of one.  The
+    // list is streamed (evict-first) so the positions stay resident in L2.
+    constexpr uint32_t kUnroll = 8;
+    for (uint32_t k0 = 0; k0 < n_warp; k0 += kUnroll) {
+      uint32_t j[kUnroll];
+#pragma unroll
+      for (uint32_t u = 0; u < kUnroll; ++u) {
+        j[u] = (k0 + u < n) ? __ldcs(list + (size_t)(k0 + u) * kGroup) : i;
+      }
+      float4 xj[kUnroll];
+#pragma unroll
+      for (uint32_t u = 0; u < kUnroll; ++u) xj[u] = __ldg(&v.pos[j[u]]);
+#pragma unroll
+      for (uint32_t u = 0; u < kUnroll; ++u) {
+        // Plain differences are already the once-rounded exact values unless
+        // the pair straddles the periodic boundary, which needs r^2 above
+        // (L_min/2)^2 with plain differences; only then (warp-uniform branch)
+        // recompute with the exactly rounded minimum image.
+        float dx = __fsub_rn(xi.x, xj[u].x);
+        float dy = __fsub_rn(xi.y, xj[u].y);
+        float dz = __fsub_rn(xi.z, xj[u].z);
+        float r2 = norm2(dx, dy, dz);
+        if (__any_sync(kFull, r2 >= half_min_sq)) {
+          if (r2 >= half_min_sq) {
+            dx = acc_delta(xi.x, xj[u].x, p.len[0], p.half[0]);
+            dy = acc_delta(xi.y, xj[u].y, p.len[1], p.half[1]);
+            dz = acc_delta(xi.z, xj[u].z, p.len[2], p.half[2]);
+            r2 = norm2(dx, dy, dz);
+          }
+        }
+        if (k0 + u < n && r2 < rc2) {
+          const LjCoeff c = row[__float_as_int(xj[u].w)];
+          if (kClamp) r2 = fmaxf(r2, 0.49f * c.sigma2);
+          const float inv_r2 = __fdividef(1.0f, r2);
+          const float sr2 = c.sigma2 * inv_r2;
+          const float sr6 = sr2 * sr2 * sr2;
+          const float sr12 = sr6 * sr6;
+          const float fs = c.eps24 * inv_r2 * __fmaf_rn(2.0f, sr12, -sr6);
+          fx = __fmaf_rn(fs, dx, fx);
+          fy = __fmaf_rn(fs, dy, fy);
+          fz = __fmaf_rn(fs, dz, fz);
+          if (kObs) {
+            e += __fmaf_rn(c.eps4, sr12 - sr6, -c.shift);
+            w = __fmaf_rn(fs, r2, w);
+          }
+        }
       }
     }
   }
@@ -877,11 +912,13 @@ uint32_t cell_grid_x(uint32_t max_cells) {
 
 }  // namespace
 
-void launch_pre(const StepLaunch& l, int mode) {
+void launch_pre(const StepLaunch& l, int mode, cudaGraphConditionalHandle cond, bool use_cond) {
   if (mode == kPreDescent) {
-    k_pre<kPreDescent><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, l.sd_dmax, l.sd_fref);
+    k_pre<kPreDescent><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, l.sd_dmax, l.sd_fref, cond,
+                                                              use_cond ? 1 : 0);
   } else {
-    k_pre<kPreVerlet><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, 0.f, 0.f);
+    k_pre<kPreVerlet><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, 0.f, 0.f, cond,
+                                                             use_cond ? 1 : 0);
   }
   check_launch("pre");
 }

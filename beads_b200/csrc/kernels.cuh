@@ -22,7 +22,10 @@ struct StepLaunch {
   float sd_fref;          // descent: force floor
 };
 
-void launch_pre(const StepLaunch& l, int mode);
+// use_cond: the launch is captured in front of a conditional graph node whose
+// handle is `cond`; the kernel switches that node on when a replica rebuilds.
+void launch_pre(const StepLaunch& l, int mode, cudaGraphConditionalHandle cond = 0,
+                bool use_cond = false);
 void launch_rebuild(const StepLaunch& l, bool force_all);
 void launch_forces(const StepLaunch& l, bool observables, bool clamp);
 void launch_post(const StepLaunch& l, bool kick, bool observables);
