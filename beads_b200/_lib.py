@@ -157,6 +157,7 @@ EXPORTED = (
     "beads_minimize",
     "beads_profile",
     "beads_list_stats",
+    "beads_counters",
     "beads_cell_sort_static",
     "beads_debug_cells",
     "beads_debug_neighbors",
@@ -200,6 +201,7 @@ def load():
     L.beads_minimize.argtypes = [vp, ctypes.c_uint32, ctypes.c_float, ctypes.c_float]
     L.beads_profile.argtypes = [vp, ctypes.c_int32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]
     L.beads_list_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint32)]
+    L.beads_counters.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)]
     L.beads_cell_sort_static.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float),
                                          ctypes.POINTER(ctypes.c_float), ctypes.c_double,
                                          ctypes.c_double, vp, vp, vp, ctypes.c_uint32,

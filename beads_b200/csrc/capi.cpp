@@ -373,6 +373,14 @@ int beads_list_stats(beads_ctx* ctx, uint64_t* total_entries, uint32_t* max_coun
   });
 }
 
+int beads_counters(beads_ctx* ctx, uint32_t replica, uint64_t* counters) {
+  return guarded([&] {
+    require(ctx && ctx->engine && counters, "NULL argument.");
+    require(replica < ctx->engine->n_replicas(), "replica index out of range.");
+    ctx->engine->counters(replica, counters);
+  });
+}
+
 int beads_debug_cells(beads_ctx* ctx, uint32_t replica, uint32_t* cell_by_tag) {
   return guarded([&] {
     require(ctx && ctx->engine && cell_by_tag, "NULL argument.");

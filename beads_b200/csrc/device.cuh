@@ -16,8 +16,13 @@ namespace bb {
 constexpr int kBlock = 128;          // threads per block of per-slot kernels
 constexpr int kGroup = 32;           // neighbour-list interleave width
 constexpr int kMaxTypes = 16;        // LJ type table held in shared memory
-constexpr double kFixScale = 268435456.0;  // 2^28: fixed-point totals
-constexpr double kFixLimit = 1.0e9;  // |per-slot value| above this -> status
+// Fixed-point totals: a per-slot value v is split into floor(v) and the
+// fraction in units of 2^-32, each summed in its own 64-bit integer word.
+// Integer sums do not depend on the order of the additions, so totals are
+// bit-identical whatever the grid, batch or block shape; the whole words
+// hold any total below 2^63, the fraction words any number of slots < 2^31.
+constexpr double kFixFrac = 4294967296.0;  // 2^32
+constexpr double kFixLimit = 4.0e18;       // |per-slot value| at or above -> status
 
 // status bits (ReplicaState::status)
 constexpr unsigned kStatusNeighborOverflow = 1u;
@@ -87,7 +92,8 @@ struct ReplicaState {
   unsigned int status;              // kStatus* bits
   unsigned int pad0;
   double lambda;                    // pending Berendsen velocity scale
-  long long acc[kAccLanes];         // fixed-point totals of the current eval
+  long long acc[kAccLanes];         // fixed-point totals of the current eval:
+  long long acc_frac[kAccLanes];    //   whole words and 2^-32 fraction words
 };
 
 // Observables of the last evaluation of one replica (device copy).
@@ -178,6 +184,7 @@ struct DeviceView {
   ReplicaState* rs;
   ReplicaObs* obs;
   const uint32_t* block_replica;
+  const uint32_t* cell_replica;  // replica of each global cell
   const LjCoeff* lj;
   uint32_t n_replicas;
   uint32_t n_slots;

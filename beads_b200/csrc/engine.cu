@@ -378,6 +378,14 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   v.rs = dalloc<ReplicaState>(n);
   v.obs = dalloc<ReplicaObs>(n);
   uint32_t* d_block_replica = dalloc<uint32_t>(block_replica.size());
+  std::vector<uint32_t> cell_replica(C);
+  bool all_regular = true;
+  for (uint32_t r = 0; r < n; ++r) {
+    std::fill(cell_replica.begin() + rp[r].cell_begin,
+              cell_replica.begin() + rp[r].cell_begin + rp[r].n_cells, r);
+    for (int a = 0; a < 3; ++a) all_regular = all_regular && rp[r].nc[a] >= 4u;
+  }
+  uint32_t* d_cell_replica = dalloc<uint32_t>(C);
   LjCoeff* d_lj = dalloc<LjCoeff>(h_lj.size());
 
   auto up = [&](void* dst, const void* src, size_t bytes) {
@@ -402,6 +410,7 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   up(d_dc, h_dc.data(), h_dc.size() * sizeof(DihedralCoeff));
   up(d_rp, rp.data(), n * sizeof(ReplicaParams));
   up(d_block_replica, block_replica.data(), block_replica.size() * sizeof(uint32_t));
+  up(d_cell_replica, cell_replica.data(), C * sizeof(uint32_t));
   up(d_lj, h_lj.data(), h_lj.size() * sizeof(LjCoeff));
   std::vector<ReplicaState> rs(n);
   std::memset(rs.data(), 0, n * sizeof(ReplicaState));
@@ -420,6 +429,7 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   v.dihedral_coeff = d_dc;
   v.rp = d_rp;
   v.block_replica = d_block_replica;
+  v.cell_replica = d_cell_replica;
   v.lj = d_lj;
 
   cuda_check(cudaMallocHost(&h_obs_, n * sizeof(ReplicaObs)), "cudaMallocHost");
@@ -428,6 +438,7 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   launch_.v = v;
   launch_.stream = stream_;
   launch_.max_cells_per_replica = max_cells;
+  launch_.all_regular = all_regular ? 1 : 0;
   launch_.max_atoms_per_replica = max_atoms;
   launch_.excl_cap = excl_cap;
   launch_.need_kinetic = any_thermostat ? 1 : 0;
@@ -459,7 +470,8 @@ void Engine::check_status() {
       throw NeighborOverflow(m.str());
     }
     if (s & kStatusFixedOverflow) {
-      throw OverflowError("energy/virial total exceeds the fixed-point accumulator range.");
+      throw OverflowError("energy, virial or kinetic energy of a particle is not finite or "
+                          "exceeds the fixed-point accumulator range (|value| < 4e18).");
     }
     if (s & kStatusNonFinite) {
       throw NonFinite("non-finite velocity after force evaluation (replica " +
@@ -480,13 +492,13 @@ void Engine::eval() {
 void Engine::record_step(bool observables) {
   launch_pre(launch_, kPreVerlet);
   launch_rebuild(launch_, false);
-  launch_forces(launch_, observables, false);
-  launch_post(launch_, true, observables);
+  launch_forces(launch_, observables, false, true);
 }
 
 // One step inside a stream capture, with the rebuild chain as the body of an
 // IF conditional node that the pre kernel switches on (CUDA 12.4+ graphs).
-// Steps without a rebuild then launch only pre, forces and post.
+// Steps without a rebuild then launch only pre and the force kernel(s), the
+// last of which also does the second half-kick.
 void Engine::record_step_conditional(bool observables) {
   cudaStreamCaptureStatus status;
   cudaGraph_t graph = nullptr;
@@ -527,8 +539,7 @@ void Engine::record_step_conditional(bool observables) {
     throw;
   }
   cuda_check(cudaStreamEndCapture(side_stream_, &body), "body capture end");
-  launch_forces(launch_, observables, false);
-  launch_post(launch_, true, observables);
+  launch_forces(launch_, observables, false, true);
 }
 
 cudaGraphExec_t Engine::graph_for(uint32_t steps, bool obs_last) {
@@ -596,6 +607,14 @@ bool Engine::run(uint64_t steps, uint64_t obs_every) {
         obs = true;
       }
     }
+    // Chunks are powers of two, so a run of any length replays at most
+    // log2(kChunkMax) + 1 distinct captured graphs (instantiated once each).
+    uint64_t pow2 = 1;
+    while (pow2 * 2 <= chunk) pow2 *= 2;
+    if (pow2 != chunk) {
+      chunk = pow2;
+      obs = false;
+    }
     launch_chunk(static_cast<uint32_t>(chunk), obs);
     step_ += chunk;
     remaining -= chunk;
@@ -644,12 +663,25 @@ double Engine::profile(int stage, uint32_t reps) {
   cuda_check(cudaEventCreate(&start), "event create");
   cuda_check(cudaEventCreate(&stop), "event create");
   float ms = 0.f;
+  std::vector<ReplicaState> saved;
+  if (stage == 3) {
+    // The kick variant changes velocities and the per-replica step state:
+    // keep copies and put them back after timing.
+    saved.resize(rep_.size());
+    sync();
+    cuda_check(cudaMemcpy(saved.data(), v_.rs, saved.size() * sizeof(ReplicaState),
+                          cudaMemcpyDeviceToHost), "state save");
+    cuda_check(cudaMemcpyAsync(v_.vel2, v_.vel, v_.n_slots * sizeof(float4),
+                               cudaMemcpyDeviceToDevice, stream_), "velocity save");
+  }
   try {
     sync();
     cuda_check(cudaEventRecord(start, stream_), "event record");
     for (uint32_t k = 0; k < reps; ++k) {
       if (stage == 0) {
         launch_forces(launch_, false, false);
+      } else if (stage == 3) {
+        launch_forces(launch_, false, false, true);
       } else if (stage == 1) {
         launch_chunk(1, false);
         step_ += 1;
@@ -669,8 +701,25 @@ double Engine::profile(int stage, uint32_t reps) {
   }
   cudaEventDestroy(start);
   cudaEventDestroy(stop);
+  if (stage == 3) {
+    cuda_check(cudaMemcpyAsync(v_.vel, v_.vel2, v_.n_slots * sizeof(float4),
+                               cudaMemcpyDeviceToDevice, stream_), "velocity restore");
+    cuda_check(cudaMemcpyAsync(v_.rs, saved.data(), saved.size() * sizeof(ReplicaState),
+                               cudaMemcpyHostToDevice, stream_), "state restore");
+    sync();
+  }
   check_status();
   return static_cast<double>(ms) / reps;
+}
+
+void Engine::counters(uint32_t replica, uint64_t out[3]) {
+  sync();
+  ReplicaState st;
+  cuda_check(cudaMemcpy(&st, v_.rs + replica, sizeof(ReplicaState), cudaMemcpyDeviceToHost),
+             "counters download");
+  out[0] = st.step;
+  out[1] = st.builds;
+  out[2] = st.dangerous;
 }
 
 void Engine::list_stats(uint64_t* total, uint32_t* max_count) {

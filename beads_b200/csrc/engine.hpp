@@ -85,6 +85,8 @@ class Engine {
   void flush_lambda();
   double profile(int stage, uint32_t reps);
   void list_stats(uint64_t* total, uint32_t* max_count);
+  // Completed steps, neighbour builds and dangerous rebuilds of one replica.
+  void counters(uint32_t replica, uint64_t out[3]);
   void check_status();
 
  private:

@@ -31,33 +31,68 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-__device__ __forceinline__ long long to_fixed(double v, unsigned* status) {
+// One slot's contribution to a fixed-point total: floor(v) and the fraction
+// v - floor(v) (exact in double) truncated to units of 2^-32.
+struct Fixed {
+  long long whole;
+  long long frac;
+};
+
+__device__ __forceinline__ Fixed to_fixed(double v, unsigned* status) {
   if (!(fabs(v) < kFixLimit)) {
     atomicOr(status, kStatusFixedOverflow);
-    return 0;
+    return Fixed{0, 0};
   }
-  return __double2ll_rn(v * kFixScale);
+  const double w = floor(v);
+  return Fixed{(long long)w, (long long)((v - w) * kFixFrac)};
 }
 
-__device__ __forceinline__ double from_fixed(long long v) {
-  return (double)v / kFixScale;
+__device__ __forceinline__ double from_fixed(long long whole, long long frac) {
+  return (double)whole + (double)frac / kFixFrac;
 }
 
-// Warp + block sum of a 64-bit integer, one atomic per block.
+// Warp + block sum of one fixed-point contribution, two atomics per block.
 template <int kThreads>
-__device__ __forceinline__ void block_add_ll(long long v, long long* target) {
-  __shared__ long long partial[kThreads / 32];
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+__device__ __forceinline__ void block_add_fixed(Fixed f, long long* whole, long long* frac) {
+  __shared__ long long partial[2][kThreads / 32];
+  long long a = f.whole, c = f.frac;
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(kFull, a, o);
+    c += __shfl_down_sync(kFull, c, o);
+  }
   const int warp = threadIdx.x >> 5;
-  if ((threadIdx.x & 31) == 0) partial[warp] = v;
+  if ((threadIdx.x & 31) == 0) {
+    partial[0][warp] = a;
+    partial[1][warp] = c;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    long long s = 0;
-    for (int w = 0; w < kThreads / 32; ++w) s += partial[w];
-    if (s != 0) atomicAdd(reinterpret_cast<unsigned long long*>(target),
-                          static_cast<unsigned long long>(s));
+    long long sa = 0, sc = 0;
+    for (int w = 0; w < kThreads / 32; ++w) {
+      sa += partial[0][w];
+      sc += partial[1][w];
+    }
+    if (sa != 0) atomicAdd(reinterpret_cast<unsigned long long*>(whole),
+                           static_cast<unsigned long long>(sa));
+    if (sc != 0) atomicAdd(reinterpret_cast<unsigned long long*>(frac),
+                           static_cast<unsigned long long>(sc));
   }
   __syncthreads();
+}
+
+template <int kThreads>
+__device__ __forceinline__ void block_add_lane(bool real, double v, ReplicaState* st, int lane) {
+  block_add_fixed<kThreads>(real ? to_fixed(v, &st->status) : Fixed{0, 0}, &st->acc[lane],
+                            &st->acc_frac[lane]);
+}
+
+// Reads and clears one fixed-point total (last block of a replica only).
+__device__ __forceinline__ double take_total(ReplicaState* st, int lane) {
+  unsigned long long* w = reinterpret_cast<unsigned long long*>(st->acc);
+  unsigned long long* f = reinterpret_cast<unsigned long long*>(st->acc_frac);
+  const long long whole = (long long)atomicExch(&w[lane], 0ull);
+  const long long frac = (long long)atomicExch(&f[lane], 0ull);
+  return from_fixed(whole, frac);
 }
 
 // Minimum image exactly as the reference applies it to wrapped coordinates
@@ -421,85 +456,291 @@ k_project_exclusions(DeviceView v, int force_all) {
 // rebuild 7: full neighbour list over the cell stencil, reference inclusion
 // rule: skip self and excluded partners, keep r^2 <= (rc+skin)^2, count
 // overflow past max_neighbors.  Also captures the displacement reference.
-template <int kCap>
-__global__ void __launch_bounds__(kBlock) k_build(DeviceView v) {
-  const uint32_t b = blockIdx.x;
-  const uint32_t r = v.block_replica[b];
+//
+// One warp per cell: lane l owns the l-th particle of the cell (cells of more
+// than 32 particles take several passes).  Candidates are staged 32 at a time
+// in shared memory (structure of arrays, so two consecutive candidates are
+// one 8-byte broadcast read per coordinate) and every lane tests them two at
+// a time on the packed FP32x2 pipe.  Candidates are visited in the
+// reference's stencil order (z, y, x cells; ascending slot inside a cell), so
+// each particle's list order is fixed.
+//
+// kRegular (every axis has >= 4 cells): a stencil cell reached across the
+// periodic boundary gets one shift s = +-L for the whole cell and the
+// difference is fl(fl(xi - xj) + s).  For any pair that can pass the search
+// cutoff this is exactly the reference's form (fl(xi - xj), then fl(d -+ L)
+// when |d| > L/2), because with >= 4 cells per axis a neighbour-cell pair
+// has |xi - xj| < L/2 unless it wraps, and a wrapped one has |xi - xj| > L/2.
+// Otherwise (small-dimension and direct paths) the reference form is applied
+// per pair.
+constexpr int kBuildWarps = kBlock / 32;
+
+template <int kCap, bool kRegular>
+struct BuildLane {
+  uint32_t i;
+  float2 xx, xy, xz;  // own coordinates, duplicated for the packed pipe
+  float4 xi;
+  uint32_t* row;      // entry 0 of this particle's list; entry k at row[k * kGroup]
+  uint32_t cap;
+  uint32_t count;     // candidates accepted (may pass cap: overflow)
+  uint32_t ex[kCap > 0 ? kCap : 1];
+
+  // Branch-free append: the store is predicated, the count always advances
+  // for an accepted candidate so overflow is count > cap at the end.
+  __device__ __forceinline__ void put(bool ok, uint32_t j) {
+    if (ok && count < cap) row[count * kGroup] = j;
+    count += ok ? 1u : 0u;
+  }
+
+  __device__ __forceinline__ bool excluded(uint32_t j) const {
+    bool e = false;
+#pragma unroll
+    for (int k = 0; k < kCap; ++k) e |= (ex[k] == j);
+    return e;
+  }
+};
+
+// Tests the staged candidates [0, m) of this warp against one lane.
+template <int kCap, bool kRegular>
+__device__ __forceinline__ void test_staged(const ReplicaParams& p, BuildLane<kCap, kRegular>& L,
+                                            const float* sx, const float* sy, const float* sz,
+                                            const uint32_t* sj, uint32_t m, float2 s2x,
+                                            float2 s2y, float2 s2z) {
+  const float2 neg1 = make_float2(-1.0f, -1.0f);
+  const float cut = p.search_cut_sq;
+  for (uint32_t t = 0; t < m; t += 2) {
+    const float2 jx = *reinterpret_cast<const float2*>(sx + t);
+    const float2 jy = *reinterpret_cast<const float2*>(sy + t);
+    const float2 jz = *reinterpret_cast<const float2*>(sz + t);
+    const uint2 jj = *reinterpret_cast<const uint2*>(sj + t);
+    float2 dx, dy, dz;
+    if (kRegular) {
+      // fl(xi - xj) (xj * -1 is exact), then fl(d + s).
+      dx = __fadd2_rn(__ffma2_rn(jx, neg1, L.xx), s2x);
+      dy = __fadd2_rn(__ffma2_rn(jy, neg1, L.xy), s2y);
+      dz = __fadd2_rn(__ffma2_rn(jz, neg1, L.xz), s2z);
+    } else {
+      dx = make_float2(ref_delta(L.xi.x, jx.x, p.len[0], p.half[0]),
+                       ref_delta(L.xi.x, jx.y, p.len[0], p.half[0]));
+      dy = make_float2(ref_delta(L.xi.y, jy.x, p.len[1], p.half[1]),
+                       ref_delta(L.xi.y, jy.y, p.len[1], p.half[1]));
+      dz = make_float2(ref_delta(L.xi.z, jz.x, p.len[2], p.half[2]),
+                       ref_delta(L.xi.z, jz.y, p.len[2], p.half[2]));
+    }
+    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+    // The staged tail entry of an odd chunk carries slot 0xffffffff.
+    L.put(!(r2.x > cut) && jj.x != L.i && !L.excluded(jj.x), jj.x);
+    L.put(!(r2.y > cut) && jj.y != L.i && jj.y != 0xffffffffu && !L.excluded(jj.y), jj.y);
+  }
+}
+
+// Stages candidates [q0, q1) of cell_atoms 32 at a time in this warp's
+// shared arrays and tests them against every active lane.
+template <int kCap, bool kRegular>
+__device__ __forceinline__ void scan_range(const DeviceView& v, const ReplicaParams& p,
+                                           BuildLane<kCap, kRegular>& L, bool active,
+                                           uint32_t lane, uint32_t q0, uint32_t q1,
+                                           float2 s2x, float2 s2y, float2 s2z, float* sx,
+                                           float* sy, float* sz, uint32_t* sj) {
+  for (uint32_t q = q0; q < q1; q += 32u) {
+    const uint32_t m = min(32u, q1 - q);
+    __syncwarp();
+    if (lane < m) {
+      const uint32_t j = v.cell_atoms[q + lane];
+      const float4 xj = v.pos[j];
+      sx[lane] = xj.x;
+      sy[lane] = xj.y;
+      sz[lane] = xj.z;
+      sj[lane] = j;
+    } else if (lane == m) {  // pad the odd tail: tested, never appended
+      sx[lane] = 0.f;
+      sy[lane] = 0.f;
+      sz[lane] = 0.f;
+      sj[lane] = 0xffffffffu;
+    }
+    __syncwarp();
+    if (active) test_staged<kCap, kRegular>(p, L, sx, sy, sz, sj, m, s2x, s2y, s2z);
+  }
+}
+
+template <int kCap, bool kRegular>
+__global__ void __launch_bounds__(kBlock, kCap > 16 ? 2 : 8) k_build(DeviceView v) {
+  __shared__ __align__(16) float sh_x[kBuildWarps][32];
+  __shared__ __align__(16) float sh_y[kBuildWarps][32];
+  __shared__ __align__(16) float sh_z[kBuildWarps][32];
+  __shared__ __align__(16) uint32_t sh_j[kBuildWarps][32];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t g = blockIdx.x * kBuildWarps + warp;  // global cell
+  if (g >= v.total_cells) return;                      // warp-uniform exits
+  const uint32_t r = v.cell_replica[g];
   ReplicaState* st = &v.rs[r];
   if (!st->need_rebuild) return;
   const ReplicaParams& p = v.rp[r];
-  const uint32_t i = b * kBlock + threadIdx.x;
-  if (i - p.atom_begin >= p.n_atoms) return;
+  const uint32_t c = g - p.cell_begin;
+  const uint32_t* start = v.cell_start + p.start_base;
+  const uint32_t cs = start[c], ce = start[c + 1];
+  const uint32_t nx = p.nc[0], ny = p.nc[1], nz = p.nc[2];
+  const uint32_t cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+  float* sx = sh_x[warp];
+  float* sy = sh_y[warp];
+  float* sz = sh_z[warp];
+  uint32_t* sj = sh_j[warp];
+  bool any_overflow = false;
 
-  const float4 xi = v.pos[i];
-  uint32_t ex[kCap > 0 ? kCap : 1];
-  if (kCap > 0) {
-    const uint32_t* row = v.excl_slot + (size_t)i * v.excl_cap;
+  for (uint32_t i0 = cs; i0 < ce; i0 += 32u) {
+    const bool active = i0 + lane < ce;
+    BuildLane<kCap, kRegular> L;
+    L.i = active ? v.cell_atoms[i0 + lane] : 0xfffffffeu;
+    L.xi = active ? v.pos[L.i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    L.xx = make_float2(L.xi.x, L.xi.x);
+    L.xy = make_float2(L.xi.y, L.xi.y);
+    L.xz = make_float2(L.xi.z, L.xi.z);
+    L.count = 0;
+    L.cap = p.max_neighbors;
+    L.row = v.nbr + nbr_index(active ? L.i : 0u, 0, v.nbr_stride);
+    if (kCap > 0) {
+      const uint32_t* row = v.excl_slot + (size_t)(active ? L.i : 0u) * v.excl_cap;
 #pragma unroll
-    for (int e = 0; e < kCap; ++e) ex[e] = row[e];
-  }
-  const uint32_t cell = v.cell_of_slot[i] - p.cell_begin;
-  const uint32_t cx = cell % p.nc[0];
-  const uint32_t cyz = cell / p.nc[0];
-  const uint32_t cy = cyz % p.nc[1];
-  const uint32_t cz = cyz / p.nc[1];
-  const uint32_t nx = min(p.nc[0], 3u), ny = min(p.nc[1], 3u), nz = min(p.nc[2], 3u);
-
-  uint32_t count = 0;
-  bool overflow = false;
-  const uint32_t cap = p.max_neighbors;
-  for (uint32_t a = 0; a < nz; ++a) {
-    const uint32_t zc = stencil_cell(cz, p.nc[2], a);
-    for (uint32_t bb = 0; bb < ny; ++bb) {
-      const uint32_t rowcell = p.nc[0] * (stencil_cell(cy, p.nc[1], bb) + p.nc[1] * zc);
-      for (uint32_t c = 0; c < nx; ++c) {
-        const uint32_t lc = stencil_cell(cx, p.nc[0], c) + rowcell;
-        const uint32_t s0 = v.cell_start[p.start_base + lc];
-        const uint32_t s1 = v.cell_start[p.start_base + lc + 1];
-        // Candidates in batches of 8 (slots first, then positions) so the
-        // dependent loads of a batch overlap; insertion order is unchanged.
-        for (uint32_t q0 = s0; q0 < s1; q0 += 8u) {
-          uint32_t jj[8];
-#pragma unroll
-          for (uint32_t u = 0; u < 8u; ++u) jj[u] = (q0 + u < s1) ? v.cell_atoms[q0 + u] : i;
-          float4 xj[8];
-#pragma unroll
-          for (uint32_t u = 0; u < 8u; ++u) xj[u] = __ldg(&v.pos[jj[u]]);
-#pragma unroll
-          for (uint32_t u = 0; u < 8u; ++u) {
-            const uint32_t j = jj[u];
-            if (j == i) continue;  // self, or a lane past the end of the cell
-            bool excluded = false;
-#pragma unroll
-            for (int e = 0; e < kCap; ++e) excluded |= (ex[e] == j);
-            if (excluded) continue;
-            const float dx = ref_delta(xi.x, xj[u].x, p.len[0], p.half[0]);
-            const float dy = ref_delta(xi.y, xj[u].y, p.len[1], p.half[1]);
-            const float dz = ref_delta(xi.z, xj[u].z, p.len[2], p.half[2]);
-            if (norm2(dx, dy, dz) > p.search_cut_sq) continue;
-            if (count < cap) {
-              v.nbr[nbr_index(i, count, v.nbr_stride)] = j;
-              ++count;
-            } else {
-              overflow = true;
-            }
+      for (int e = 0; e < kCap; ++e) L.ex[e] = active ? row[e] : 0xffffffffu;
+    }
+    if (kRegular) {
+      // 9 rows of three x-cells; a row is one contiguous run of cell_atoms
+      // unless it wraps in x, where it splits at the boundary.
+      for (uint32_t a = 0; a < 3u; ++a) {
+        const uint32_t zc = stencil_cell(cz, nz, a);
+        const float sz_ = (cz == 0u && a == 0u) ? p.len[2]
+                          : (cz == nz - 1u && a == 2u) ? -p.len[2] : 0.0f;
+        for (uint32_t bb = 0; bb < 3u; ++bb) {
+          const uint32_t yc = stencil_cell(cy, ny, bb);
+          const float sy_ = (cy == 0u && bb == 0u) ? p.len[1]
+                            : (cy == ny - 1u && bb == 2u) ? -p.len[1] : 0.0f;
+          const uint32_t row = nx * (yc + ny * zc);
+          const float2 s2y = make_float2(sy_, sy_), s2z = make_float2(sz_, sz_);
+          // Up to two segments: [first run, second run) with their x shifts.
+          uint32_t c0 = cx - 1u, c1 = cx + 2u, d0 = 0u, d1 = 0u;
+          float sx0 = 0.0f, sx1 = 0.0f;
+          uint32_t nseg = 1u;
+          if (cx == 0u) {
+            c0 = nx - 1u, c1 = nx, sx0 = p.len[0], d0 = 0u, d1 = 2u, nseg = 2u;
+          } else if (cx == nx - 1u) {
+            c0 = nx - 2u, c1 = nx, d0 = 0u, d1 = 1u, sx1 = -p.len[0], nseg = 2u;
+          }
+          for (uint32_t sg = 0; sg < nseg; ++sg) {
+            const uint32_t lo = sg == 0u ? c0 : d0, hi = sg == 0u ? c1 : d1;
+            const float shx = sg == 0u ? sx0 : sx1;
+            scan_range(v, p, L, active, lane, start[row + lo], start[row + hi],
+                       make_float2(shx, shx), s2y, s2z, sx, sy, sz, sj);
+          }
+        }
+      }
+    } else {
+      const uint32_t sxn = min(nx, 3u), syn = min(ny, 3u), szn = min(nz, 3u);
+      const float2 zero = make_float2(0.f, 0.f);
+      for (uint32_t a = 0; a < szn; ++a) {
+        const uint32_t zc = stencil_cell(cz, nz, a);
+        for (uint32_t bb = 0; bb < syn; ++bb) {
+          const uint32_t row = nx * (stencil_cell(cy, ny, bb) + ny * zc);
+          for (uint32_t k = 0; k < sxn; ++k) {
+            const uint32_t lc = row + stencil_cell(cx, nx, k);
+            scan_range(v, p, L, active, lane, start[lc], start[lc + 1], zero, zero, zero,
+                       sx, sy, sz, sj);
           }
         }
       }
     }
+    if (active) {
+      v.nbr_count[L.i] = min(L.count, L.cap);
+      v.ref_pos[L.i] = L.xi;
+      v.ref_img[L.i] = v.img[L.i];
+    }
+    any_overflow |= active && L.count > L.cap;
   }
-  v.nbr_count[i] = count;
-  v.ref_pos[i] = xi;
-  v.ref_img[i] = v.img[i];
-  if (overflow) atomicOr(&st->status, kStatusNeighborOverflow);
+  if (__any_sync(kFull, any_overflow) && lane == 0) atomicOr(&st->status, kStatusNeighborOverflow);
+}
+
+// ---------------------------------------------------------------------------
+// Second half-kick of a step, shared by k_post and by the force kernels that
+// finish a step themselves (see k_post).
+enum ForceMode : int {
+  kForcePlain = 0,        // forces only
+  kForceClamp = 1,        // forces on r^2 clamped to >= 0.49 sigma^2 (descent)
+  kForcePost = 2,         // forces, then the second half-kick
+  kForcePostKinetic = 3,  // forces, kick and the kinetic-energy total
+};
+
+// Kick of one slot with its final force; returns its kinetic energy.
+template <bool kKick, bool kKinetic>
+__device__ __forceinline__ double post_slot(const DeviceView& v, const ReplicaParams& p,
+                                            ReplicaState* st, uint32_t i, bool real,
+                                            float fx, float fy, float fz) {
+  double ke = 0.0;
+  if (real) {
+    float4 vm = v.vel[i];
+    if (kKick) {
+      const float h = __fdiv_rn(__fmul_rn(0.5f, p.dt), vm.w);
+      vm.x = __fmaf_rn(h, fx, vm.x);
+      vm.y = __fmaf_rn(h, fy, vm.y);
+      vm.z = __fmaf_rn(h, fz, vm.z);
+      v.vel[i] = vm;
+      if (!isfinite(vm.x + vm.y + vm.z)) atomicOr(&st->status, kStatusNonFinite);
+    }
+    if (kKinetic) {
+      const double vx = vm.x, vy = vm.y, vz = vm.z;
+      ke = 0.5 * (double)vm.w * (vx * vx + vy * vy + vz * vz);
+    }
+  }
+  return ke;
+}
+
+// Block sum of the kinetic energy and, in the replica's last block, the
+// step's per-replica work.  Every block of the replica must call it.
+template <bool kKick, bool kObs, bool kKinetic>
+__device__ __forceinline__ void post_finish(const DeviceView& v, const ReplicaParams& p,
+                                            ReplicaState* st, uint32_t r, bool real,
+                                            double ke) {
+  if (kKinetic) block_add_lane<kBlock>(real, ke, st, kAccKinetic);
+  const uint32_t n_blocks = p.n_pad / kBlock;
+  if (arrive_last(&st->done_post, n_blocks) && threadIdx.x == 0) {
+    const double kin = kKinetic ? take_total(st, kAccKinetic) : 0.0;
+    double lam = 1.0;
+    if (kKick && kKinetic && p.thermostat == 1 && kin > 0.0 && p.dof > 0.0) {
+      const double current = 2.0 * kin / p.dof;
+      const double arg = 1.0 + ((double)p.dt / p.tau) * (p.kt_target / current - 1.0);
+      lam = sqrt(arg > 0.0 ? arg : 0.0);
+    }
+    if (kKick) {
+      st->lambda = lam;
+      st->step += 1ull;
+    }
+    if (kObs) {
+      ReplicaObs o;
+      o.step = st->step;
+      o.pair_pe = take_total(st, kAccPair);
+      o.bond_pe = take_total(st, kAccBond);
+      o.angle_pe = take_total(st, kAccAngle);
+      o.dihedral_pe = take_total(st, kAccDihedral);
+      o.virial = take_total(st, kAccVirial);
+      o.ke_pre = kin;
+      o.lambda = lam;
+      o.builds = st->builds;
+      o.dangerous = st->dangerous;
+      o.status = st->status;
+      o.pad = 0;
+      v.obs[r] = o;
+    }
+    st->done_post = 0u;
+  }
 }
 
 // ---------------------------------------------------------------------------
 // LJ pair forces over the full list (each pair evaluated from both ends, no
 // atomics).  FP32 pair arithmetic; per-slot energy and virial are converted to
 // fixed point once per slot and reduced per block.
-template <bool kObs, bool kClamp>
-__global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
+template <bool kObs, int kMode>
+__global__ void __launch_bounds__(kBlock, kObs ? 6 : 8) k_lj(DeviceView v) {
+  constexpr bool kClamp = kMode == kForceClamp;
+  constexpr bool kPost = kMode >= kForcePost;
+  constexpr bool kKinetic = kMode == kForcePostKinetic || (kPost && kObs);
   const uint32_t b = blockIdx.x;
   const uint32_t r = v.block_replica[b];
   const ReplicaParams& p = v.rp[r];
@@ -521,6 +762,10 @@ __global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
     const float rc2 = p.force_cut_sq;
     const float hmin = fminf(p.half[0], fminf(p.half[1], p.half[2]));
     const float half_min_sq = hmin * hmin;
+    const float2 xi2x = make_float2(xi.x, xi.x);
+    const float2 xi2y = make_float2(xi.y, xi.y);
+    const float2 xi2z = make_float2(xi.z, xi.z);
+    float2 f2x = make_float2(0.f, 0.f), f2y = f2x, f2z = f2x, e2 = f2x, w2 = f2x;
     const uint32_t* list = v.nbr + nbr_index(i, 0, v.nbr_stride);
     // Software-pipelined over batches of kUnroll pairs: all list loads of a
     // batch are issued, then all position gathers, then the arithmetic, so a
@@ -536,51 +781,81 @@ __global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
       float4 xj[kUnroll];
 #pragma unroll
       for (uint32_t u = 0; u < kUnroll; ++u) xj[u] = __ldg(&v.pos[j[u]]);
+      // Pairs 2h and 2h+1 of the batch run through the packed FP32x2 pipe of
+      // sm_100 (__fadd2_rn / __fmul2_rn / __ffma2_rn round each lane exactly
+      // as the scalar operation would): one instruction per two pairs.  Pairs
+      // beyond the cutoff and padding entries get a zero force scale rather
+      // than a branch.
 #pragma unroll
-      for (uint32_t u = 0; u < kUnroll; ++u) {
+      for (uint32_t h = 0; h < kUnroll / 2; ++h) {
+        const uint32_t u0 = 2 * h, u1 = 2 * h + 1;
+        float2 dx = __fadd2_rn(xi2x, make_float2(-xj[u0].x, -xj[u1].x));
+        float2 dy = __fadd2_rn(xi2y, make_float2(-xj[u0].y, -xj[u1].y));
+        float2 dz = __fadd2_rn(xi2z, make_float2(-xj[u0].z, -xj[u1].z));
+        float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
         // Plain differences are already the once-rounded exact values unless
         // the pair straddles the periodic boundary, which needs r^2 above
-        // (L_min/2)^2 with plain differences; only then (warp-uniform branch)
-        // recompute with the exactly rounded minimum image.
-        float dx = __fsub_rn(xi.x, xj[u].x);
-        float dy = __fsub_rn(xi.y, xj[u].y);
-        float dz = __fsub_rn(xi.z, xj[u].z);
-        float r2 = norm2(dx, dy, dz);
-        if (__any_sync(kFull, r2 >= half_min_sq)) {
-          if (r2 >= half_min_sq) {
-            dx = acc_delta(xi.x, xj[u].x, p.len[0], p.half[0]);
-            dy = acc_delta(xi.y, xj[u].y, p.len[1], p.half[1]);
-            dz = acc_delta(xi.z, xj[u].z, p.len[2], p.half[2]);
-            r2 = norm2(dx, dy, dz);
+        // (L_min/2)^2; only then (warp-uniform branch) recompute that pair
+        // with the exactly rounded minimum image.
+        const bool far0 = r2.x >= half_min_sq, far1 = r2.y >= half_min_sq;
+        if (__any_sync(kFull, far0 || far1)) {
+          if (far0) {
+            dx.x = acc_delta(xi.x, xj[u0].x, p.len[0], p.half[0]);
+            dy.x = acc_delta(xi.y, xj[u0].y, p.len[1], p.half[1]);
+            dz.x = acc_delta(xi.z, xj[u0].z, p.len[2], p.half[2]);
+            r2.x = norm2(dx.x, dy.x, dz.x);
+          }
+          if (far1) {
+            dx.y = acc_delta(xi.x, xj[u1].x, p.len[0], p.half[0]);
+            dy.y = acc_delta(xi.y, xj[u1].y, p.len[1], p.half[1]);
+            dz.y = acc_delta(xi.z, xj[u1].z, p.len[2], p.half[2]);
+            r2.y = norm2(dx.y, dy.y, dz.y);
           }
         }
-        if (k0 + u < n && r2 < rc2) {
-          const LjCoeff c = row[__float_as_int(xj[u].w)];
-          if (kClamp) r2 = fmaxf(r2, 0.49f * c.sigma2);
-          const float inv_r2 = __fdividef(1.0f, r2);
-          const float sr2 = c.sigma2 * inv_r2;
-          const float sr6 = sr2 * sr2 * sr2;
-          const float sr12 = sr6 * sr6;
-          const float fs = c.eps24 * inv_r2 * __fmaf_rn(2.0f, sr12, -sr6);
-          fx = __fmaf_rn(fs, dx, fx);
-          fy = __fmaf_rn(fs, dy, fy);
-          fz = __fmaf_rn(fs, dz, fz);
-          if (kObs) {
-            e += __fmaf_rn(c.eps4, sr12 - sr6, -c.shift);
-            w = __fmaf_rn(fs, r2, w);
-          }
+        const bool in0 = (k0 + u0 < n) && r2.x < rc2;
+        const bool in1 = (k0 + u1 < n) && r2.y < rc2;
+        const LjCoeff c0 = row[__float_as_int(xj[u0].w)];
+        const LjCoeff c1 = row[__float_as_int(xj[u1].w)];
+        float2 rr = make_float2(in0 ? r2.x : 1.0f, in1 ? r2.y : 1.0f);
+        if (kClamp) {
+          rr.x = fmaxf(rr.x, 0.49f * c0.sigma2);
+          rr.y = fmaxf(rr.y, 0.49f * c1.sigma2);
+        }
+        const float2 inv = make_float2(__fdividef(1.0f, rr.x), __fdividef(1.0f, rr.y));
+        const float2 sr2 = __fmul2_rn(make_float2(c0.sigma2, c1.sigma2), inv);
+        const float2 sr6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
+        const float2 sr12 = __fmul2_rn(sr6, sr6);
+        const float2 neg6 = make_float2(-sr6.x, -sr6.y);
+        const float2 g = __ffma2_rn(make_float2(2.0f, 2.0f), sr12, neg6);
+        float2 fs = __fmul2_rn(__fmul2_rn(make_float2(c0.eps24, c1.eps24), inv), g);
+        fs.x = in0 ? fs.x : 0.0f;
+        fs.y = in1 ? fs.y : 0.0f;
+        f2x = __ffma2_rn(fs, dx, f2x);
+        f2y = __ffma2_rn(fs, dy, f2y);
+        f2z = __ffma2_rn(fs, dz, f2z);
+        if (kObs) {
+          const float2 ep = __ffma2_rn(make_float2(c0.eps4, c1.eps4), __fadd2_rn(sr12, neg6),
+                                       make_float2(-c0.shift, -c1.shift));
+          e2 = __fadd2_rn(e2, make_float2(in0 ? ep.x : 0.0f, in1 ? ep.y : 0.0f));
+          w2 = __ffma2_rn(fs, rr, w2);
         }
       }
     }
+    fx = f2x.x + f2x.y;
+    fy = f2y.x + f2y.y;
+    fz = f2z.x + f2z.y;
+    e = e2.x + e2.y;
+    w = w2.x + w2.y;
   }
   v.force[i] = make_float4(fx, fy, fz, 0.f);
+  ReplicaState* st = &v.rs[r];
+  double ke = 0.0;
+  if (kPost) ke = post_slot<true, kKinetic>(v, p, st, i, real, fx, fy, fz);
   if (kObs) {
-    ReplicaState* st = &v.rs[r];
-    const long long ev = real ? to_fixed(0.5 * (double)e, &st->status) : 0ll;
-    const long long wv = real ? to_fixed(0.5 * (double)w, &st->status) : 0ll;
-    block_add_ll<kBlock>(ev, &st->acc[kAccPair]);
-    block_add_ll<kBlock>(wv, &st->acc[kAccVirial]);
+    block_add_lane<kBlock>(real, 0.5 * (double)e, st, kAccPair);
+    block_add_lane<kBlock>(real, 0.5 * (double)w, st, kAccVirial);
   }
+  if (kPost) post_finish<true, kObs, kKinetic>(v, p, st, r, real, ke);
 }
 
 // ---------------------------------------------------------------------------
@@ -715,14 +990,17 @@ __device__ V3 dihedral_term(const DeviceView& v, const ReplicaParams& p,
   }
 }
 
-template <bool kObs>
+template <bool kObs, int kMode>
 __global__ void __launch_bounds__(kBlock) k_bonded(DeviceView v) {
+  constexpr bool kPost = kMode >= kForcePost;
+  constexpr bool kKinetic = kMode == kForcePostKinetic || (kPost && kObs);
   const uint32_t b = blockIdx.x;
   const uint32_t r = v.block_replica[b];
   const ReplicaParams& p = v.rp[r];
   const uint32_t i = b * kBlock + threadIdx.x;
   const bool real = (i - p.atom_begin) < p.n_atoms;
   float eb = 0.f, ea = 0.f, ed = 0.f, w = 0.f;
+  float4 fo = make_float4(0.f, 0.f, 0.f, 0.f);
   if (real) {
     const uint32_t t = v.tag[i];
     const uint32_t e0 = v.term_off[t];
@@ -751,26 +1029,36 @@ __global__ void __launch_bounds__(kBlock) k_bonded(DeviceView v) {
         f.y += g.y;
         f.z += g.z;
       }
-      float4 fo = v.force[i];
+      fo = v.force[i];
       fo.x += f.x;
       fo.y += f.y;
       fo.z += f.z;
       v.force[i] = fo;
+    } else if (kPost) {
+      fo = v.force[i];
     }
   }
+  ReplicaState* st = &v.rs[r];
+  double ke = 0.0;
+  if (kPost) ke = post_slot<true, kKinetic>(v, p, st, i, real, fo.x, fo.y, fo.z);
   if (kObs) {
-    ReplicaState* st = &v.rs[r];
-    block_add_ll<kBlock>(real ? to_fixed(eb, &st->status) : 0ll, &st->acc[kAccBond]);
-    block_add_ll<kBlock>(real ? to_fixed(ea, &st->status) : 0ll, &st->acc[kAccAngle]);
-    block_add_ll<kBlock>(real ? to_fixed(ed, &st->status) : 0ll, &st->acc[kAccDihedral]);
-    block_add_ll<kBlock>(real ? to_fixed(w, &st->status) : 0ll, &st->acc[kAccVirial]);
+    block_add_lane<kBlock>(real, eb, st, kAccBond);
+    block_add_lane<kBlock>(real, ea, st, kAccAngle);
+    block_add_lane<kBlock>(real, ed, st, kAccDihedral);
+    block_add_lane<kBlock>(real, w, st, kAccVirial);
   }
+  if (kPost) post_finish<true, kObs, kKinetic>(v, p, st, r, real, ke);
 }
 
 // ---------------------------------------------------------------------------
 // post: second half-kick, kinetic energy (FP64 per slot, fixed-point total),
 // and per replica (last block): observables, Berendsen lambda for the next
-// step (applied lazily by pre), step counter.
+// step (applied lazily by pre), step counter.  The per-slot part and the
+// per-replica epilogue are shared by k_post and by the force kernels that
+// finish a step themselves (the last force kernel of a step holds the final
+// force of its slot in registers, so the kick needs no force re-read and no
+// extra launch).
+
 template <bool kKick, bool kObs, bool kKinetic>
 __global__ void __launch_bounds__(kBlock) k_post(DeviceView v) {
   const uint32_t b = blockIdx.x;
@@ -779,59 +1067,10 @@ __global__ void __launch_bounds__(kBlock) k_post(DeviceView v) {
   ReplicaState* st = &v.rs[r];
   const uint32_t i = b * kBlock + threadIdx.x;
   const bool real = (i - p.atom_begin) < p.n_atoms;
-  double ke = 0.0;
-  if (real) {
-    float4 vm = v.vel[i];
-    if (kKick) {
-      const float4 f = v.force[i];
-      const float h = __fdiv_rn(__fmul_rn(0.5f, p.dt), vm.w);
-      vm.x = __fmaf_rn(h, f.x, vm.x);
-      vm.y = __fmaf_rn(h, f.y, vm.y);
-      vm.z = __fmaf_rn(h, f.z, vm.z);
-      v.vel[i] = vm;
-      if (!isfinite(vm.x + vm.y + vm.z)) atomicOr(&st->status, kStatusNonFinite);
-    }
-    if (kKinetic || kObs) {
-      const double vx = vm.x, vy = vm.y, vz = vm.z;
-      ke = 0.5 * (double)vm.w * (vx * vx + vy * vy + vz * vz);
-    }
-  }
-  if (kKinetic || kObs) {
-    block_add_ll<kBlock>(real ? to_fixed(ke, &st->status) : 0ll,
-                         &st->acc[kAccKinetic]);
-  }
-  const uint32_t n_blocks = p.n_pad / kBlock;
-  if (arrive_last(&st->done_post, n_blocks) && threadIdx.x == 0) {
-    unsigned long long* acc = reinterpret_cast<unsigned long long*>(st->acc);
-    const double kin = from_fixed((long long)atomicExch(&acc[kAccKinetic], 0ull));
-    double lam = 1.0;
-    if (kKick && p.thermostat == 1 && kin > 0.0 && p.dof > 0.0) {
-      const double current = 2.0 * kin / p.dof;
-      const double arg = 1.0 + ((double)p.dt / p.tau) * (p.kt_target / current - 1.0);
-      lam = sqrt(arg > 0.0 ? arg : 0.0);
-    }
-    if (kKick) {
-      st->lambda = lam;
-      st->step += 1ull;
-    }
-    if (kObs) {
-      ReplicaObs o;
-      o.step = st->step;
-      o.pair_pe = from_fixed((long long)atomicExch(&acc[kAccPair], 0ull));
-      o.bond_pe = from_fixed((long long)atomicExch(&acc[kAccBond], 0ull));
-      o.angle_pe = from_fixed((long long)atomicExch(&acc[kAccAngle], 0ull));
-      o.dihedral_pe = from_fixed((long long)atomicExch(&acc[kAccDihedral], 0ull));
-      o.virial = from_fixed((long long)atomicExch(&acc[kAccVirial], 0ull));
-      o.ke_pre = kin;
-      o.lambda = lam;
-      o.builds = st->builds;
-      o.dangerous = st->dangerous;
-      o.status = st->status;
-      o.pad = 0;
-      v.obs[r] = o;
-    }
-    st->done_post = 0u;
-  }
+  float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (kKick && real) f = v.force[i];
+  const double ke = post_slot<kKick, kKinetic || kObs>(v, p, st, i, real, f.x, f.y, f.z);
+  post_finish<kKick, kObs, kKinetic || kObs>(v, p, st, r, real, ke);
 }
 
 // Applies the pending Berendsen scale so host reads see the scaled velocities.
@@ -951,33 +1190,55 @@ void launch_rebuild(const StepLaunch& l, bool force_all) {
     k_project_exclusions<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, 0);
     check_launch("project_exclusions");
   }
+  const uint32_t bg = (l.v.total_cells + kBuildWarps - 1) / kBuildWarps;
+#define BB_BUILD(cap)                                                          \
+  (l.all_regular ? k_build<cap, true><<<bg, kBlock, 0, l.stream>>>(l.v)        \
+                 : k_build<cap, false><<<bg, kBlock, 0, l.stream>>>(l.v))
   switch (l.excl_cap) {
-    case 0: k_build<0><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); break;
-    case 4: k_build<4><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); break;
-    case 8: k_build<8><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); break;
-    case 16: k_build<16><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); break;
-    case 32: k_build<32><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); break;
-    case 64: k_build<64><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); break;
+    case 0: BB_BUILD(0); break;
+    case 4: BB_BUILD(4); break;
+    case 8: BB_BUILD(8); break;
+    case 16: BB_BUILD(16); break;
+    case 32: BB_BUILD(32); break;
+    case 64: BB_BUILD(64); break;
     default: throw std::runtime_error("unsupported exclusion capacity");
   }
+#undef BB_BUILD
   check_launch("build");
 }
 
-void launch_forces(const StepLaunch& l, bool observables, bool clamp) {
-  if (clamp) {
-    k_lj<false, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post) {
+  const int fin = !post ? kForcePlain : (l.need_kinetic ? kForcePostKinetic : kForcePost);
+  const bool bonded = l.v.has_bonded != 0;
+  const int lj_mode = clamp ? kForceClamp : (bonded ? kForcePlain : fin);
+#define BB_LJ(obs, mode) k_lj<obs, mode><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v)
+  if (lj_mode == kForceClamp) {
+    BB_LJ(false, kForceClamp);
   } else if (observables) {
-    k_lj<true, false><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+    if (lj_mode == kForcePlain) BB_LJ(true, kForcePlain);
+    else BB_LJ(true, kForcePost);  // the kinetic total is part of the observables
   } else {
-    k_lj<false, false><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
-  }
-  check_launch("lj");
-  if (l.v.has_bonded) {
-    if (observables) {
-      k_bonded<true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
-    } else {
-      k_bonded<false><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+    switch (lj_mode) {
+      case kForcePlain: BB_LJ(false, kForcePlain); break;
+      case kForcePost: BB_LJ(false, kForcePost); break;
+      default: BB_LJ(false, kForcePostKinetic); break;
     }
+  }
+#undef BB_LJ
+  check_launch("lj");
+  if (bonded) {
+#define BB_BONDED(obs, mode) k_bonded<obs, mode><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v)
+    if (observables) {
+      if (fin == kForcePlain) BB_BONDED(true, kForcePlain);
+      else BB_BONDED(true, kForcePost);
+    } else {
+      switch (fin) {
+        case kForcePlain: BB_BONDED(false, kForcePlain); break;
+        case kForcePost: BB_BONDED(false, kForcePost); break;
+        default: BB_BONDED(false, kForcePostKinetic); break;
+      }
+    }
+#undef BB_BONDED
     check_launch("bonded");
   }
 }

@@ -17,6 +17,7 @@ struct StepLaunch {
   uint32_t max_cells_per_replica;
   uint32_t max_atoms_per_replica;
   int excl_cap;           // 0, 4, 8, 16, 32 or 64
+  int all_regular;        // every replica has >= 4 cells on every axis
   int need_kinetic;       // a thermostat is active in some replica
   float sd_dmax;          // descent: displacement cap
   float sd_fref;          // descent: force floor
@@ -27,7 +28,9 @@ struct StepLaunch {
 void launch_pre(const StepLaunch& l, int mode, cudaGraphConditionalHandle cond = 0,
                 bool use_cond = false);
 void launch_rebuild(const StepLaunch& l, bool force_all);
-void launch_forces(const StepLaunch& l, bool observables, bool clamp);
+// post: the last force kernel of the step also does the second half-kick,
+// the kinetic-energy total and the per-replica step epilogue (k_post's work).
+void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post = false);
 void launch_post(const StepLaunch& l, bool kick, bool observables);
 void launch_project_exclusions(const StepLaunch& l, bool force_all);
 void launch_apply_lambda(const StepLaunch& l);

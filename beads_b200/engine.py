@@ -61,6 +61,49 @@ class ReplicaSpec:
     def n(self) -> int:
         return int(np.asarray(self.positions).shape[0])
 
+    @classmethod
+    def from_spec(cls, spec: dict) -> "ReplicaSpec":
+        """The replica a ``Simulation._native_spec()`` dict describes."""
+        s, f, d, nb = spec["system"], spec["forcefield"], spec["dynamics"], spec["neighbor"]
+        nt = int(np.asarray(s["types"]).max())
+        eps = np.zeros((nt, nt))
+        sig = np.zeros((nt, nt))
+        for c in f["pair_coeffs"]:
+            a, b = c["type_i"] - 1, c["type_j"] - 1
+            eps[a, b] = eps[b, a] = c["params"]["epsilon"]
+            sig[a, b] = sig[b, a] = c["params"]["sigma"]
+        t = s["topology"]
+
+        def recs(items, keys):
+            return None if not items else np.array([[x[k] for k in keys] for x in items],
+                                                   np.uint32)
+
+        def coeffs(kind, key):
+            cs = f.get(f"{kind}_coeffs") or []
+            return [c["params"][key] for c in sorted(cs, key=lambda c: c["type"])] or None
+
+        thermo = d.get("thermostat")
+        return cls(
+            positions=np.asarray(s["positions"]), types=np.asarray(s["types"]),
+            box_bound=np.asarray(s["box_bound"]), epsilon=eps, sigma=sig,
+            cutoff=f["pair_style"]["params"]["cutoff"], dt=d["params"]["dt"], units=s["units"],
+            velocities=np.asarray(s["velocities"]), masses=np.asarray(s["masses"]),
+            tags=np.asarray(s["tags"]), molecule_ids=np.asarray(s["molecule_ids"]),
+            images=np.asarray(s["images"]),
+            shift=bool(f["pair_style"]["params"].get("shift", False)),
+            bonds=recs(t["bonds"], ("tag_i", "tag_j", "type")),
+            angles=recs(t["angles"], ("tag_i", "tag_j", "tag_k", "type")),
+            dihedrals=recs(t["dihedrals"], ("tag_i", "tag_j", "tag_k", "tag_l", "type")),
+            bond_k=coeffs("bond", "k"), bond_r0=coeffs("bond", "r0"),
+            angle_k=coeffs("angle", "k"), angle_theta0=coeffs("angle", "theta0"),
+            dihedral_k=coeffs("dihedral", "k"), dihedral_d=coeffs("dihedral", "d"),
+            dihedral_n=coeffs("dihedral", "n"),
+            exclusion_distance=f.get("bonded_exclusion_distance") or 0,
+            cutoff_buffer=nb["cutoff_buffer"], rebuild_check_every=nb["rebuild_check_every"],
+            sort_every_rebuild=nb["sort_every_rebuild"], max_neighbors=nb["max_neighbors"],
+            thermostat=None if thermo is None else (thermo["params"]["temperature"],
+                                                    thermo["params"]["tau"]))
+
 
 def _descriptors(spec: ReplicaSpec, keep: _lib.Keep):
     sd = _lib.SystemDesc()
@@ -216,13 +259,21 @@ class Engine:
         return {"n_replicas": nr.value, "n_particles": nt.value, "stream": st.value or 0}
 
     def profile(self, stage: str, reps: int) -> float:
-        """Mean milliseconds per launch of 'forces', 'step' or 'rebuild'."""
-        code = {"forces": 0, "step": 1, "rebuild": 2}[stage]
+        """Mean milliseconds per launch of 'forces', 'step', 'rebuild' or
+        'forces_kick' (the force kernel as a step runs it, with the second
+        half-kick; velocities and step state are restored afterwards)."""
+        code = {"forces": 0, "step": 1, "rebuild": 2, "forces_kick": 3}[stage]
         out = ctypes.c_double()
         _lib.check(self._lib.beads_profile(self._h, code, int(reps), ctypes.byref(out)))
         if code == 1:
             self.step += int(reps)
         return out.value
+
+    def counters(self, replica: int = 0) -> dict:
+        """Completed steps, neighbour builds and dangerous rebuilds."""
+        out = (ctypes.c_uint64 * 3)()
+        _lib.check(self._lib.beads_counters(self._h, int(replica), out))
+        return {"steps": int(out[0]), "builds": int(out[1]), "dangerous": int(out[2])}
 
     def list_stats(self) -> dict:
         total = ctypes.c_uint64()

@@ -118,36 +118,52 @@ def polymer_melt(n_chains: int = 2000, beads: int = 200, density: float = 0.85, 
 
     def clash(p):
         kx, ky, kz = key(p)
-        for dx in (-1, 0, 1):
-            for dy in (-1, 0, 1):
-                for dz in (-1, 0, 1):
-                    for j in grid.get(((kx + dx) % ncell, (ky + dy) % ncell, (kz + dz) % ncell), ()):
-                        d = p - pos[j]
-                        d -= length * np.round(d / length)
-                        if d @ d < reject * reject:
-                            return True
-        return False
+        near = [j for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1)
+                for j in grid.get(((kx + dx) % ncell, (ky + dy) % ncell, (kz + dz) % ncell), ())]
+        if not near:
+            return False
+        d = p - pos[near]
+        d -= length * np.round(d / length)
+        return bool(((d * d).sum(axis=1) < reject * reject).any())
 
+    def place(p, at):
+        pos[at] = p
+        grid.setdefault(key(p), []).append(at)
+
+    def unplace(at):
+        grid[key(pos[at])].remove(at)
+
+    # Every bead keeps at least `reject` from every bead placed before it.  A
+    # walk that finds no free direction in 200 tries backs off a few beads;
+    # after 50 back-offs the chain restarts from a new random point.
     idx = 0
     for _ in range(n_chains):
-        while True:
-            p = rng.uniform(0.0, length, 3)
-            if not clash(p):
-                break
-        for b in range(beads):
-            if b > 0:
-                for _attempt in range(200):
-                    u = rng.standard_normal(3)
-                    u /= np.linalg.norm(u)
-                    cand = np.mod(pos[idx - 1] + step * u, length)
-                    if not clash(cand):
-                        p = cand
+        start, backoffs = idx, 0
+        while idx < start + beads:
+            if idx == start:
+                while True:
+                    p = rng.uniform(0.0, length, 3)
+                    if not clash(p):
                         break
-                else:
-                    p = np.mod(pos[idx - 1] + step * u, length)
-            pos[idx] = p
-            grid.setdefault(key(p), []).append(idx)
-            idx += 1
+                place(p, idx)
+                idx += 1
+                continue
+            for _attempt in range(200):
+                u = rng.standard_normal(3)
+                u /= np.linalg.norm(u)
+                cand = np.mod(pos[idx - 1] + step * u, length)
+                if not clash(cand):
+                    place(cand, idx)
+                    idx += 1
+                    break
+            else:
+                backoffs += 1
+                back = idx - start if backoffs > 50 else min(idx - start - 1, 4)
+                if backoffs > 50:
+                    backoffs = 0
+                for _k in range(back):
+                    idx -= 1
+                    unplace(idx)
     lo = np.zeros(3)
     hi = np.full(3, length)
     posf = _inside(pos, lo, hi)

@@ -288,17 +288,24 @@ def run_ours(args) -> None:
             dist.barrier()
         torch.cuda.synchronize()
 
+    builds_before = eng.counters()["builds"]
+    profile_region = os.environ.get("BEADS_PROFILE_TIMED") == "1"
     sampler = ClockSampler(local)
     barrier()
     sampler.start()
+    if profile_region:  # lets a profiler started with capture off see only these steps
+        torch.cuda.profiler.start()
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     start.record(stream)
     eng.run(args.steps)
     stop.record(stream)
     stop.synchronize()
+    if profile_region:
+        torch.cuda.profiler.stop()
     barrier()
     clocks = sampler.stop()
+    timed_builds = eng.counters()["builds"] - builds_before
     elapsed_ms = start.elapsed_time(stop)
     if dist is not None:
         t = torch.tensor([elapsed_ms], device="cuda")
@@ -306,10 +313,12 @@ def run_ours(args) -> None:
         elapsed_ms = float(t.item())
     value = world * spec.n * args.steps / (elapsed_ms / 1e3)
 
-    # Dominant kernel: LJ pair forces, timed alone on the engine stream.
-    force_ms = eng.profile("forces", 50)
+    # Dominant kernel: LJ pair forces with the fused second half-kick, as a
+    # step launches it, timed alone on the engine stream.
+    force_ms = eng.profile("forces_kick", 50)
     step_ms_alone = elapsed_ms / args.steps
-    bytes_per_atom = 4.0 * mean_nbr + 36.0  # list + own pos + count + force write
+    # list + own position + count + force write + velocity read and write
+    bytes_per_atom = 4.0 * mean_nbr + 68.0
     achieved = spec.n * bytes_per_atom / (force_ms / 1e3) / 1e9
     peak, peak_kind = _peaks()
     traffic = _traffic_from_profile()
@@ -347,7 +356,9 @@ def run_ours(args) -> None:
         st = eng.state()
         cpu = _cpu_baseline(st["positions"], spec, args.cpu_budget)
 
-    launches_per_step = 10  # pre, 7 rebuild-chain kernels, forces, post
+    # Every step launches pre and the fused force kernel; a step that rebuilds
+    # also runs the 7 kernels of the rebuild chain (conditional graph node).
+    gpu_launches = 2 * args.steps + 7 * int(timed_builds)
     line = {
         "metric": METRIC,
         "value": value,
@@ -368,10 +379,11 @@ def run_ours(args) -> None:
             "l2": "inputs larger than L2 (list ~4*mean_nbr*N bytes + state)",
             "mean_neighbors": round(mean_nbr, 2),
             "max_neighbors_seen": stats["max"],
+            "neighbor_builds_timed": int(timed_builds),
         },
         "roofline": {
             "bound": "hbm",
-            "kernel": "k_lj (pair forces)",
+            "kernel": "k_lj (pair forces + second half-kick)",
             "achieved": achieved,
             "peak": peak,
             "unit": "GB/s",
@@ -383,7 +395,7 @@ def run_ours(args) -> None:
         },
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "md_steps_per_call": E2E_STEPS},
-        "gpu_launches": launches_per_step * args.steps,
+        "gpu_launches": gpu_launches,
         "clocks": clocks,
     }
     if cpu is not None:
@@ -393,6 +405,90 @@ def run_ours(args) -> None:
     eng.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+REPLICA_METRIC = ("atom-steps/s on 1 B200 (512-replica batch of uneven LJ systems in one launch "
+                  "per kernel, FP32 pair math, fixed-point totals)")
+
+
+def run_replicas(args) -> None:
+    """The 512-replica batch: uneven single-type LJ replicas (sizes seeded
+    log-uniform in [256, 32768], density U[0.7, 0.9], Berendsen target T
+    U[0.8, 1.5] tau 1, rc 2.5, dt 0.005) stepped together, beside the same
+    replicas run one at a time through the same engine."""
+    import torch
+
+    from beads_b200 import workloads
+    from beads_b200.engine import Engine
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    specs = workloads.replica_batch(args.replicas, seed=7 + rank)
+    atoms = sum(s.n for s in specs)
+    eng = Engine(specs)
+    stream = torch.cuda.ExternalStream(eng.info()["stream"], device=torch.device("cuda", local))
+    eng.run(max(3, args.warmup))
+    builds_before = sum(eng.counters(r)["builds"] for r in range(len(specs)))
+    sampler = ClockSampler(local)
+    torch.cuda.synchronize()
+    sampler.start()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    eng.run(args.steps)
+    stop.record(stream)
+    stop.synchronize()
+    clocks = sampler.stop()
+    batch_ms = start.elapsed_time(stop)
+    builds = sum(eng.counters(r)["builds"] for r in range(len(specs))) - builds_before
+    value = atoms * args.steps / (batch_ms / 1e3)
+    eng.close()
+
+    # The same replicas one at a time (one engine each, same kernels), every
+    # replica for `seq_steps` steps after warm-up; the sequential rate is the
+    # total atom-steps over the summed device time.
+    seq_steps = max(10, min(args.steps, 200))
+    seq_ms = 0.0
+    for spec in specs:
+        with Engine(spec) as one:
+            one.run(3)
+            s1 = torch.cuda.ExternalStream(one.info()["stream"],
+                                           device=torch.device("cuda", local))
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(s1)
+            one.run(seq_steps)
+            b.record(s1)
+            b.synchronize()
+            seq_ms += a.elapsed_time(b)
+    seq_value = atoms * seq_steps / (seq_ms / 1e3)
+    line = {
+        "metric": REPLICA_METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": batch_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"{len(specs)} LJ replicas, {atoms} beads in total, sizes log-uniform "
+                        "[256, 32768], rho U[0.7, 0.9], Berendsen T U[0.8, 1.5], rc 2.5, skin 0.3",
+            "parallelism": "replicas in one batch",
+            "sequential_value": seq_value,
+            "sequential_steps_per_replica": seq_steps,
+            "batch_over_sequential": value / seq_value,
+            "neighbor_builds_timed": int(builds),
+        },
+        "gpu_launches": 2 * args.steps + 7 * int(builds),
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line))
 
 
 def main() -> None:
@@ -407,6 +503,10 @@ def main() -> None:
                         help="seconds of host work for the whole reference arm")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    parser.add_argument("--workload", default="mixture", choices=["mixture", "replicas"],
+                        help="mixture: the 1M-bead mixture (default); replicas: the "
+                             "512-replica batch beside one-at-a-time runs")
+    parser.add_argument("--replicas", type=int, default=512)
     parser.add_argument("--beads", type=int, default=N_BEADS,
                         help="system size (same density); profiling of small cases only")
     args = parser.parse_args()
@@ -414,6 +514,8 @@ def main() -> None:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "replicas":
+        run_replicas(args)
     else:
         run_ours(args)
 

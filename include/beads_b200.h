@@ -255,13 +255,21 @@ BEADS_API int beads_ctx_info(beads_ctx* ctx, uint32_t* n_replicas,
  * with CUDA events (synchronized on both sides) and returns the mean duration
  * per launch in milliseconds.  stage 0: pair + bonded forces on the current
  * list (no observables); 1: one full MD step; 2: one forced neighbour
- * rebuild.  Stages 1 and 2 advance or rebuild the state they time. */
+ * rebuild; 3: the force kernels as a step launches them (with the second
+ * half-kick and the kinetic-energy total), velocities and per-replica step
+ * state restored afterwards.  Stages 1 and 2 advance or rebuild the state
+ * they time. */
 BEADS_API int beads_profile(beads_ctx* ctx, int32_t stage, uint32_t reps,
                             double* avg_ms);
 /* Neighbour-list statistics of the last build over all replicas: total list
  * entries and the largest per-particle count. */
 BEADS_API int beads_list_stats(beads_ctx* ctx, uint64_t* total_entries,
                                uint32_t* max_count);
+
+/* Device counters of one replica, without stepping it: counters[0] completed
+ * MD steps, [1] neighbour builds, [2] dangerous rebuilds (the quantities the
+ * reference's run log reports, log_output.cpp:370-404). */
+BEADS_API int beads_counters(beads_ctx* ctx, uint32_t replica, uint64_t* counters);
 
 /* Steepest descent with a per-particle displacement cap, used to relax
  * random initial configurations: x += dmax * F / max(|F|, fref), with the LJ

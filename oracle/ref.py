@@ -97,6 +97,10 @@ def run(precision: str, spec: dict, workdir: pathlib.Path, timeout: float = 1800
 def main(argv: list[str]) -> None:
     precision, jp, npz, workdir = argv
     spec = load_spec(pathlib.Path(jp), pathlib.Path(npz))
+    if precision == "f64":
+        # The double build takes float64 reals; the float32 inputs convert exactly.
+        for key in ("box_bound", "positions", "velocities", "masses"):
+            spec["system"][key] = np.ascontiguousarray(spec["system"][key], dtype=np.float64)
     mod = _load(precision)
     os.chdir(workdir)
     mod.execute_simulation(spec)

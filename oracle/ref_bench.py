@@ -50,9 +50,9 @@ def _relaxed_mixture(n: int):
 def main(argv: list[str]) -> None:
     out_path = pathlib.Path(argv[0])
     quick = "--quick" in argv
-    cases = [("lattice_4096", workloads.lj_lattice(n_side=16), 1000)]
+    cases = [("lattice_4096", workloads.lj_lattice(n_side=16), 5000)]
     n_mix = 131072 if quick else 1_048_576
-    cases.append((f"mixture_{n_mix}", _relaxed_mixture(n_mix), 200 if quick else 500))
+    cases.append((f"mixture_{n_mix}", _relaxed_mixture(n_mix), 200 if quick else 2000))
     results = {}
     for name, r, steps in cases:
         spec = spec_for(r, steps, "run", forces=False, thermo_every=steps)

@@ -11,7 +11,7 @@ the reference's ``_native.execute_simulation`` twice per precision:
   * a short dynamics run: thermo rows, final state, neighbour build counts
     (from the reference's log).
 
-    python tests/golden/make_reference_fixtures.py <output dir>
+    python tests/golden/make_reference_fixtures.py <output dir> [case ...]
 """
 
 from __future__ import annotations
@@ -100,7 +100,7 @@ def cases() -> dict:
     rng = np.random.default_rng(13)
     mixture.positions = workloads._inside((g + 0.5) * a + rng.uniform(-0.02, 0.02, g.shape),
                                           np.zeros(3), np.full(3, side * a))
-    chains = workloads.polymer_melt(n_chains=27, beads=16, seed=17, max_neighbors=64)
+    chains = workloads.polymer_melt(n_chains=27, beads=16, seed=17, max_neighbors=128)
     return {"lattice": (lattice, 200, 20), "mixture": (mixture, 200, 20),
             "chains": (chains, 100, 10)}
 
@@ -115,10 +115,12 @@ def _log_value(text: str, key: str) -> str:
     return m.group(1).strip() if m else ""
 
 
-def main(out_dir: str) -> None:
+def main(out_dir: str, only: list[str]) -> None:
     out = pathlib.Path(out_dir)
     out.mkdir(parents=True, exist_ok=True)
     for name, (r, steps, every) in cases().items():
+        if only and name not in only:
+            continue
         fixture: dict = {}
         spec0 = spec_for(r, 0, "zero", forces=True, thermo_every=1)
         ref.save_spec(spec0, out / f"ref_{name}_spec.json", out / f"ref_{name}_spec.npz")
@@ -157,4 +159,4 @@ def main(out_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1])
+    main(sys.argv[1], sys.argv[2:])
