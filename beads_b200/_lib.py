@@ -158,6 +158,11 @@ EXPORTED = (
     "beads_profile",
     "beads_list_stats",
     "beads_counters",
+    "beads_set_tuning",
+    "beads_get_tuning",
+    "beads_set_lj",
+    "beads_adjoint_forward",
+    "beads_adjoint_backward",
     "beads_cell_sort_static",
     "beads_debug_cells",
     "beads_debug_neighbors",
@@ -202,6 +207,11 @@ def load():
     L.beads_profile.argtypes = [vp, ctypes.c_int32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]
     L.beads_list_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint32)]
     L.beads_counters.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)]
+    L.beads_set_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+    L.beads_get_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+    L.beads_set_lj.argtypes = [vp, ctypes.c_uint32, vp, vp]
+    L.beads_adjoint_forward.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, vp]
+    L.beads_adjoint_backward.argtypes = [vp, vp, vp, vp, vp, vp]
     L.beads_cell_sort_static.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float),
                                          ctypes.POINTER(ctypes.c_float), ctypes.c_double,
                                          ctypes.c_double, vp, vp, vp, ctypes.c_uint32,

@@ -1,0 +1,637 @@
+// adjoint.cu -- reverse-mode gradients of a velocity-Verlet trajectory.
+//
+// Forward step n -> n+1 as the engine runs it (Berendsen scale lambda_n is
+// applied lazily by the next step's first kernel):
+//   u      = lambda_n v_n + (dt/2m) F(x_n)
+//   x_n+1  = x_n + dt u
+//   v_n+1  = u + (dt/2m) F(x_n+1)
+//   K_n+1  = 1/2 sum m v_n+1^2,  lambda_n+1 = g(K_n+1)
+//          = sqrt(max(0, 1 + dt/tau (kT0 dof / (2 K) - 1)))
+// with observables PE(x_n), W(x_n) (virial sum r.F) and KE_n = lambda_n^2 K_n.
+//
+// Walking back over step m (m = T .. 0), with u_bar_m+1 the adjoint of the
+// next step's pre-kick velocity (0 after the last step):
+//   K_bar = g_KE lambda^2 + (sum u_bar_m+1 . v_m + g_KE 2 lambda K) g'(K)
+//   v_bar = lambda u_bar_m+1 + K_bar m v_m
+//   F_bar = (dt/2m) (u_bar_m+1 + v_bar)        (m = 0: (dt/2m) u_bar_1)
+//   x_bar += g_PE grad PE + g_W grad W + J(x_m) F_bar,  J = dF/dx (symmetric)
+//   u_bar_m = v_bar + dt x_bar
+// and the parameter adjoints collect F_bar . dF/dtheta + g_PE dPE/dtheta +
+// g_W dW/dtheta.  For a pair with d = x_i - x_j and phi = F_ij / d (so that
+// F_i = sum_j phi d), A_ij = phi I + (phi'/r) d d^T and
+//   (J F_bar)_i = sum_j A_ij (F_bar_i - F_bar_j)
+// over the full neighbour list: every particle gathers, no atomics.
+//
+// The neighbour list of each replayed step is the one the forward step used:
+// it is rebuilt (deterministically, slots never reorder during an adjoint
+// run) from the positions of that step's last build.
+#include "adjoint.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "device_util.cuh"
+#include "engine.hpp"
+#include "kernels.cuh"
+
+namespace bb {
+
+AdjointStore::~AdjointStore() {
+  for (void* p : allocations) cudaFree(p);
+}
+
+template <typename T>
+T* AdjointStore::alloc(size_t count) {
+  void* p = nullptr;
+  cuda_check(cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(T)), "cudaMalloc (adjoint)");
+  allocations.push_back(p);
+  cuda_check(cudaMemset(p, 0, std::max<size_t>(1, count) * sizeof(T)), "cudaMemset (adjoint)");
+  return static_cast<T*>(p);
+}
+
+namespace {
+
+constexpr int kAdjTypes = 4;  // largest LJ table side the adjoint supports
+
+// Device view of the adjoint store.
+struct AdjView {
+  float4* seg_pos;
+  float4* seg_vel;
+  const double* seg_lam;
+  const double* seg_kin;
+  float4* xbar;
+  float4* vbar;
+  float4* fbar;
+  float4* ubar;
+  const double* obs_grad;
+  long long* theta;
+  const float4* ck_ref_pos;
+  const int* list_src;   // per replica: -1 checkpoint build positions, else step index
+  const int* shift_on;   // per replica: LJ energy shift active
+  uint32_t slots;
+  uint32_t replicas;
+};
+
+__global__ void k_adj_record(DeviceView v, double* lam, double* kin, uint32_t* flags,
+                             uint32_t k) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= v.n_replicas) return;
+  const ReplicaState& st = v.rs[r];
+  lam[(size_t)k * v.n_replicas + r] = st.lambda;
+  kin[(size_t)k * v.n_replicas + r] = st.last_kinetic;
+  flags[(size_t)k * v.n_replicas + r] = st.need_rebuild;
+}
+
+// Positions from which each replica's list of the current replayed step was
+// built, and the rebuild flags for the replicas whose list changes.
+__global__ void k_adj_list_positions(DeviceView v, AdjView a, uint32_t segment,
+                                     const uint32_t* changed) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const uint32_t i = b * kBlock + threadIdx.x;
+  if (threadIdx.x == 0 && (i - v.rp[r].atom_begin) == 0u) {
+    v.rs[r].need_rebuild = changed[r];
+    v.rs[r].reorder_now = 0u;
+  }
+  if (!changed[r]) return;
+  const int src = a.list_src[r];
+  v.pos[i] = src < 0 ? a.ck_ref_pos[(size_t)segment * a.slots + i]
+                     : a.seg_pos[(size_t)src * a.slots + i];
+}
+
+__global__ void k_adj_mark_all(DeviceView v) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= v.n_replicas) return;
+  v.rs[r].need_rebuild = 1u;
+  v.rs[r].reorder_now = 0u;
+}
+
+// Step m, part 1: kinetic-energy and Berendsen adjoints, v_bar, F_bar.
+// Reads the sum u_bar_m+1 . v_m from accumulator lane `lane_in` (written by
+// the pair kernel of step m+1) and clears it in its last block.
+__global__ void __launch_bounds__(kBlock)
+k_adj_prepare(DeviceView v, AdjView a, uint32_t m, uint32_t k, int first, int last,
+              int lane_in) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const ReplicaParams& p = v.rp[r];
+  ReplicaState* st = &v.rs[r];
+  const uint32_t i = b * kBlock + threadIdx.x;
+  const bool real = (i - p.atom_begin) < p.n_atoms;
+  const double lam = a.seg_lam[(size_t)k * v.n_replicas + r];
+  const double kin = a.seg_kin[(size_t)k * v.n_replicas + r];
+  const double g_ke = a.obs_grad[((size_t)m * v.n_replicas + r) * 3 + 2];
+  const double dot = last ? 0.0 : from_fixed(st->acc[lane_in], st->acc_frac[lane_in]);
+  double gp = 0.0;
+  if (!first && p.thermostat == 1 && kin > 0.0 && p.dof > 0.0 && lam > 0.0) {
+    const double c = (double)p.dt / p.tau;
+    const double big_a = 0.5 * p.kt_target * p.dof;
+    gp = c * (-big_a / (kin * kin)) / (2.0 * lam);
+  }
+  const double k_bar = g_ke * lam * lam + (dot + g_ke * 2.0 * lam * kin) * gp;
+  if (real) {
+    const float4 vel = a.seg_vel[(size_t)k * a.slots + i];
+    const float4 u = last ? make_float4(0.f, 0.f, 0.f, 0.f) : a.ubar[i];
+    const float l = (float)lam;
+    const float km = (float)(k_bar * (double)vel.w);
+    float4 vb;
+    vb.x = __fmaf_rn(l, u.x, km * vel.x);
+    vb.y = __fmaf_rn(l, u.y, km * vel.y);
+    vb.z = __fmaf_rn(l, u.z, km * vel.z);
+    vb.w = 0.f;
+    const float h = __fdiv_rn(__fmul_rn(0.5f, p.dt), vel.w);
+    float4 fb;
+    if (first) {
+      fb = make_float4(h * u.x, h * u.y, h * u.z, 0.f);
+    } else {
+      fb = make_float4(h * (u.x + vb.x), h * (u.y + vb.y), h * (u.z + vb.z), 0.f);
+    }
+    a.vbar[i] = vb;
+    a.fbar[i] = fb;
+  }
+  const uint32_t n_blocks = p.n_pad / kBlock;
+  if (arrive_last(&st->done_post, n_blocks) && threadIdx.x == 0) {
+    st->acc[lane_in] = 0;
+    st->acc_frac[lane_in] = 0;
+    st->done_post = 0u;
+  }
+}
+
+__device__ __forceinline__ void add_typed(float (&acc)[kAdjTypes], int t, float v) {
+#pragma unroll
+  for (int c = 0; c < kAdjTypes; ++c) acc[c] += (c == t) ? v : 0.0f;
+}
+
+// Step m, part 2: x_bar += g_PE grad PE + g_W grad W + J F_bar over the LJ
+// pairs, parameter adjoints, then u_bar_m and the sum u_bar_m . v_m-1 (lane
+// `lane_out`).  Positions in v.pos are x_m.
+__global__ void __launch_bounds__(kBlock)
+k_adj_lj(DeviceView v, AdjView a, uint32_t m, uint32_t k, int first, int lane_out) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const ReplicaParams& p = v.rp[r];
+  ReplicaState* st = &v.rs[r];
+  __shared__ LjCoeff table[kAdjTypes * kAdjTypes];
+  __shared__ unsigned long long theta_sh[kAdjTypes * kAdjTypes * 2 * 2];
+  const int nt = p.n_types;
+  for (int t = threadIdx.x; t < nt * nt; t += kBlock) table[t] = v.lj[p.lj_offset + t];
+  for (int t = threadIdx.x; t < kAdjTypes * kAdjTypes * 4; t += kBlock) theta_sh[t] = 0ull;
+  __syncthreads();
+
+  const uint32_t i = b * kBlock + threadIdx.x;
+  const bool real = (i - p.atom_begin) < p.n_atoms;
+  const float g_pe = (float)a.obs_grad[((size_t)m * v.n_replicas + r) * 3 + 0];
+  const float g_w = (float)a.obs_grad[((size_t)m * v.n_replicas + r) * 3 + 1];
+  const bool shift_on = a.shift_on[r] != 0;
+  float gx = 0.f, gy = 0.f, gz = 0.f;
+  float te[kAdjTypes], ts[kAdjTypes];
+#pragma unroll
+  for (int c = 0; c < kAdjTypes; ++c) te[c] = ts[c] = 0.f;
+  const float4 xi = v.pos[i];
+  const int ti = __float_as_int(xi.w);
+  if (real) {
+    const float4 fi = a.fbar[i];
+    const uint32_t n = v.nbr_count[i];
+    const uint32_t* list = v.nbr + nbr_index(i, 0, v.nbr_stride);
+    const float rc2 = p.force_cut_sq;
+    for (uint32_t q = 0; q < n; ++q) {
+      const uint32_t j = list[(size_t)q * kGroup];
+      const float4 xj = v.pos[j];
+      const float dx = acc_delta(xi.x, xj.x, p.len[0], p.half[0]);
+      const float dy = acc_delta(xi.y, xj.y, p.len[1], p.half[1]);
+      const float dz = acc_delta(xi.z, xj.z, p.len[2], p.half[2]);
+      const float r2 = norm2(dx, dy, dz);
+      if (!(r2 < rc2)) continue;
+      const int tj = __float_as_int(xj.w);
+      const LjCoeff c = table[ti * nt + tj];
+      const float inv = 1.0f / r2;
+      const float sr2 = c.sigma2 * inv;
+      const float sr6 = sr2 * sr2 * sr2;
+      const float sr12 = sr6 * sr6;
+      const float phi = c.eps24 * inv * (2.0f * sr12 - sr6);
+      const float psi = 4.0f * c.eps24 * inv * inv * (2.0f * sr6 - 7.0f * sr12);
+      const float4 fj = a.fbar[j];
+      const float ddx = fi.x - fj.x, ddy = fi.y - fj.y, ddz = fi.z - fj.z;
+      const float d_dot = dx * ddx + dy * ddy + dz * ddz;
+      const float coef = psi * d_dot - g_pe * phi + g_w * (psi * r2 + 2.0f * phi);
+      gx += phi * ddx + coef * dx;
+      gy += phi * ddy + coef * dy;
+      gz += phi * ddz + coef * dz;
+      // Parameter adjoints of this ordered pair (the pair's PE and W are
+      // split half and half between its two ordered entries).
+      const float fd = fi.x * dx + fi.y * dy + fi.z * dz;
+      const float eps = 0.25f * c.eps4;
+      const float sig = sqrtf(c.sigma2);
+      const float u = c.eps4 * (sr12 - sr6) - c.shift;
+      const float w = phi * r2;
+      const float d_eps = eps != 0.0f ? (phi * fd + 0.5f * g_pe * u + 0.5f * g_w * w) / eps : 0.0f;
+      float dshift = 0.0f;
+      if (shift_on) {
+        const float sc2 = c.sigma2 / rc2;
+        const float sc6 = sc2 * sc2 * sc2;
+        dshift = c.eps4 * (12.0f * sc6 * sc6 - 6.0f * sc6) / sig;
+      }
+      const float dphi = c.eps24 * inv * (24.0f * sr12 - 6.0f * sr6) / sig;
+      const float du = c.eps4 * (12.0f * sr12 - 6.0f * sr6) / sig - dshift;
+      const float dw = c.eps24 * (24.0f * sr12 - 6.0f * sr6) / sig;
+      const float d_sig = dphi * fd + 0.5f * g_pe * du + 0.5f * g_w * dw;
+      add_typed(te, tj, d_eps);
+      add_typed(ts, tj, d_sig);
+    }
+  }
+  double dot = 0.0;
+  if (real) {
+    float4 xb = a.xbar[i];
+    xb.x += gx;
+    xb.y += gy;
+    xb.z += gz;
+    a.xbar[i] = xb;
+    if (!first) {
+      const float4 vb = a.vbar[i];
+      const float4 ub = make_float4(__fmaf_rn(p.dt, xb.x, vb.x), __fmaf_rn(p.dt, xb.y, vb.y),
+                                    __fmaf_rn(p.dt, xb.z, vb.z), 0.f);
+      a.ubar[i] = ub;
+      const float4 vp = a.seg_vel[(size_t)(k - 1) * a.slots + i];
+      dot = (double)ub.x * vp.x + (double)ub.y * vp.y + (double)ub.z * vp.z;
+    }
+  }
+  if (!first) block_add_lane<kBlock>(real, dot, st, lane_out);
+  if (real) {
+    for (int c = 0; c < nt; ++c) {
+      const int slot = (ti * kAdjTypes + c) * 2;
+      const Fixed fe = to_fixed((double)te[c], &st->status);
+      const Fixed fs = to_fixed((double)ts[c], &st->status);
+      atomicAdd(&theta_sh[(slot + 0) * 2 + 0], (unsigned long long)fe.whole);
+      atomicAdd(&theta_sh[(slot + 0) * 2 + 1], (unsigned long long)fe.frac);
+      atomicAdd(&theta_sh[(slot + 1) * 2 + 0], (unsigned long long)fs.whole);
+      atomicAdd(&theta_sh[(slot + 1) * 2 + 1], (unsigned long long)fs.frac);
+    }
+  }
+  __syncthreads();
+  unsigned long long* out =
+      reinterpret_cast<unsigned long long*>(a.theta) + (size_t)r * kAdjTypes * kAdjTypes * 4;
+  for (int t = threadIdx.x; t < kAdjTypes * kAdjTypes * 4; t += kBlock) {
+    if (theta_sh[t] != 0ull) atomicAdd(&out[t], theta_sh[t]);
+  }
+}
+
+// Tag-order copy of a per-slot adjoint vector.
+__global__ void k_adj_gather(DeviceView v, const float4* src, float* dst, uint32_t n_tags) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_tags) return;
+  const float4 x = src[v.slot_of_tag[t]];
+  dst[3 * (size_t)t] = x.x;
+  dst[3 * (size_t)t + 1] = x.y;
+  dst[3 * (size_t)t + 2] = x.z;
+}
+
+void launch_check(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    throw std::runtime_error(std::string("CUDA launch of ") + what + " failed: " +
+                             cudaGetErrorString(e));
+  }
+}
+
+}  // namespace
+
+void Engine::set_lj(uint32_t replica, const double* eps, const double* sigma) {
+  const ReplicaHost& h = rep_.at(replica);
+  const int nt = h.n_types;
+  std::vector<LjCoeff> table(static_cast<size_t>(nt) * nt);
+  const float rc = static_cast<float>(h.lj_cutoff);
+  for (int i = 0; i < nt; ++i) {
+    for (int j = 0; j < nt; ++j) {
+      const double e = eps[i * nt + j], s = sigma[i * nt + j];
+      if (!(e >= 0.0) || !(s > 0.0) || !std::isfinite(e) || !std::isfinite(s)) {
+        throw InvalidArgument("LJ epsilon must be >= 0 and sigma > 0.");
+      }
+      if (eps[i * nt + j] != eps[j * nt + i] || sigma[i * nt + j] != sigma[j * nt + i]) {
+        throw InvalidArgument("LJ tables must be symmetric.");
+      }
+      LjCoeff c;
+      const float sig = static_cast<float>(s);
+      c.sigma2 = sig * sig;
+      c.eps4 = 4.0f * static_cast<float>(e);
+      c.eps24 = 6.0f * c.eps4;
+      c.shift = 0.0f;
+      if (h.lj_shift) {
+        const float sr2 = c.sigma2 / (rc * rc);
+        const float sr6 = sr2 * sr2 * sr2;
+        c.shift = c.eps4 * (sr6 * sr6 - sr6);
+      }
+      table[static_cast<size_t>(i) * nt + j] = c;
+    }
+  }
+  sync();
+  cuda_check(cudaMemcpy(const_cast<LjCoeff*>(v_.lj) + h.lj_offset, table.data(),
+                        table.size() * sizeof(LjCoeff), cudaMemcpyHostToDevice),
+             "LJ table upload");
+  initialized_ = false;  // forces of the current state are stale
+}
+
+void Engine::adjoint_record(uint32_t k) {
+  AdjointStore& A = *adj_;
+  const size_t S = A.slots;
+  cuda_check(cudaMemcpyAsync(A.seg_pos + k * S, v_.pos, S * sizeof(float4),
+                             cudaMemcpyDeviceToDevice, stream_), "adjoint record");
+  cuda_check(cudaMemcpyAsync(A.seg_vel + k * S, v_.vel, S * sizeof(float4),
+                             cudaMemcpyDeviceToDevice, stream_), "adjoint record");
+  k_adj_record<<<(A.replicas + 127) / 128, 128, 0, stream_>>>(v_, A.seg_lam, A.seg_kin,
+                                                               A.seg_flags, k);
+  launch_check("adjoint record");
+}
+
+// Puts the particle state of checkpoint c back, with the neighbour list the
+// forward run had at that point (rebuilt from its build positions).
+void Engine::adjoint_restore(uint32_t c) {
+  AdjointStore& A = *adj_;
+  const size_t S = A.slots;
+  auto d2d = [&](void* dst, const void* src, size_t bytes) {
+    cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream_),
+               "adjoint restore");
+  };
+  d2d(v_.pos, A.ck_ref_pos + c * S, S * sizeof(float4));
+  d2d(v_.img, A.ck_ref_img + c * S, S * sizeof(int4));
+  k_adj_mark_all<<<(A.replicas + 127) / 128, 128, 0, stream_>>>(v_);
+  launch_check("adjoint mark");
+  launch_rebuild(launch_, false);
+  d2d(v_.pos, A.ck_pos + c * S, S * sizeof(float4));
+  d2d(v_.vel, A.ck_vel + c * S, S * sizeof(float4));
+  d2d(v_.img, A.ck_img + c * S, S * sizeof(int4));
+  d2d(v_.ref_pos, A.ck_ref_pos + c * S, S * sizeof(float4));
+  d2d(v_.ref_img, A.ck_ref_img + c * S, S * sizeof(int4));
+  cuda_check(cudaMemcpyAsync(v_.rs, A.ck_state.data() + static_cast<size_t>(c) * A.replicas,
+                             A.replicas * sizeof(ReplicaState), cudaMemcpyHostToDevice, stream_),
+             "adjoint restore");
+  sync();
+}
+
+void Engine::adjoint_forward(uint64_t steps, uint64_t record_from, uint32_t every, double* obs) {
+  if (steps == 0) throw InvalidArgument("adjoint runs need at least one step.");
+  if (record_from > steps) throw InvalidArgument("record_from must not exceed steps.");
+  if (every == 0) throw InvalidArgument("checkpoint interval must be positive.");
+  if (v_.has_bonded) throw InvalidArgument("the adjoint supports pair-only systems.");
+  int max_types = 0;
+  for (const auto& h : rep_) max_types = std::max(max_types, h.n_types);
+  if (max_types > kAdjTypes) throw InvalidArgument("the adjoint supports up to 4 particle types.");
+
+  if (!adj_) adj_ = std::make_unique<AdjointStore>();
+  AdjointStore& A = *adj_;
+  const uint32_t R = n_replicas();
+  const size_t S = v_.n_slots;
+  A.steps = steps;
+  A.record_from = record_from;
+  A.every = every;
+  A.segments = static_cast<uint32_t>((steps + every - 1) / every);
+  A.slots = static_cast<uint32_t>(S);
+  A.replicas = R;
+  A.max_types = max_types;
+  if (A.ck_capacity < A.segments + 1ull) {
+    A.ck_capacity = A.segments + 1ull;
+    A.ck_pos = A.alloc<float4>(A.ck_capacity * S);
+    A.ck_vel = A.alloc<float4>(A.ck_capacity * S);
+    A.ck_img = A.alloc<int4>(A.ck_capacity * S);
+    A.ck_ref_pos = A.alloc<float4>(A.ck_capacity * S);
+    A.ck_ref_img = A.alloc<int4>(A.ck_capacity * S);
+  }
+  A.ck_state.assign(static_cast<size_t>(A.segments + 1) * R, ReplicaState{});
+  A.forward_done = false;
+
+  // Slots must not move during an adjoint run: switch off the periodic
+  // reorder on the device (restored at the end of the backward pass).
+  set_sort_enabled(false);
+
+  auto save = [&](uint32_t c) {
+    auto d2d = [&](void* dst, const void* src, size_t bytes) {
+      cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream_),
+                 "checkpoint");
+    };
+    d2d(A.ck_pos + c * S, v_.pos, S * sizeof(float4));
+    d2d(A.ck_vel + c * S, v_.vel, S * sizeof(float4));
+    d2d(A.ck_img + c * S, v_.img, S * sizeof(int4));
+    d2d(A.ck_ref_pos + c * S, v_.ref_pos, S * sizeof(float4));
+    d2d(A.ck_ref_img + c * S, v_.ref_img, S * sizeof(int4));
+    sync();
+    cuda_check(cudaMemcpy(A.ck_state.data() + static_cast<size_t>(c) * R, v_.rs,
+                          R * sizeof(ReplicaState), cudaMemcpyDeviceToHost),
+               "checkpoint");
+  };
+  std::vector<beads_observables> o;
+  auto put_obs = [&](uint64_t n) {
+    observables(o);
+    for (uint32_t r = 0; r < R; ++r) {
+      double* row = obs + ((n - record_from) * R + r) * 3;
+      row[0] = o[r].pe;
+      row[1] = o[r].virial;
+      row[2] = o[r].ke;
+    }
+  };
+
+  eval();
+  if (!tuned_ && !tuning_fixed_) autotune();
+  save(0);
+  if (record_from == 0) put_obs(0);
+  uint64_t n = 0;
+  while (n < steps) {
+    const uint64_t next_ck = (n / every + 1) * every;
+    if (n + 1 >= record_from) {
+      run(1, 1);
+      n += 1;
+      put_obs(n);
+    } else {
+      const uint64_t upto = std::min({next_ck, record_from - 1, steps});
+      run(upto - n, 0);
+      n = upto;
+    }
+    if (n % every == 0 && n < steps) save(static_cast<uint32_t>(n / every));
+  }
+  save(A.segments);  // the final state
+  A.forward_done = true;
+}
+
+void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* grad_sigma,
+                              float* grad_pos, float* grad_vel) {
+  if (!adj_ || !adj_->forward_done) throw InvalidArgument("adjoint_backward needs a forward run.");
+  AdjointStore& A = *adj_;
+  const uint32_t R = A.replicas;
+  const size_t S = A.slots;
+  const uint64_t T = A.steps;
+  const uint32_t K = A.every;
+
+  if (A.seg_capacity < K + 1) {
+    A.seg_capacity = K + 1;
+    A.seg_pos = A.alloc<float4>(static_cast<size_t>(K + 1) * S);
+    A.seg_vel = A.alloc<float4>(static_cast<size_t>(K + 1) * S);
+    A.seg_lam = A.alloc<double>(static_cast<size_t>(K + 1) * R);
+    A.seg_kin = A.alloc<double>(static_cast<size_t>(K + 1) * R);
+    A.seg_flags = A.alloc<uint32_t>(static_cast<size_t>(K + 1) * R);
+  }
+  if (!A.xbar) {
+    A.xbar = A.alloc<float4>(S);
+    A.vbar = A.alloc<float4>(S);
+    A.fbar = A.alloc<float4>(S);
+    A.ubar = A.alloc<float4>(S);
+    A.theta = A.alloc<long long>(static_cast<size_t>(R) * kAdjTypes * kAdjTypes * 4);
+    A.tag_xfer = A.alloc<float>(3 * n_tags_);
+    A.list_src = A.alloc<int>(R);
+    A.shift_on = A.alloc<int>(R);
+    A.list_changed = A.alloc<uint32_t>(R);
+  }
+  if (A.obs_capacity < (T + 1) * R * 3) {
+    A.obs_capacity = (T + 1) * R * 3;
+    A.obs_grad = A.alloc<double>(A.obs_capacity);
+  }
+  int* d_src = A.list_src;
+  int* d_shift = A.shift_on;
+  uint32_t* d_changed = A.list_changed;
+  {
+    std::vector<double> g((T + 1) * R * 3, 0.0);
+    std::copy(obs_grad, obs_grad + (T + 1 - A.record_from) * R * 3,
+              g.begin() + A.record_from * R * 3);
+    cuda_check(cudaMemcpy(A.obs_grad, g.data(), g.size() * sizeof(double),
+                          cudaMemcpyHostToDevice), "adjoint upload");
+    std::vector<int> sh(R);
+    for (uint32_t r = 0; r < R; ++r) sh[r] = rep_[r].lj_shift ? 1 : 0;
+    cuda_check(cudaMemcpy(d_shift, sh.data(), R * sizeof(int), cudaMemcpyHostToDevice),
+               "adjoint upload");
+  }
+  sync();
+  cuda_check(cudaMemset(A.xbar, 0, S * sizeof(float4)), "memset");
+  cuda_check(cudaMemset(A.ubar, 0, S * sizeof(float4)), "memset");
+  cuda_check(cudaMemset(A.vbar, 0, S * sizeof(float4)), "memset");
+  cuda_check(cudaMemset(A.theta, 0, static_cast<size_t>(R) * kAdjTypes * kAdjTypes * 4 * 8),
+             "memset");
+  {
+    // accumulator lanes used by the adjoint start at zero
+    std::vector<ReplicaState> st(R);
+    cuda_check(cudaMemcpy(st.data(), v_.rs, R * sizeof(ReplicaState), cudaMemcpyDeviceToHost),
+               "state");
+    for (auto& x : st) {
+      x.acc[kAccAdjoint] = x.acc_frac[kAccAdjoint] = 0;
+      x.acc[kAccAdjoint + 1] = x.acc_frac[kAccAdjoint + 1] = 0;
+    }
+    cuda_check(cudaMemcpy(v_.rs, st.data(), R * sizeof(ReplicaState), cudaMemcpyHostToDevice),
+               "state");
+  }
+
+  AdjView av{};
+  av.seg_pos = A.seg_pos;
+  av.seg_vel = A.seg_vel;
+  av.seg_lam = A.seg_lam;
+  av.seg_kin = A.seg_kin;
+  av.xbar = A.xbar;
+  av.vbar = A.vbar;
+  av.fbar = A.fbar;
+  av.ubar = A.ubar;
+  av.obs_grad = A.obs_grad;
+  av.theta = A.theta;
+  av.ck_ref_pos = A.ck_ref_pos;
+  av.list_src = d_src;
+  av.shift_on = d_shift;
+  av.slots = A.slots;
+  av.replicas = R;
+
+  std::vector<uint32_t> flags;
+  std::vector<int> current(R), wanted(R);
+  std::vector<uint32_t> changed(R);
+  for (int s = static_cast<int>(A.segments) - 1; s >= 0; --s) {
+    const uint64_t a = static_cast<uint64_t>(s) * K;
+    const uint64_t b = std::min<uint64_t>(a + K, T);
+    // Replay the segment, recording every step.
+    adjoint_restore(static_cast<uint32_t>(s));
+    adjoint_record(0);
+    for (uint64_t k = 1; k <= b - a; ++k) {
+      launch_chunk(1, false);
+      adjoint_record(static_cast<uint32_t>(k));
+    }
+    sync();
+    flags.resize(static_cast<size_t>(b - a + 1) * R);
+    cuda_check(cudaMemcpy(flags.data(), A.seg_flags, flags.size() * sizeof(uint32_t),
+                          cudaMemcpyDeviceToHost), "flags");
+    std::fill(current.begin(), current.end(), -2);  // list state unknown
+    const uint64_t m_lo = (s == 0) ? 0 : a + 1;
+    for (uint64_t m = b + 1; m-- > m_lo;) {
+      const uint32_t k = static_cast<uint32_t>(m - a);
+      // The list the forward step m used: built at the replica's last rebuild
+      // at or before m inside this segment, else the checkpoint's.
+      bool any = false;
+      for (uint32_t r = 0; r < R; ++r) {
+        int src = -1;
+        for (uint32_t q = k; q >= 1; --q) {
+          if (flags[static_cast<size_t>(q) * R + r]) {
+            src = static_cast<int>(q);
+            break;
+          }
+        }
+        wanted[r] = src;
+        changed[r] = (src != current[r]) ? 1u : 0u;
+        any = any || changed[r];
+      }
+      if (any) {
+        cuda_check(cudaMemcpyAsync(d_src, wanted.data(), R * sizeof(int), cudaMemcpyHostToDevice,
+                                   stream_), "adjoint list");
+        cuda_check(cudaMemcpyAsync(d_changed, changed.data(), R * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice, stream_), "adjoint list");
+        k_adj_list_positions<<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, static_cast<uint32_t>(s),
+                                                                  d_changed);
+        launch_check("adjoint list positions");
+        launch_rebuild(launch_, false);
+        sync();
+        current = wanted;
+      }
+      cuda_check(cudaMemcpyAsync(v_.pos, A.seg_pos + static_cast<size_t>(k) * S,
+                                 S * sizeof(float4), cudaMemcpyDeviceToDevice, stream_),
+                 "adjoint positions");
+      const int first = (m == 0) ? 1 : 0;
+      const int last = (m == T) ? 1 : 0;
+      const int lane_in = kAccAdjoint + static_cast<int>((m + 1) & 1u);
+      const int lane_out = kAccAdjoint + static_cast<int>(m & 1u);
+      k_adj_prepare<<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, static_cast<uint32_t>(m), k,
+                                                        first, last, lane_in);
+      launch_check("adjoint prepare");
+      k_adj_lj<<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, static_cast<uint32_t>(m), k, first,
+                                                   lane_out);
+      launch_check("adjoint pair");
+    }
+    sync();
+  }
+
+  // Outputs.
+  const uint32_t tb = static_cast<uint32_t>((n_tags_ + 255) / 256);
+  k_adj_gather<<<tb, 256, 0, stream_>>>(v_, A.xbar, A.tag_xfer, static_cast<uint32_t>(n_tags_));
+  launch_check("adjoint gather");
+  cuda_check(cudaMemcpyAsync(grad_pos, A.tag_xfer, 3 * n_tags_ * sizeof(float),
+                             cudaMemcpyDeviceToHost, stream_), "adjoint download");
+  sync();
+  k_adj_gather<<<tb, 256, 0, stream_>>>(v_, A.vbar, A.tag_xfer, static_cast<uint32_t>(n_tags_));
+  launch_check("adjoint gather");
+  cuda_check(cudaMemcpyAsync(grad_vel, A.tag_xfer, 3 * n_tags_ * sizeof(float),
+                             cudaMemcpyDeviceToHost, stream_), "adjoint download");
+  std::vector<long long> th(static_cast<size_t>(R) * kAdjTypes * kAdjTypes * 4);
+  sync();
+  cuda_check(cudaMemcpy(th.data(), A.theta, th.size() * sizeof(long long), cudaMemcpyDeviceToHost),
+             "adjoint download");
+  size_t out = 0;
+  for (uint32_t r = 0; r < R; ++r) {
+    const int nt = rep_[r].n_types;
+    for (int i = 0; i < nt; ++i) {
+      for (int j = 0; j < nt; ++j) {
+        const size_t base = ((static_cast<size_t>(r) * kAdjTypes + i) * kAdjTypes + j) * 4;
+        grad_eps[out] = static_cast<double>(th[base + 0]) +
+                        static_cast<double>(th[base + 1]) / kFixFrac;
+        grad_sigma[out] = static_cast<double>(th[base + 2]) +
+                          static_cast<double>(th[base + 3]) / kFixFrac;
+        ++out;
+      }
+    }
+  }
+  // Back to the end-of-forward state, list included.
+  adjoint_restore(A.segments);
+  set_sort_enabled(true);
+  check_status();
+}
+
+}  // namespace bb

@@ -1,0 +1,66 @@
+// adjoint.hpp -- device storage of the reverse-mode (adjoint) pass.
+//
+// The forward pass keeps checkpoints of the full step state every K steps
+// (and one of the final state); the backward pass replays one segment at a
+// time from its checkpoint, recording positions, velocities, Berendsen scales
+// and kinetic energies of every step of the segment, then walks the segment
+// backwards.  Memory: (segments + 1) checkpoints of 80 bytes per slot plus
+// K + 1 recorded steps of 32 bytes per slot.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace bb {
+
+struct AdjointStore {
+  uint64_t steps = 0;         // T
+  uint64_t record_from = 0;   // first step whose observables enter the loss
+  uint32_t every = 0;         // K
+  uint32_t segments = 0;      // ceil(T / K)
+  uint32_t slots = 0;         // S
+  uint32_t replicas = 0;      // R
+  int max_types = 0;          // LJ table side of the largest replica table
+  bool forward_done = false;
+
+  // checkpoints: segment starts 0..segments-1, then the final state
+  float4* ck_pos = nullptr;
+  float4* ck_vel = nullptr;
+  int4* ck_img = nullptr;
+  float4* ck_ref_pos = nullptr;
+  int4* ck_ref_img = nullptr;
+  std::vector<ReplicaState> ck_state;
+  uint64_t ck_capacity = 0;   // checkpoints allocated
+
+  // one replayed segment: steps a..a+K
+  float4* seg_pos = nullptr;
+  float4* seg_vel = nullptr;
+  double* seg_lam = nullptr;     // [k * R + r] Berendsen scale after step a+k
+  double* seg_kin = nullptr;     // [k * R + r] kinetic energy after step a+k
+  uint32_t* seg_flags = nullptr; // [k * R + r] replica rebuilt its list at step a+k
+  uint32_t seg_capacity = 0;     // K + 1 allocated
+
+  // adjoint vectors (per slot) and reductions
+  float4* xbar = nullptr;
+  float4* vbar = nullptr;
+  float4* fbar = nullptr;
+  float4* ubar = nullptr;
+  double* obs_grad = nullptr;    // [(T + 1) * R * 3]
+  uint64_t obs_capacity = 0;
+  long long* theta = nullptr;    // [R][types^2][eps, sigma][whole, frac]
+  float* tag_xfer = nullptr;     // [3 * particles] tag-order staging
+  int* list_src = nullptr;       // [R] list build source of the replayed step
+  int* shift_on = nullptr;       // [R] LJ energy shift active
+  uint32_t* list_changed = nullptr;  // [R]
+
+  std::vector<void*> allocations;
+  ~AdjointStore();
+  template <typename T>
+  T* alloc(size_t count);
+};
+
+}  // namespace bb

@@ -373,6 +373,53 @@ int beads_list_stats(beads_ctx* ctx, uint64_t* total_entries, uint32_t* max_coun
   });
 }
 
+int beads_set_tuning(beads_ctx* ctx, const int32_t* schedule) {
+  return guarded([&] {
+    require(ctx && ctx->engine && schedule, "NULL argument.");
+    ctx->engine->set_tuning(schedule[0], schedule[1], schedule[2], schedule[3]);
+  });
+}
+
+int beads_get_tuning(beads_ctx* ctx, int32_t* schedule) {
+  return guarded([&] {
+    require(ctx && ctx->engine && schedule, "NULL argument.");
+    int t = 0, f = 0, u = 0, pf = 0, a = 0;
+    ctx->engine->tuning(&t, &f, &u, &pf, &a);
+    schedule[0] = t;
+    schedule[1] = f;
+    schedule[2] = u;
+    schedule[3] = pf;
+    schedule[4] = a;
+  });
+}
+
+int beads_set_lj(beads_ctx* ctx, uint32_t replica, const double* epsilon, const double* sigma) {
+  return guarded([&] {
+    require(ctx && ctx->engine && epsilon && sigma, "NULL argument.");
+    require(replica < ctx->engine->n_replicas(), "replica index out of range.");
+    ctx->engine->set_lj(replica, epsilon, sigma);
+  });
+}
+
+int beads_adjoint_forward(beads_ctx* ctx, uint64_t steps, uint64_t record_from,
+                          uint32_t checkpoint_every, double* observables) {
+  return guarded([&] {
+    require(ctx && ctx->engine && observables, "NULL argument.");
+    ctx->engine->adjoint_forward(steps, record_from, checkpoint_every, observables);
+  });
+}
+
+int beads_adjoint_backward(beads_ctx* ctx, const double* observables_grad, double* grad_epsilon,
+                           double* grad_sigma, float* grad_positions, float* grad_velocities) {
+  return guarded([&] {
+    require(ctx && ctx->engine && observables_grad && grad_epsilon && grad_sigma &&
+                grad_positions && grad_velocities,
+            "NULL argument.");
+    ctx->engine->adjoint_backward(observables_grad, grad_epsilon, grad_sigma, grad_positions,
+                                  grad_velocities);
+  });
+}
+
 int beads_counters(beads_ctx* ctx, uint32_t replica, uint64_t* counters) {
   return guarded([&] {
     require(ctx && ctx->engine && counters, "NULL argument.");

@@ -38,6 +38,7 @@ enum AccLane : int {
   kAccDihedral = 3,
   kAccVirial = 4,
   kAccKinetic = 5,
+  kAccAdjoint = 6,  // adjoint: sum of u_bar . v (Berendsen scale adjoint)
   kAccLanes = 8
 };
 
@@ -92,6 +93,7 @@ struct ReplicaState {
   unsigned int status;              // kStatus* bits
   unsigned int pad0;
   double lambda;                    // pending Berendsen velocity scale
+  double last_kinetic;              // kinetic energy of the last post (before scaling)
   long long acc[kAccLanes];         // fixed-point totals of the current eval:
   long long acc_frac[kAccLanes];    //   whole words and 2^-32 fraction words
 };
@@ -185,6 +187,7 @@ struct DeviceView {
   ReplicaObs* obs;
   const uint32_t* block_replica;
   const uint32_t* cell_replica;  // replica of each global cell
+  unsigned long long* chain_launches;  // launches of the rebuild chain so far
   const LjCoeff* lj;
   uint32_t n_replicas;
   uint32_t n_slots;

@@ -1,6 +1,9 @@
 // engine.cu -- host side of the batched device engine: memory layout, static
 // tables, the captured step loop and host transfers.
 #include "engine.hpp"
+#include "adjoint.hpp"
+
+#include <cstdio>
 
 #include <algorithm>
 #include <cmath>
@@ -66,6 +69,129 @@ Engine::Engine(uint32_t n, const beads_system_desc* systems,
   }
 }
 
+void Engine::set_sort_enabled(bool on) {
+  sync();
+  for (uint32_t r = 0; r < rep_.size(); ++r) {
+    const uint32_t value = on ? rep_[r].sort_every : 0u;
+    ReplicaParams* dst = const_cast<ReplicaParams*>(v_.rp) + r;
+    cuda_check(cudaMemcpy(&dst->sort_every, &value, sizeof(value), cudaMemcpyHostToDevice),
+               "sort cadence");
+  }
+}
+
+void Engine::clear_graphs() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto& kv : graphs_) {
+    cudaGraphExecDestroy(kv.second.second);
+    cudaGraphDestroy(kv.second.first);
+  }
+  graphs_.clear();
+}
+
+void Engine::set_tuning(int tpa, int fuse_post, int unroll, int prefetch) {
+  if (tpa == 0) {
+    tuning_fixed_ = false;
+    tuned_ = false;
+    return;
+  }
+  if (tpa != 1 && tpa != 2 && tpa != 4) throw InvalidArgument("threads per particle must be 1, 2 or 4.");
+  if (unroll != 4 && unroll != 8) throw InvalidArgument("batch depth must be 4 or 8.");
+  clear_graphs();
+  launch_.lj_tpa = tpa;
+  launch_.lj_unroll = unroll;
+  launch_.lj_prefetch = prefetch ? 1 : 0;
+  launch_.fuse_post = fuse_post ? 1 : 0;
+  tuning_fixed_ = true;
+}
+
+void Engine::tuning(int* tpa, int* fuse_post, int* unroll, int* prefetch, int* autotuned) const {
+  *tpa = launch_.lj_tpa;
+  *fuse_post = launch_.fuse_post;
+  *unroll = launch_.lj_unroll;
+  *prefetch = launch_.lj_prefetch;
+  *autotuned = (tuned_ && !tuning_fixed_) ? 1 : 0;
+}
+
+// Times the force stage of a step (pair forces, bonded terms, second
+// half-kick and kinetic total) under every schedule on the current list and
+// keeps the fastest.  The kicks of the trial launches are undone.  With
+// BEADS_TUNE_LOG=1 the timings go to stderr.
+void Engine::autotune() {
+  if (!initialized_) eval();
+  constexpr int kWarm = 2, kReps = 8;
+  const bool log = [] {
+    const char* e = std::getenv("BEADS_TUNE_LOG");
+    return e && std::string(e) == "1";
+  }();
+  std::vector<ReplicaState> saved(rep_.size());
+  sync();
+  cuda_check(cudaMemcpy(saved.data(), v_.rs, saved.size() * sizeof(ReplicaState),
+                        cudaMemcpyDeviceToHost), "state save");
+  cuda_check(cudaMemcpyAsync(v_.vel2, v_.vel, v_.n_slots * sizeof(float4),
+                             cudaMemcpyDeviceToDevice, stream_), "velocity save");
+  cudaEvent_t a = nullptr, b = nullptr;
+  cuda_check(cudaEventCreate(&a), "event create");
+  cuda_check(cudaEventCreate(&b), "event create");
+  float best = 0.f;
+  StepLaunch chosen = launch_;
+  auto trial = [&](const StepLaunch& l) {
+    for (int k = 0; k < kWarm; ++k) launch_forces(l, false, false, true);
+    cuda_check(cudaEventRecord(a, stream_), "event record");
+    for (int k = 0; k < kReps; ++k) launch_forces(l, false, false, true);
+    cuda_check(cudaEventRecord(b, stream_), "event record");
+    cuda_check(cudaEventSynchronize(b), "event sync");
+    float ms = 0.f;
+    cuda_check(cudaEventElapsedTime(&ms, a, b), "event elapsed");
+    if (log) {
+      std::fprintf(stderr, "beads autotune: tpa %d depth %d prefetch %d fuse_post %d: %.4f ms\n",
+                   l.lj_tpa, l.lj_unroll, l.lj_prefetch, l.fuse_post, ms / kReps);
+    }
+    if (best == 0.f || ms < best) {
+      best = ms;
+      chosen = l;
+    }
+  };
+  try {
+    // The pair-force shape first (second half-kick as its own kernel), then
+    // the best shape with the kick fused.
+    for (int tpa : {1, 2, 4}) {
+      for (int unroll : {8, 4}) {
+        for (int prefetch : {1, 0}) {
+          StepLaunch l = launch_;
+          l.lj_tpa = tpa;
+          l.lj_unroll = unroll;
+          l.lj_prefetch = prefetch;
+          l.fuse_post = 0;
+          trial(l);
+        }
+      }
+    }
+    StepLaunch fused = chosen;
+    fused.fuse_post = 1;
+    trial(fused);
+  } catch (...) {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    throw;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cuda_check(cudaMemcpyAsync(v_.vel, v_.vel2, v_.n_slots * sizeof(float4),
+                             cudaMemcpyDeviceToDevice, stream_), "velocity restore");
+  cuda_check(cudaMemcpyAsync(v_.rs, saved.data(), saved.size() * sizeof(ReplicaState),
+                             cudaMemcpyHostToDevice, stream_), "state restore");
+  sync();
+  if (chosen.lj_tpa != launch_.lj_tpa || chosen.fuse_post != launch_.fuse_post ||
+      chosen.lj_unroll != launch_.lj_unroll || chosen.lj_prefetch != launch_.lj_prefetch) {
+    clear_graphs();
+  }
+  launch_.lj_tpa = chosen.lj_tpa;
+  launch_.lj_unroll = chosen.lj_unroll;
+  launch_.lj_prefetch = chosen.lj_prefetch;
+  launch_.fuse_post = chosen.fuse_post;
+  tuned_ = true;
+}
+
 Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   for (auto& kv : graphs_) {
@@ -111,6 +237,9 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
     h.n_dihedrals = s.n_dihedrals;
     h.dt = dyns[r].dt;
     h.thermostat = dyns[r].thermostat;
+    h.n_types = f.n_types;
+    h.lj_cutoff = f.lj_cutoff;
+    h.lj_shift = f.lj_shift;
     slots += h.n_pad;
     tags += s.n_particles;
     if (slots > 0xF0000000ull) throw OverflowError("total particle slots exceed index range.");
@@ -150,6 +279,7 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
     p.sort_every = h.plan.path == kPathDirect
                        ? 0u
                        : static_cast<uint32_t>(std::min<uint64_t>(nbrs[r].sort_every_rebuild, 0xFFFFFFFFull));
+    h.sort_every = p.sort_every;
     p.dt = static_cast<float>(dyns[r].dt);
     p.thermostat = dyns[r].thermostat;
     p.kb = s.units == BEADS_UNITS_NM_KJMOL ? kKbNmKjMol : 1.0;
@@ -160,6 +290,7 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
     p.dof = dof > 0.0 ? dof : 0.0;
     p.volume = static_cast<double>(p.len[0]) * p.len[1] * p.len[2];
     p.lj_offset = static_cast<uint32_t>(lj_entries);
+    rep_[r].lj_offset = p.lj_offset;
     p.n_types = f.n_types;
     lj_entries += static_cast<uint64_t>(f.n_types) * f.n_types;
     p.bond_type_base = bond_types;
@@ -386,6 +517,8 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
     for (int a = 0; a < 3; ++a) all_regular = all_regular && rp[r].nc[a] >= 4u;
   }
   uint32_t* d_cell_replica = dalloc<uint32_t>(C);
+  v.chain_launches = dalloc<unsigned long long>(1);
+  cuda_check(cudaMemsetAsync(v.chain_launches, 0, sizeof(unsigned long long), stream_), "memset");
   LjCoeff* d_lj = dalloc<LjCoeff>(h_lj.size());
 
   auto up = [&](void* dst, const void* src, size_t bytes) {
@@ -439,6 +572,10 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   launch_.stream = stream_;
   launch_.max_cells_per_replica = max_cells;
   launch_.all_regular = all_regular ? 1 : 0;
+  launch_.lj_tpa = 1;
+  launch_.lj_unroll = 8;
+  launch_.lj_prefetch = 1;
+  launch_.fuse_post = 0;
   launch_.max_atoms_per_replica = max_atoms;
   launch_.excl_cap = excl_cap;
   launch_.need_kinetic = any_thermostat ? 1 : 0;
@@ -595,6 +732,7 @@ void Engine::launch_chunk(uint32_t steps, bool obs_last) {
 
 bool Engine::run(uint64_t steps, uint64_t obs_every) {
   if (!initialized_) eval();
+  if (!tuned_ && !tuning_fixed_ && steps > 0) autotune();
   bool last_obs = false;
   uint64_t remaining = steps;
   while (remaining > 0) {
@@ -712,7 +850,7 @@ double Engine::profile(int stage, uint32_t reps) {
   return static_cast<double>(ms) / reps;
 }
 
-void Engine::counters(uint32_t replica, uint64_t out[3]) {
+void Engine::counters(uint32_t replica, uint64_t out[4]) {
   sync();
   ReplicaState st;
   cuda_check(cudaMemcpy(&st, v_.rs + replica, sizeof(ReplicaState), cudaMemcpyDeviceToHost),
@@ -720,6 +858,8 @@ void Engine::counters(uint32_t replica, uint64_t out[3]) {
   out[0] = st.step;
   out[1] = st.builds;
   out[2] = st.dangerous;
+  cuda_check(cudaMemcpy(&out[3], v_.chain_launches, sizeof(unsigned long long),
+                        cudaMemcpyDeviceToHost), "counters download");
 }
 
 void Engine::list_stats(uint64_t* total, uint32_t* max_count) {

@@ -3,6 +3,7 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <string>
 #include <utility>
 #include <vector>
@@ -41,7 +42,14 @@ struct ReplicaHost {
   uint32_t n_bonds = 0, n_angles = 0, n_dihedrals = 0;
   double dt = 0;
   int thermostat = 0;
+  int n_types = 0;
+  uint32_t lj_offset = 0;        // first entry of the replica's LJ table
+  double lj_cutoff = 0;
+  int lj_shift = 0;
+  uint32_t sort_every = 0;       // reorder cadence in builds (0 = never)
 };
+
+struct AdjointStore;  // adjoint.cu
 
 class Engine {
  public:
@@ -85,11 +93,47 @@ class Engine {
   void flush_lambda();
   double profile(int stage, uint32_t reps);
   void list_stats(uint64_t* total, uint32_t* max_count);
-  // Completed steps, neighbour builds and dangerous rebuilds of one replica.
-  void counters(uint32_t replica, uint64_t out[3]);
+  // Completed steps, neighbour builds and dangerous rebuilds of one replica,
+  // and the launches of the rebuild chain so far (whole batch).
+  void counters(uint32_t replica, uint64_t out[4]);
   void check_status();
+  // Kernel schedule of the step: threads per particle of the pair-force
+  // kernel (1, 2 or 4), its batch depth (4 or 8 list entries in flight per
+  // thread), whether it requests the next batch's list entries early, and
+  // whether the second half-kick runs inside the last force kernel.  Every choice gives bit-identical results.  tpa = 0 hands
+  // the choice back to the autotuner, which times every candidate on this
+  // batch at the first run (velocities and step state restored) and keeps
+  // the fastest.
+  void set_tuning(int tpa, int fuse_post, int unroll, int prefetch);
+  void tuning(int* tpa, int* fuse_post, int* unroll, int* prefetch, int* autotuned) const;
+  void autotune();
+
+  // ---- adjoint (reverse-mode gradients of a trajectory; adjoint.cu) ----
+  // Replaces the LJ eps/sigma tables of one replica (full n_types^2 tables).
+  void set_lj(uint32_t replica, const double* eps, const double* sigma);
+  // Runs `steps` velocity-Verlet steps from the current state (forces and
+  // the list are rebuilt first, as a fresh run), keeping a checkpoint every
+  // `checkpoint_every` steps.  obs receives [step - record_from][replica]
+  // {pair+bonded PE, virial, thermo KE} for steps record_from..steps.
+  void adjoint_forward(uint64_t steps, uint64_t record_from, uint32_t checkpoint_every,
+                       double* obs);
+  // Given dL/d(obs) in the same layout, returns dL/d(eps), dL/d(sigma)
+  // ([replica][n_types^2] each, per ordered type pair of the table), dL/dx0
+  // and dL/dv0 (tag order, [n_particles_total][3]).  The particle state is
+  // the end-of-forward state again afterwards.
+  void adjoint_backward(const double* obs_grad, double* grad_eps, double* grad_sigma,
+                        float* grad_pos, float* grad_vel);
 
  private:
+  // Switches the periodic slot reorder off (false) or back to each replica's
+  // own cadence (true); adjoint runs need fixed slots.
+  void set_sort_enabled(bool on);
+  void adjoint_restore(uint32_t segment);
+  void adjoint_record(uint32_t k);
+  void adjoint_select_list(uint32_t a, uint32_t m, std::vector<int>& current,
+                           const std::vector<uint32_t>& flags);
+  std::unique_ptr<AdjointStore> adj_;
+  void clear_graphs();
   template <typename T>
   T* dalloc(size_t count);
   void upload_static(uint32_t n, const beads_system_desc* systems,
@@ -112,6 +156,8 @@ class Engine {
   bool initialized_ = false;
   bool use_graphs_ = true;
   bool use_conditional_ = true;
+  bool tuning_fixed_ = false;          // set_tuning() with an explicit choice
+  bool tuned_ = false;                 // autotune() has run
   cudaStream_t side_stream_ = nullptr;
   std::map<std::pair<uint32_t, bool>, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs_;
   ReplicaObs* h_obs_ = nullptr;        // pinned

@@ -21,6 +21,7 @@
 // bonded forces are gathered per particle (each thread evaluates the terms its
 // particle belongs to) so no force atomics exist anywhere.
 #include "kernels.cuh"
+#include "device_util.cuh"
 
 #include <cstdio>
 #include <stdexcept>
@@ -28,144 +29,6 @@
 
 namespace bb {
 namespace {
-
-constexpr unsigned kFull = 0xffffffffu;
-
-// One slot's contribution to a fixed-point total: floor(v) and the fraction
-// v - floor(v) (exact in double) truncated to units of 2^-32.
-struct Fixed {
-  long long whole;
-  long long frac;
-};
-
-__device__ __forceinline__ Fixed to_fixed(double v, unsigned* status) {
-  if (!(fabs(v) < kFixLimit)) {
-    atomicOr(status, kStatusFixedOverflow);
-    return Fixed{0, 0};
-  }
-  const double w = floor(v);
-  return Fixed{(long long)w, (long long)((v - w) * kFixFrac)};
-}
-
-__device__ __forceinline__ double from_fixed(long long whole, long long frac) {
-  return (double)whole + (double)frac / kFixFrac;
-}
-
-// Warp + block sum of one fixed-point contribution, two atomics per block.
-template <int kThreads>
-__device__ __forceinline__ void block_add_fixed(Fixed f, long long* whole, long long* frac) {
-  __shared__ long long partial[2][kThreads / 32];
-  long long a = f.whole, c = f.frac;
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_down_sync(kFull, a, o);
-    c += __shfl_down_sync(kFull, c, o);
-  }
-  const int warp = threadIdx.x >> 5;
-  if ((threadIdx.x & 31) == 0) {
-    partial[0][warp] = a;
-    partial[1][warp] = c;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    long long sa = 0, sc = 0;
-    for (int w = 0; w < kThreads / 32; ++w) {
-      sa += partial[0][w];
-      sc += partial[1][w];
-    }
-    if (sa != 0) atomicAdd(reinterpret_cast<unsigned long long*>(whole),
-                           static_cast<unsigned long long>(sa));
-    if (sc != 0) atomicAdd(reinterpret_cast<unsigned long long*>(frac),
-                           static_cast<unsigned long long>(sc));
-  }
-  __syncthreads();
-}
-
-template <int kThreads>
-__device__ __forceinline__ void block_add_lane(bool real, double v, ReplicaState* st, int lane) {
-  block_add_fixed<kThreads>(real ? to_fixed(v, &st->status) : Fixed{0, 0}, &st->acc[lane],
-                            &st->acc_frac[lane]);
-}
-
-// Reads and clears one fixed-point total (last block of a replica only).
-__device__ __forceinline__ double take_total(ReplicaState* st, int lane) {
-  unsigned long long* w = reinterpret_cast<unsigned long long*>(st->acc);
-  unsigned long long* f = reinterpret_cast<unsigned long long*>(st->acc_frac);
-  const long long whole = (long long)atomicExch(&w[lane], 0ull);
-  const long long frac = (long long)atomicExch(&f[lane], 0ull);
-  return from_fixed(whole, frac);
-}
-
-// Minimum image exactly as the reference applies it to wrapped coordinates
-// (box_geometry_view.cuh:50-62): one subtraction, then one shift by L.
-__device__ __forceinline__ float ref_delta(float xi, float xj, float len,
-                                           float half) {
-  float d = __fsub_rn(xi, xj);
-  if (d > half) {
-    d = __fsub_rn(d, len);
-  } else if (d < -half) {
-    d = __fadd_rn(d, len);
-  }
-  return d;
-}
-
-// Minimum image rounded once from the exact difference.  When the pair spans
-// the periodic boundary the reference's form rounds xi - xj at the magnitude
-// of L before shifting; here the rounding error of xi - xj is recovered with
-// Knuth's TwoSum and added back after the (exact, by Sterbenz) shift by L.
-__device__ __forceinline__ float acc_delta(float xi, float xj, float len,
-                                           float half) {
-  float d = __fsub_rn(xi, xj);
-  if (fabsf(d) > half) {
-    const float nxj = -xj;
-    const float bp = __fsub_rn(d, xi);
-    const float ap = __fsub_rn(d, bp);
-    const float err = __fadd_rn(__fsub_rn(xi, ap), __fsub_rn(nxj, bp));
-    const float shifted = d > 0.0f ? __fsub_rn(d, len) : __fadd_rn(d, len);
-    d = __fadd_rn(shifted, err);
-  }
-  return d;
-}
-
-// |d|^2 with the contraction order fixed: fma(dz,dz, fma(dy,dy, dx*dx)).
-__device__ __forceinline__ float norm2(float dx, float dy, float dz) {
-  return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-}
-
-__device__ __forceinline__ uint32_t axis_cell(float x, float lo, float inv,
-                                              uint32_t n) {
-  const float scaled = __fmul_rn(__fsub_rn(x, lo), inv);
-  if (scaled <= 0.0f) return 0u;
-  if (scaled >= (float)n) return n - 1u;   // also catches NaN-free overflow
-  const uint32_t idx = (uint32_t)scaled;
-  return idx >= n ? n - 1u : idx;
-}
-
-// Cells visited along one axis around centre c, unique so that one or two
-// cells per axis are not visited twice (same set rule as the reference's
-// unique_axis_cells, small_dimension_neighbor_builder.cu:56-76): the k-th of
-// min(n, 3) cells, computed without an indexed array so the hot loop's state
-// stays in registers.
-__device__ __forceinline__ uint32_t stencil_cell(uint32_t c, uint32_t n, uint32_t k) {
-  if (n < 3u) return k;
-  const uint32_t t = c + k + n - 1u;  // c - 1 + k, wrapped
-  return t >= n ? (t >= 2u * n ? t - 2u * n : t - n) : t;
-}
-
-// Last block of a replica to finish a kernel (threadfence-reduction pattern:
-// no waiting, the last arriving block does the per-replica epilogue).
-__device__ __forceinline__ bool arrive_last(unsigned int* counter,
-                                            unsigned int n_blocks) {
-  __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned prev = atomicAdd(counter, 1u);
-    last = (prev + 1u == n_blocks);
-  }
-  __syncthreads();
-  if (last) __threadfence();
-  return last;
-}
 
 // ---------------------------------------------------------------------------
 // pre: Berendsen lambda of the previous step, half-kick, drift, wrap, image
@@ -292,6 +155,7 @@ __global__ void k_force_rebuild_flags(DeviceView v, int count_build) {
 // rebuild 1: cell id and per-cell count.
 __global__ void __launch_bounds__(kBlock) k_bin(DeviceView v) {
   const uint32_t b = blockIdx.x;
+  if (b == 0 && threadIdx.x == 0) *v.chain_launches += 1ull;  // launches of the chain
   const uint32_t r = v.block_replica[b];
   if (!v.rs[r].need_rebuild) return;
   const ReplicaParams& p = v.rp[r];
@@ -697,9 +561,9 @@ __device__ __forceinline__ double post_slot(const DeviceView& v, const ReplicaPa
 template <bool kKick, bool kObs, bool kKinetic>
 __device__ __forceinline__ void post_finish(const DeviceView& v, const ReplicaParams& p,
                                             ReplicaState* st, uint32_t r, bool real,
-                                            double ke) {
+                                            double ke, uint32_t blocks_per_128 = 1) {
   if (kKinetic) block_add_lane<kBlock>(real, ke, st, kAccKinetic);
-  const uint32_t n_blocks = p.n_pad / kBlock;
+  const uint32_t n_blocks = p.n_pad / kBlock * blocks_per_128;
   if (arrive_last(&st->done_post, n_blocks) && threadIdx.x == 0) {
     const double kin = kKinetic ? take_total(st, kAccKinetic) : 0.0;
     double lam = 1.0;
@@ -712,6 +576,7 @@ __device__ __forceinline__ void post_finish(const DeviceView& v, const ReplicaPa
       st->lambda = lam;
       st->step += 1ull;
     }
+    if (kKinetic) st->last_kinetic = kin;
     if (kObs) {
       ReplicaObs o;
       o.step = st->step;
@@ -736,22 +601,79 @@ __device__ __forceinline__ void post_finish(const DeviceView& v, const ReplicaPa
 // LJ pair forces over the full list (each pair evaluated from both ends, no
 // atomics).  FP32 pair arithmetic; per-slot energy and virial are converted to
 // fixed point once per slot and reduced per block.
-template <bool kObs, int kMode>
-__global__ void __launch_bounds__(kBlock, kObs ? 6 : 8) k_lj(DeviceView v) {
+//
+// kTpa threads share one particle (threads-per-atom 1, 2 or 4, chosen by the
+// engine's autotuner): thread `sub` takes list entries k = sub, sub + kTpa, ...
+// Whatever kTpa, a particle's force is summed in one canonical order: four
+// partial sums by k mod 4, each in ascending k, combined as
+// (s0 + s1) + (s2 + s3).  So every kTpa gives the same bits and the tuning
+// choice never changes a result.
+template <int kTpa>
+struct LjAcc {
+  // kTpa 1: a[0] = (s0, s1), a[1] = (s2, s3); kTpa 2: a[0] = (s_sub, s_sub+2);
+  // kTpa 4: a[0].x = s_sub.
+  float2 a[kTpa == 1 ? 2 : 1];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int c = 0; c < (kTpa == 1 ? 2 : 1); ++c) a[c] = make_float2(0.f, 0.f);
+  }
+  // Adds the packed contributions of own entries 2h and 2h + 1 of a batch.
+  __device__ __forceinline__ void add_fma(uint32_t h, float2 s, float2 d) {
+    if (kTpa == 1) {
+      a[h & 1u] = __ffma2_rn(s, d, a[h & 1u]);
+    } else if (kTpa == 2) {
+      a[0] = __ffma2_rn(s, d, a[0]);
+    } else {
+      a[0].x = __fmaf_rn(s.x, d.x, a[0].x);
+      a[0].x = __fmaf_rn(s.y, d.y, a[0].x);
+    }
+  }
+  __device__ __forceinline__ void add(uint32_t h, float2 t) {
+    if (kTpa == 1) {
+      a[h & 1u] = __fadd2_rn(a[h & 1u], t);
+    } else if (kTpa == 2) {
+      a[0] = __fadd2_rn(a[0], t);
+    } else {
+      a[0].x = __fadd_rn(a[0].x, t.x);
+      a[0].x = __fadd_rn(a[0].x, t.y);
+    }
+  }
+  // (s0 + s1) + (s2 + s3); the threads of one particle are adjacent lanes.
+  __device__ __forceinline__ float total() const {
+    if (kTpa == 1) return __fadd_rn(__fadd_rn(a[0].x, a[0].y), __fadd_rn(a[1].x, a[1].y));
+    if (kTpa == 2) {
+      const float px = __shfl_xor_sync(kFull, a[0].x, 1);
+      const float py = __shfl_xor_sync(kFull, a[0].y, 1);
+      return __fadd_rn(__fadd_rn(a[0].x, px), __fadd_rn(a[0].y, py));
+    }
+    const float pair = __fadd_rn(a[0].x, __shfl_xor_sync(kFull, a[0].x, 1));
+    return __fadd_rn(pair, __shfl_xor_sync(kFull, pair, 2));
+  }
+};
+
+template <bool kObs, int kMode, int kTpa, int kUnroll, bool kPrefetch>
+__global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
   constexpr bool kClamp = kMode == kForceClamp;
   constexpr bool kPost = kMode >= kForcePost;
   constexpr bool kKinetic = kMode == kForcePostKinetic || (kPost && kObs);
-  const uint32_t b = blockIdx.x;
-  const uint32_t r = v.block_replica[b];
+  constexpr uint32_t kAtoms = kBlock / kTpa;  // particles per block
+  const uint32_t sb = blockIdx.x / kTpa;      // 128-slot block of the particles
+  const uint32_t r = v.block_replica[sb];
   const ReplicaParams& p = v.rp[r];
   __shared__ LjCoeff table[kMaxTypes * kMaxTypes];
   const int nt = p.n_types;
   for (int t = threadIdx.x; t < nt * nt; t += kBlock) table[t] = v.lj[p.lj_offset + t];
   __syncthreads();
 
-  const uint32_t i = b * kBlock + threadIdx.x;
+  const uint32_t sub = threadIdx.x % kTpa;
+  const uint32_t i = sb * kBlock + (blockIdx.x % kTpa) * kAtoms + threadIdx.x / kTpa;
   const bool real = (i - p.atom_begin) < p.n_atoms;
-  float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f, w = 0.f;
+  LjAcc<kTpa> ax, ay, az, ae, aw;
+  ax.zero();
+  ay.zero();
+  az.zero();
+  ae.zero();
+  aw.zero();
   {
     // Every lane of the warp (padding lanes included, with n = 0) runs the
     // same number of batches, so the warp votes below are convergent.
@@ -765,27 +687,50 @@ __global__ void __launch_bounds__(kBlock, kObs ? 6 : 8) k_lj(DeviceView v) {
     const float2 xi2x = make_float2(xi.x, xi.x);
     const float2 xi2y = make_float2(xi.y, xi.y);
     const float2 xi2z = make_float2(xi.z, xi.z);
-    float2 f2x = make_float2(0.f, 0.f), f2y = f2x, f2z = f2x, e2 = f2x, w2 = f2x;
-    const uint32_t* list = v.nbr + nbr_index(i, 0, v.nbr_stride);
-    // Software-pipelined over batches of kUnroll pairs: all list loads of a
-    // batch are issued, then all position gathers, then the arithmetic, so a
-    // warp keeps kUnroll independent misses in flight instead of one.  The
-    // list is streamed (evict-first) so the positions stay resident in L2.
-    constexpr uint32_t kUnroll = 8;
-    for (uint32_t k0 = 0; k0 < n_warp; k0 += kUnroll) {
+    const uint32_t* list = v.nbr + nbr_index(i, 0, v.nbr_stride) + sub * kGroup;
+    // Software-pipelined over batches of kUnroll (4 or 8) own entries: all
+    // list loads of a batch are issued, then all position gathers, then the
+    // arithmetic, so a warp keeps kUnroll independent misses in flight
+    // instead of one (8: more misses in flight, 4: fewer registers and more
+    // resident warps).  The list is streamed (evict-first) so the positions
+    // stay in L2.
+    // kPrefetch: the list entries of the next batch are requested before the
+    // arithmetic of the current one, so the (HBM) list latency overlaps it and
+    // only the (mostly L1/L2) position gathers stay on the critical path.
+    constexpr uint32_t kStep = kUnroll * kTpa;
+    uint32_t jn[kUnroll];
+    if (kPrefetch) {
+#pragma unroll
+      for (uint32_t u = 0; u < kUnroll; ++u) {
+        const uint32_t k = u * kTpa + sub;
+        jn[u] = k < n ? __ldcs(list + (size_t)(u * kTpa) * kGroup) : i;
+      }
+    }
+    for (uint32_t k0 = 0; k0 < n_warp; k0 += kStep) {
       uint32_t j[kUnroll];
 #pragma unroll
       for (uint32_t u = 0; u < kUnroll; ++u) {
-        j[u] = (k0 + u < n) ? __ldcs(list + (size_t)(k0 + u) * kGroup) : i;
+        if (kPrefetch) {
+          j[u] = jn[u];
+        } else {
+          const uint32_t k = k0 + u * kTpa + sub;
+          j[u] = k < n ? __ldcs(list + (size_t)(k0 + u * kTpa) * kGroup) : i;
+        }
       }
       float4 xj[kUnroll];
 #pragma unroll
       for (uint32_t u = 0; u < kUnroll; ++u) xj[u] = __ldg(&v.pos[j[u]]);
-      // Pairs 2h and 2h+1 of the batch run through the packed FP32x2 pipe of
-      // sm_100 (__fadd2_rn / __fmul2_rn / __ffma2_rn round each lane exactly
-      // as the scalar operation would): one instruction per two pairs.  Pairs
-      // beyond the cutoff and padding entries get a zero force scale rather
-      // than a branch.
+      if (kPrefetch) {
+#pragma unroll
+        for (uint32_t u = 0; u < kUnroll; ++u) {
+          const uint32_t k = k0 + kStep + u * kTpa + sub;
+          jn[u] = k < n ? __ldcs(list + (size_t)(k0 + kStep + u * kTpa) * kGroup) : i;
+        }
+      }
+      // Own entries 2h and 2h+1 of the batch run through the packed FP32x2
+      // pipe of sm_100 (__fadd2_rn / __fmul2_rn / __ffma2_rn round each lane
+      // exactly as the scalar operation would).  Pairs beyond the cutoff and
+      // padding entries get a zero force scale rather than a branch.
 #pragma unroll
       for (uint32_t h = 0; h < kUnroll / 2; ++h) {
         const uint32_t u0 = 2 * h, u1 = 2 * h + 1;
@@ -812,8 +757,8 @@ __global__ void __launch_bounds__(kBlock, kObs ? 6 : 8) k_lj(DeviceView v) {
             r2.y = norm2(dx.y, dy.y, dz.y);
           }
         }
-        const bool in0 = (k0 + u0 < n) && r2.x < rc2;
-        const bool in1 = (k0 + u1 < n) && r2.y < rc2;
+        const bool in0 = (k0 + u0 * kTpa + sub < n) && r2.x < rc2;
+        const bool in1 = (k0 + u1 * kTpa + sub < n) && r2.y < rc2;
         const LjCoeff c0 = row[__float_as_int(xj[u0].w)];
         const LjCoeff c1 = row[__float_as_int(xj[u1].w)];
         float2 rr = make_float2(in0 ? r2.x : 1.0f, in1 ? r2.y : 1.0f);
@@ -830,32 +775,30 @@ __global__ void __launch_bounds__(kBlock, kObs ? 6 : 8) k_lj(DeviceView v) {
         float2 fs = __fmul2_rn(__fmul2_rn(make_float2(c0.eps24, c1.eps24), inv), g);
         fs.x = in0 ? fs.x : 0.0f;
         fs.y = in1 ? fs.y : 0.0f;
-        f2x = __ffma2_rn(fs, dx, f2x);
-        f2y = __ffma2_rn(fs, dy, f2y);
-        f2z = __ffma2_rn(fs, dz, f2z);
+        ax.add_fma(h, fs, dx);
+        ay.add_fma(h, fs, dy);
+        az.add_fma(h, fs, dz);
         if (kObs) {
           const float2 ep = __ffma2_rn(make_float2(c0.eps4, c1.eps4), __fadd2_rn(sr12, neg6),
                                        make_float2(-c0.shift, -c1.shift));
-          e2 = __fadd2_rn(e2, make_float2(in0 ? ep.x : 0.0f, in1 ? ep.y : 0.0f));
-          w2 = __ffma2_rn(fs, rr, w2);
+          ae.add(h, make_float2(in0 ? ep.x : 0.0f, in1 ? ep.y : 0.0f));
+          aw.add_fma(h, fs, rr);
         }
       }
     }
-    fx = f2x.x + f2x.y;
-    fy = f2y.x + f2y.y;
-    fz = f2z.x + f2z.y;
-    e = e2.x + e2.y;
-    w = w2.x + w2.y;
   }
-  v.force[i] = make_float4(fx, fy, fz, 0.f);
+  const float fx = ax.total(), fy = ay.total(), fz = az.total();
+  const bool owner = real && sub == 0u;
+  if (sub == 0u) v.force[i] = make_float4(fx, fy, fz, 0.f);
   ReplicaState* st = &v.rs[r];
   double ke = 0.0;
-  if (kPost) ke = post_slot<true, kKinetic>(v, p, st, i, real, fx, fy, fz);
+  if (kPost) ke = post_slot<true, kKinetic>(v, p, st, i, owner, fx, fy, fz);
   if (kObs) {
-    block_add_lane<kBlock>(real, 0.5 * (double)e, st, kAccPair);
-    block_add_lane<kBlock>(real, 0.5 * (double)w, st, kAccVirial);
+    const float e = ae.total(), w = aw.total();
+    block_add_lane<kBlock>(owner, 0.5 * (double)e, st, kAccPair);
+    block_add_lane<kBlock>(owner, 0.5 * (double)w, st, kAccVirial);
   }
-  if (kPost) post_finish<true, kObs, kKinetic>(v, p, st, r, real, ke);
+  if (kPost) post_finish<true, kObs, kKinetic>(v, p, st, r, owner, ke, kTpa);
 }
 
 // ---------------------------------------------------------------------------
@@ -1207,24 +1150,43 @@ void launch_rebuild(const StepLaunch& l, bool force_all) {
   check_launch("build");
 }
 
-void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post) {
-  const int fin = !post ? kForcePlain : (l.need_kinetic ? kForcePostKinetic : kForcePost);
-  const bool bonded = l.v.has_bonded != 0;
-  const int lj_mode = clamp ? kForceClamp : (bonded ? kForcePlain : fin);
-#define BB_LJ(obs, mode) k_lj<obs, mode><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v)
-  if (lj_mode == kForceClamp) {
-    BB_LJ(false, kForceClamp);
-  } else if (observables) {
-    if (lj_mode == kForcePlain) BB_LJ(true, kForcePlain);
+template <int kTpa, int kUnroll, bool kPrefetch>
+void launch_lj_tpa(const StepLaunch& l, bool observables, int mode) {
+  const dim3 grid(l.v.n_blocks * kTpa);
+#define BB_LJ(obs, m) k_lj<obs, m, kTpa, kUnroll, kPrefetch><<<grid, kBlock, 0, l.stream>>>(l.v)
+  if (observables) {
+    if (mode == kForcePlain) BB_LJ(true, kForcePlain);
     else BB_LJ(true, kForcePost);  // the kinetic total is part of the observables
   } else {
-    switch (lj_mode) {
+    switch (mode) {
       case kForcePlain: BB_LJ(false, kForcePlain); break;
       case kForcePost: BB_LJ(false, kForcePost); break;
       default: BB_LJ(false, kForcePostKinetic); break;
     }
   }
 #undef BB_LJ
+}
+
+void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post) {
+  const bool fuse = post && l.fuse_post != 0;
+  const int fin = !fuse ? kForcePlain : (l.need_kinetic ? kForcePostKinetic : kForcePost);
+  const bool bonded = l.v.has_bonded != 0;
+  if (clamp) {
+    k_lj<false, kForceClamp, 1, 8, false><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  } else {
+    const int mode = bonded ? kForcePlain : fin;
+    // (threads per particle, batch depth, prefetch) -> one instantiation
+    const int key = l.lj_tpa * 100 + l.lj_unroll * 10 + (l.lj_prefetch ? 1 : 0);
+    switch (key) {
+#define BB_CASE(t, u, pf) \
+  case t * 100 + u * 10 + pf: launch_lj_tpa<t, u, pf != 0>(l, observables, mode); break;
+      BB_CASE(1, 8, 0) BB_CASE(1, 8, 1) BB_CASE(1, 4, 0) BB_CASE(1, 4, 1)
+      BB_CASE(2, 8, 0) BB_CASE(2, 8, 1) BB_CASE(2, 4, 0) BB_CASE(2, 4, 1)
+      BB_CASE(4, 8, 0) BB_CASE(4, 8, 1) BB_CASE(4, 4, 0) BB_CASE(4, 4, 1)
+#undef BB_CASE
+      default: throw std::runtime_error("unsupported pair-force schedule");
+    }
+  }
   check_launch("lj");
   if (bonded) {
 #define BB_BONDED(obs, mode) k_bonded<obs, mode><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v)
@@ -1241,6 +1203,7 @@ void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post)
 #undef BB_BONDED
     check_launch("bonded");
   }
+  if (post && !fuse) launch_post(l, true, observables);
 }
 
 void launch_post(const StepLaunch& l, bool kick, bool observables) {

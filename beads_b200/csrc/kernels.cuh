@@ -18,6 +18,10 @@ struct StepLaunch {
   uint32_t max_atoms_per_replica;
   int excl_cap;           // 0, 4, 8, 16, 32 or 64
   int all_regular;        // every replica has >= 4 cells on every axis
+  int lj_tpa;             // threads per particle of the pair-force kernel: 1, 2, 4
+  int lj_unroll;          // list entries in flight per thread and batch: 4 or 8
+  int lj_prefetch;        // list entries of the next batch requested one batch early
+  int fuse_post;          // second half-kick inside the last force kernel
   int need_kinetic;       // a thermostat is active in some replica
   float sd_dmax;          // descent: displacement cap
   float sd_fref;          // descent: force floor
@@ -28,8 +32,9 @@ struct StepLaunch {
 void launch_pre(const StepLaunch& l, int mode, cudaGraphConditionalHandle cond = 0,
                 bool use_cond = false);
 void launch_rebuild(const StepLaunch& l, bool force_all);
-// post: the last force kernel of the step also does the second half-kick,
-// the kinetic-energy total and the per-replica step epilogue (k_post's work).
+// post: finish the step with the second half-kick, the kinetic-energy total
+// and the per-replica step epilogue -- inside the last force kernel when
+// fuse_post is set, else as a separate k_post launch.
 void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post = false);
 void launch_post(const StepLaunch& l, bool kick, bool observables);
 void launch_project_exclusions(const StepLaunch& l, bool force_all);

@@ -269,11 +269,29 @@ class Engine:
             self.step += int(reps)
         return out.value
 
+    def set_tuning(self, threads_per_particle: int = 0, fuse_post: bool = False,
+                   batch_depth: int = 8, prefetch: bool = True) -> None:
+        """Fix the kernel schedule (threads per particle 1, 2 or 4; fused
+        second half-kick; list entries in flight 4 or 8; early list
+        requests), or hand it back to the autotuner with threads_per_particle
+        0."""
+        sched = (ctypes.c_int32 * 4)(int(threads_per_particle), 1 if fuse_post else 0,
+                                     int(batch_depth), 1 if prefetch else 0)
+        _lib.check(self._lib.beads_set_tuning(self._h, sched))
+
+    def tuning(self) -> dict:
+        out = (ctypes.c_int32 * 5)()
+        _lib.check(self._lib.beads_get_tuning(self._h, out))
+        return {"threads_per_particle": out[0], "fuse_post": bool(out[1]),
+                "batch_depth": out[2], "prefetch": bool(out[3]), "autotuned": bool(out[4])}
+
     def counters(self, replica: int = 0) -> dict:
-        """Completed steps, neighbour builds and dangerous rebuilds."""
-        out = (ctypes.c_uint64 * 3)()
+        """Completed steps, neighbour builds and dangerous rebuilds of one
+        replica; launches of the rebuild chain (whole batch)."""
+        out = (ctypes.c_uint64 * 4)()
         _lib.check(self._lib.beads_counters(self._h, int(replica), out))
-        return {"steps": int(out[0]), "builds": int(out[1]), "dangerous": int(out[2])}
+        return {"steps": int(out[0]), "builds": int(out[1]), "dangerous": int(out[2]),
+                "chain_launches": int(out[3])}
 
     def list_stats(self) -> dict:
         total = ctypes.c_uint64()

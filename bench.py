@@ -42,6 +42,7 @@ METRIC = "atom-steps/s on 1 B200 (1M-bead binary LJ mixture, FP32 pair math, fix
 UNIT = "atom-steps/s"
 N_BEADS = 1_048_576
 E2E_STEPS = 100  # MD steps per end-to-end call
+GRAPH_WARMUP = 127  # untimed steps that instantiate every captured step graph
 
 
 def _dist():
@@ -280,6 +281,9 @@ def run_ours(args) -> None:
     # the kernel-level timing below).
     for _ in range(max(3, args.warmup)):
         eng.run(1)
+    # Runs replay captured graphs of 64, 32, ..., 1 steps; one untimed run of
+    # 127 steps instantiates each of them outside the timed region.
+    eng.run(GRAPH_WARMUP)
     stats = eng.list_stats()
     mean_nbr = stats["entries"] / spec.n
 
@@ -288,7 +292,7 @@ def run_ours(args) -> None:
             dist.barrier()
         torch.cuda.synchronize()
 
-    builds_before = eng.counters()["builds"]
+    c0 = eng.counters()
     profile_region = os.environ.get("BEADS_PROFILE_TIMED") == "1"
     sampler = ClockSampler(local)
     barrier()
@@ -305,7 +309,9 @@ def run_ours(args) -> None:
         torch.cuda.profiler.stop()
     barrier()
     clocks = sampler.stop()
-    timed_builds = eng.counters()["builds"] - builds_before
+    c1 = eng.counters()
+    timed_builds = c1["builds"] - c0["builds"]
+    timed_chains = c1["chain_launches"] - c0["chain_launches"]
     elapsed_ms = start.elapsed_time(stop)
     if dist is not None:
         t = torch.tensor([elapsed_ms], device="cuda")
@@ -356,9 +362,11 @@ def run_ours(args) -> None:
         st = eng.state()
         cpu = _cpu_baseline(st["positions"], spec, args.cpu_budget)
 
-    # Every step launches pre and the fused force kernel; a step that rebuilds
-    # also runs the 7 kernels of the rebuild chain (conditional graph node).
-    gpu_launches = 2 * args.steps + 7 * int(timed_builds)
+    # Every step launches pre, the pair-force kernel and (unless the schedule
+    # fuses it) post; a step that rebuilds also runs the 7 kernels of the
+    # rebuild chain (conditional graph node).
+    per_step = 2 if eng.tuning()["fuse_post"] else 3
+    gpu_launches = per_step * args.steps + 7 * int(timed_chains)
     line = {
         "metric": METRIC,
         "value": value,
@@ -380,6 +388,8 @@ def run_ours(args) -> None:
             "mean_neighbors": round(mean_nbr, 2),
             "max_neighbors_seen": stats["max"],
             "neighbor_builds_timed": int(timed_builds),
+            "graph_warmup_steps": GRAPH_WARMUP,
+            "schedule": eng.tuning(),
         },
         "roofline": {
             "bound": "hbm",
@@ -428,7 +438,9 @@ def run_replicas(args) -> None:
     eng = Engine(specs)
     stream = torch.cuda.ExternalStream(eng.info()["stream"], device=torch.device("cuda", local))
     eng.run(max(3, args.warmup))
+    eng.run(GRAPH_WARMUP)
     builds_before = sum(eng.counters(r)["builds"] for r in range(len(specs)))
+    chains_before = eng.counters()["chain_launches"]
     sampler = ClockSampler(local)
     torch.cuda.synchronize()
     sampler.start()
@@ -441,6 +453,8 @@ def run_replicas(args) -> None:
     clocks = sampler.stop()
     batch_ms = start.elapsed_time(stop)
     builds = sum(eng.counters(r)["builds"] for r in range(len(specs))) - builds_before
+    chains = eng.counters()["chain_launches"] - chains_before
+    schedule = eng.tuning()
     value = atoms * args.steps / (batch_ms / 1e3)
     eng.close()
 
@@ -483,8 +497,11 @@ def run_replicas(args) -> None:
             "sequential_steps_per_replica": seq_steps,
             "batch_over_sequential": value / seq_value,
             "neighbor_builds_timed": int(builds),
+            "rebuild_chain_launches_timed": int(chains),
+            "graph_warmup_steps": GRAPH_WARMUP,
+            "schedule": schedule,
         },
-        "gpu_launches": 2 * args.steps + 7 * int(builds),
+        "gpu_launches": (2 if schedule["fuse_post"] else 3) * args.steps + 7 * int(chains),
         "clocks": clocks,
     }
     if rank == 0:

@@ -266,9 +266,54 @@ BEADS_API int beads_profile(beads_ctx* ctx, int32_t stage, uint32_t reps,
 BEADS_API int beads_list_stats(beads_ctx* ctx, uint64_t* total_entries,
                                uint32_t* max_count);
 
+/* Kernel schedule of a context, as five int32 values:
+ *   schedule[0] threads per particle of the pair-force kernel: 1, 2 or 4
+ *   schedule[1] second half-kick inside the last force kernel (1) or as its
+ *               own kernel (0)
+ *   schedule[2] batch depth: neighbour-list entries in flight per thread, 4/8
+ *   schedule[3] list entries of the next batch requested early (1) or not (0)
+ *   schedule[4] (get only) 1 if the autotuner chose the schedule
+ * The choice never changes a result (forces are summed in one canonical
+ * order).  By default the first beads_run() times the candidates on the
+ * context's own batch and keeps the fastest; beads_set_tuning() with
+ * schedule[0] = 1, 2 or 4 fixes the schedule (entries 0-3 read), 0 returns it
+ * to the autotuner.  No reference counterpart (the reference has one fixed
+ * launch shape per kernel). */
+BEADS_API int beads_set_tuning(beads_ctx* ctx, const int32_t* schedule);
+BEADS_API int beads_get_tuning(beads_ctx* ctx, int32_t* schedule);
+
+/* ---- differentiation (no reference counterpart) ------------------------- */
+/* Replaces one replica's LJ tables (symmetric [n_types * n_types], same
+ * meaning as beads_forcefield_desc.lj_epsilon / lj_sigma); the cutoff and
+ * shift setting stay.  The next step re-evaluates forces. */
+BEADS_API int beads_set_lj(beads_ctx* ctx, uint32_t replica, const double* epsilon,
+                           const double* sigma);
+/* Runs `steps` MD steps from the current state (list and forces rebuilt
+ * first) keeping a checkpoint of the full step state every
+ * `checkpoint_every` steps, and writes the observables of steps
+ * record_from..steps: observables[((step - record_from) * n_replicas + r) * 3
+ * + {0, 1, 2}] = potential energy, virial (sum r.F), kinetic energy (as a
+ * thermo row reports them).  Pair-only systems with up to 4 particle types.
+ * Slots are not reordered during the run. */
+BEADS_API int beads_adjoint_forward(beads_ctx* ctx, uint64_t steps, uint64_t record_from,
+                                    uint32_t checkpoint_every, double* observables);
+/* Reverse pass of the last beads_adjoint_forward(): given dL/d(observables)
+ * in the same layout, writes dL/d(epsilon) and dL/d(sigma) per replica and
+ * ordered type pair ([r][n_types * n_types], concatenated over replicas in
+ * order, each replica with its own n_types) and dL/d(initial positions),
+ * dL/d(initial velocities) in tag order ([n_particles_total][3]).  The
+ * segments between checkpoints are replayed with the neighbour list of each
+ * forward step frozen; afterwards the context is in its end-of-forward
+ * state. */
+BEADS_API int beads_adjoint_backward(beads_ctx* ctx, const double* observables_grad,
+                                     double* grad_epsilon, double* grad_sigma,
+                                     float* grad_positions, float* grad_velocities);
+
 /* Device counters of one replica, without stepping it: counters[0] completed
  * MD steps, [1] neighbour builds, [2] dangerous rebuilds (the quantities the
- * reference's run log reports, log_output.cpp:370-404). */
+ * reference's run log reports, log_output.cpp:370-404), [3] launches of the
+ * rebuild chain so far for the whole context (a captured step launches the
+ * chain only when some replica rebuilds).  counters has 4 entries. */
 BEADS_API int beads_counters(beads_ctx* ctx, uint32_t replica, uint64_t* counters);
 
 /* Steepest descent with a per-particle displacement cap, used to relax

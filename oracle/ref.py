@@ -5,9 +5,11 @@ TEST INFRASTRUCTURE ONLY.  Both precisions export a module named ``_native``,
 so each run happens in a fresh subprocess that loads exactly one of them.
 
     python -m oracle.ref <f32|f64> <spec.json> <spec.npz> <workdir>
+    python -m oracle.ref <f32|f64> --many <root> <count>
 
 runs ``_native.execute_simulation(spec)`` with ``workdir`` as the current
-directory (the spec's output prefixes are relative to it).
+directory (the spec's output prefixes are relative to it); ``--many`` runs
+<root>/0 .. <root>/<count-1> one after another in one process.
 """
 
 from __future__ import annotations
@@ -94,13 +96,44 @@ def run(precision: str, spec: dict, workdir: pathlib.Path, timeout: float = 1800
                     str(workdir)], check=True, env=env, timeout=timeout)
 
 
-def main(argv: list[str]) -> None:
-    precision, jp, npz, workdir = argv
-    spec = load_spec(pathlib.Path(jp), pathlib.Path(npz))
+def run_many(precision: str, specs: list[dict], workdir: pathlib.Path,
+             timeout: float = 3600.0) -> list[pathlib.Path]:
+    """Runs every spec in turn in ONE subprocess (one module load); spec k runs
+    in workdir/k.  Returns the run directories."""
+    workdir = pathlib.Path(workdir)
+    dirs = []
+    for k, spec in enumerate(specs):
+        d = workdir / str(k)
+        d.mkdir(parents=True, exist_ok=True)
+        save_spec(spec, d / "spec.json", d / "spec.npz")
+        dirs.append(d)
+    env = dict(os.environ)
+    env["PYTHONPATH"] = str(ROOT) + os.pathsep + env.get("PYTHONPATH", "")
+    subprocess.run([sys.executable, "-m", "oracle.ref", precision, "--many", str(workdir),
+                    str(len(specs))], check=True, env=env, timeout=timeout)
+    return dirs
+
+
+def _prepare(spec: dict, precision: str) -> dict:
     if precision == "f64":
         # The double build takes float64 reals; the float32 inputs convert exactly.
         for key in ("box_bound", "positions", "velocities", "masses"):
             spec["system"][key] = np.ascontiguousarray(spec["system"][key], dtype=np.float64)
+    return spec
+
+
+def main(argv: list[str]) -> None:
+    if len(argv) == 4 and argv[1] == "--many":
+        precision, _, root, count = argv
+        mod = _load(precision)
+        for k in range(int(count)):
+            d = pathlib.Path(root) / str(k)
+            spec = _prepare(load_spec(d / "spec.json", d / "spec.npz"), precision)
+            os.chdir(d)
+            mod.execute_simulation(spec)
+        return
+    precision, jp, npz, workdir = argv
+    spec = _prepare(load_spec(pathlib.Path(jp), pathlib.Path(npz)), precision)
     mod = _load(precision)
     os.chdir(workdir)
     mod.execute_simulation(spec)

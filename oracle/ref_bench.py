@@ -6,7 +6,7 @@ initial neighbour build and every step).
 
 TEST INFRASTRUCTURE ONLY (needs a GPU and oracle/build_ref.py's output).
 
-    python -m oracle.ref_bench <out.json> [--quick]
+    python -m oracle.ref_bench <out.json> [--quick] [--replicas]
 """
 
 from __future__ import annotations
@@ -47,9 +47,39 @@ def _relaxed_mixture(n: int):
     return spec
 
 
+def _replica_batch(steps: int, count: int) -> dict:
+    """The uneven 512-replica batch: the reference engine one replica at a
+    time (its own timer per run, summed) against one batched beads_b200 engine
+    (wall time of the whole run(), including its first neighbour build and
+    schedule autotuning)."""
+    import time
+
+    specs = workloads.replica_batch(count)
+    atoms = sum(r.n for r in specs)
+    with tempfile.TemporaryDirectory() as tmp:
+        dirs = ref.run_many("f32", [spec_for(r, steps, "run", forces=False, thermo_every=steps)
+                                    for r in specs], pathlib.Path(tmp))
+        ref_s = sum(steps / _sps(d / "run.log") for d in dirs)
+    with Engine(specs) as eng:
+        eng.eval()
+        t0 = time.perf_counter()
+        eng.run(steps)
+        ours_s = time.perf_counter() - t0
+    return {"replicas": count, "atoms": atoms, "steps": steps,
+            "reference_sequential_s": ref_s,
+            "reference_atom_steps_per_s": atoms * steps / ref_s,
+            "ours_batched_s": ours_s, "ours_atom_steps_per_s": atoms * steps / ours_s,
+            "speedup": ref_s / ours_s}
+
+
 def main(argv: list[str]) -> None:
     out_path = pathlib.Path(argv[0])
     quick = "--quick" in argv
+    if "--replicas" in argv:
+        entry = _replica_batch(100 if quick else 500, 64 if quick else 512)
+        print("replicas", json.dumps(entry))
+        out_path.write_text(json.dumps({"replica_batch": entry}, indent=1))
+        return
     cases = [("lattice_4096", workloads.lj_lattice(n_side=16), 5000)]
     n_mix = 131072 if quick else 1_048_576
     cases.append((f"mixture_{n_mix}", _relaxed_mixture(n_mix), 200 if quick else 2000))
