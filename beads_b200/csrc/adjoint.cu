@@ -70,6 +70,7 @@ struct AdjView {
   const float4* ck_ref_pos;
   const int* list_src;   // per replica: -1 checkpoint build positions, else step index
   const int* shift_on;   // per replica: LJ energy shift active
+  long long* dot;        // [2 lanes][R][whole, frac]: sum u_bar . v, double-buffered
   uint32_t slots;
   uint32_t replicas;
 };
@@ -109,8 +110,8 @@ __global__ void k_adj_mark_all(DeviceView v) {
 }
 
 // Step m, part 1: kinetic-energy and Berendsen adjoints, v_bar, F_bar.
-// Reads the sum u_bar_m+1 . v_m from accumulator lane `lane_in` (written by
-// the pair kernel of step m+1) and clears it in its last block.
+// Reads the sum u_bar_m+1 . v_m from lane `lane_in` of a.dot (written by the
+// pair kernel of step m+1) and clears it in its last block.
 __global__ void __launch_bounds__(kBlock)
 k_adj_prepare(DeviceView v, AdjView a, uint32_t m, uint32_t k, int first, int last,
               int lane_in) {
@@ -123,7 +124,8 @@ k_adj_prepare(DeviceView v, AdjView a, uint32_t m, uint32_t k, int first, int la
   const double lam = a.seg_lam[(size_t)k * v.n_replicas + r];
   const double kin = a.seg_kin[(size_t)k * v.n_replicas + r];
   const double g_ke = a.obs_grad[((size_t)m * v.n_replicas + r) * 3 + 2];
-  const double dot = last ? 0.0 : from_fixed(st->acc[lane_in], st->acc_frac[lane_in]);
+  long long* din = a.dot + ((size_t)lane_in * v.n_replicas + r) * 2;
+  const double dot = last ? 0.0 : from_fixed(din[0], din[1]);
   double gp = 0.0;
   if (!first && p.thermostat == 1 && kin > 0.0 && p.dof > 0.0 && lam > 0.0) {
     const double c = (double)p.dt / p.tau;
@@ -153,8 +155,8 @@ k_adj_prepare(DeviceView v, AdjView a, uint32_t m, uint32_t k, int first, int la
   }
   const uint32_t n_blocks = p.n_pad / kBlock;
   if (arrive_last(&st->done_post, n_blocks) && threadIdx.x == 0) {
-    st->acc[lane_in] = 0;
-    st->acc_frac[lane_in] = 0;
+    din[0] = 0;
+    din[1] = 0;
     st->done_post = 0u;
   }
 }
@@ -166,7 +168,7 @@ __device__ __forceinline__ void add_typed(float (&acc)[kAdjTypes], int t, float 
 
 // Step m, part 2: x_bar += g_PE grad PE + g_W grad W + J F_bar over the LJ
 // pairs, parameter adjoints, then u_bar_m and the sum u_bar_m . v_m-1 (lane
-// `lane_out`).  Positions in v.pos are x_m.
+// `lane_out` of a.dot).  Positions in v.pos are x_m.
 __global__ void __launch_bounds__(kBlock)
 k_adj_lj(DeviceView v, AdjView a, uint32_t m, uint32_t k, int first, int lane_out) {
   const uint32_t b = blockIdx.x;
@@ -257,7 +259,10 @@ k_adj_lj(DeviceView v, AdjView a, uint32_t m, uint32_t k, int first, int lane_ou
       dot = (double)ub.x * vp.x + (double)ub.y * vp.y + (double)ub.z * vp.z;
     }
   }
-  if (!first) block_add_lane<kBlock>(real, dot, st, lane_out);
+  if (!first) {
+    long long* dout = a.dot + ((size_t)lane_out * v.n_replicas + r) * 2;
+    block_add_fixed<kBlock>(real ? to_fixed(dot, &st->status) : Fixed{0, 0}, dout, dout + 1);
+  }
   if (real) {
     for (int c = 0; c < nt; ++c) {
       const int slot = (ti * kAdjTypes + c) * 2;
@@ -345,7 +350,8 @@ void Engine::adjoint_record(uint32_t k) {
 }
 
 // Puts the particle state of checkpoint c back, with the neighbour list the
-// forward run had at that point (rebuilt from its build positions).
+// forward run had at that point (rebuilt from its build positions) and the
+// forces of that state.
 void Engine::adjoint_restore(uint32_t c) {
   AdjointStore& A = *adj_;
   const size_t S = A.slots;
@@ -366,6 +372,10 @@ void Engine::adjoint_restore(uint32_t c) {
   cuda_check(cudaMemcpyAsync(v_.rs, A.ck_state.data() + static_cast<size_t>(c) * A.replicas,
                              A.replicas * sizeof(ReplicaState), cudaMemcpyHostToDevice, stream_),
              "adjoint restore");
+  // The next step's pre-kick reads the forces of this state: recompute them
+  // on the restored list (every schedule sums in the same order, so these
+  // are the forward run's bits).
+  launch_forces(launch_, false, false, false);
   sync();
 }
 
@@ -479,6 +489,7 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
     A.list_src = A.alloc<int>(R);
     A.shift_on = A.alloc<int>(R);
     A.list_changed = A.alloc<uint32_t>(R);
+    A.dot = A.alloc<long long>(static_cast<size_t>(R) * 4);
   }
   if (A.obs_capacity < (T + 1) * R * 3) {
     A.obs_capacity = (T + 1) * R * 3;
@@ -504,18 +515,7 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
   cuda_check(cudaMemset(A.vbar, 0, S * sizeof(float4)), "memset");
   cuda_check(cudaMemset(A.theta, 0, static_cast<size_t>(R) * kAdjTypes * kAdjTypes * 4 * 8),
              "memset");
-  {
-    // accumulator lanes used by the adjoint start at zero
-    std::vector<ReplicaState> st(R);
-    cuda_check(cudaMemcpy(st.data(), v_.rs, R * sizeof(ReplicaState), cudaMemcpyDeviceToHost),
-               "state");
-    for (auto& x : st) {
-      x.acc[kAccAdjoint] = x.acc_frac[kAccAdjoint] = 0;
-      x.acc[kAccAdjoint + 1] = x.acc_frac[kAccAdjoint + 1] = 0;
-    }
-    cuda_check(cudaMemcpy(v_.rs, st.data(), R * sizeof(ReplicaState), cudaMemcpyHostToDevice),
-               "state");
-  }
+  cuda_check(cudaMemset(A.dot, 0, static_cast<size_t>(R) * 4 * sizeof(long long)), "memset");
 
   AdjView av{};
   av.seg_pos = A.seg_pos;
@@ -531,6 +531,7 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
   av.ck_ref_pos = A.ck_ref_pos;
   av.list_src = d_src;
   av.shift_on = d_shift;
+  av.dot = A.dot;
   av.slots = A.slots;
   av.replicas = R;
 
@@ -587,8 +588,8 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
                  "adjoint positions");
       const int first = (m == 0) ? 1 : 0;
       const int last = (m == T) ? 1 : 0;
-      const int lane_in = kAccAdjoint + static_cast<int>((m + 1) & 1u);
-      const int lane_out = kAccAdjoint + static_cast<int>(m & 1u);
+      const int lane_in = static_cast<int>((m + 1) & 1u);
+      const int lane_out = static_cast<int>(m & 1u);
       k_adj_prepare<<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, static_cast<uint32_t>(m), k,
                                                         first, last, lane_in);
       launch_check("adjoint prepare");

@@ -56,6 +56,7 @@ struct AdjointStore {
   int* list_src = nullptr;       // [R] list build source of the replayed step
   int* shift_on = nullptr;       // [R] LJ energy shift active
   uint32_t* list_changed = nullptr;  // [R]
+  long long* dot = nullptr;          // [2][R][2] sum u_bar . v (fixed point)
 
   std::vector<void*> allocations;
   ~AdjointStore();

@@ -38,7 +38,6 @@ enum AccLane : int {
   kAccDihedral = 3,
   kAccVirial = 4,
   kAccKinetic = 5,
-  kAccAdjoint = 6,  // adjoint: sum of u_bar . v (Berendsen scale adjoint)
   kAccLanes = 8
 };
 

@@ -285,6 +285,50 @@ class Engine:
         return {"threads_per_particle": out[0], "fuse_post": bool(out[1]),
                 "batch_depth": out[2], "prefetch": bool(out[3]), "autotuned": bool(out[4])}
 
+    # -- differentiation ------------------------------------------------------
+    def set_lj(self, replica: int, epsilon, sigma) -> None:
+        """Replace one replica's LJ tables (symmetric n_types x n_types)."""
+        eps = np.ascontiguousarray(epsilon, dtype=np.float64)
+        sig = np.ascontiguousarray(sigma, dtype=np.float64)
+        nt = len(self.replicas[replica].epsilon)
+        if eps.shape != (nt, nt) or sig.shape != (nt, nt):
+            raise ValueError(f"LJ tables of replica {replica} must be {nt} x {nt}.")
+        _lib.check(self._lib.beads_set_lj(self._h, int(replica), eps.ctypes.data,
+                                          sig.ctypes.data))
+
+    def adjoint_forward(self, steps: int, record_from: int, checkpoint_every: int) -> np.ndarray:
+        """Run `steps` steps keeping checkpoints; returns [PE, virial, KE] of
+        steps record_from..steps, shape (steps - record_from + 1, R, 3)."""
+        out = np.zeros((int(steps) - int(record_from) + 1, len(self.replicas), 3), np.float64)
+        _lib.check(self._lib.beads_adjoint_forward(self._h, int(steps), int(record_from),
+                                                   int(checkpoint_every), out.ctypes.data))
+        self.step += int(steps)
+        self._adjoint_shape = out.shape
+        return out
+
+    def adjoint_backward(self, obs_grad) -> tuple[list, list, np.ndarray, np.ndarray]:
+        """dL/d(eps), dL/d(sigma) (one n_types x n_types array per replica,
+        per ordered type pair) and dL/d(x0), dL/d(v0) (tag order) for the
+        last adjoint_forward, given dL/d(observables)."""
+        g = np.ascontiguousarray(obs_grad, dtype=np.float64)
+        if g.shape != getattr(self, "_adjoint_shape", None):
+            raise ValueError("observable gradient does not match the last adjoint_forward.")
+        sizes = [len(spec.epsilon) for spec in self.replicas]
+        n_par = sum(nt * nt for nt in sizes)
+        ge = np.zeros(n_par, np.float64)
+        gs = np.zeros(n_par, np.float64)
+        gx = np.zeros((int(self.offsets[-1]), 3), np.float32)
+        gv = np.zeros((int(self.offsets[-1]), 3), np.float32)
+        _lib.check(self._lib.beads_adjoint_backward(self._h, g.ctypes.data, ge.ctypes.data,
+                                                    gs.ctypes.data, gx.ctypes.data,
+                                                    gv.ctypes.data))
+        out_e, out_s, at = [], [], 0
+        for nt in sizes:
+            out_e.append(ge[at:at + nt * nt].reshape(nt, nt))
+            out_s.append(gs[at:at + nt * nt].reshape(nt, nt))
+            at += nt * nt
+        return out_e, out_s, gx, gv
+
     def counters(self, replica: int = 0) -> dict:
         """Completed steps, neighbour builds and dangerous rebuilds of one
         replica; launches of the rebuild chain (whole batch)."""

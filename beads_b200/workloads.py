@@ -224,3 +224,35 @@ def replica_batch(n_replicas: int = 512, n_min: int = 256, n_max: int = 32768, s
             units="reduced", velocities=vel, masses=masses.astype(np.float32),
             cutoff_buffer=skin, max_neighbors=max_neighbors, thermostat=(t_target, 1.0)))
     return out
+
+
+def fit_mixture(n_replicas: int = 64, n: int = 8192, density: float = 0.8,
+                temperature: float = 1.0, tau: float = 1.0, dt: float = 0.005, seed: int = 21,
+                skin: float = 0.3, max_neighbors: int = 192) -> list[ReplicaSpec]:
+    """Replicas of the binary mixture in reduced units (sigma11 = 1: the
+    nm_kjmol mixture's tables divided by 0.34 nm, eps in kJ/mol as reduced
+    energies), 80/20 types, jittered simple-cubic lattice start, Berendsen."""
+    sig = MIXTURE_SIG / 0.34
+    out = []
+    side = int(math.ceil(n ** (1.0 / 3.0)))
+    length = (n / density) ** (1.0 / 3.0)
+    for r in range(n_replicas):
+        rng = np.random.default_rng(seed * 1009 + r)
+        g = np.indices((side,) * 3).reshape(3, -1).T.astype(np.float64)
+        g = g[np.sort(rng.permutation(g.shape[0])[:n])]
+        a = length / side
+        pos = _inside((g + 0.5) * a + rng.uniform(-0.05, 0.05, g.shape), np.zeros(3),
+                      np.full(3, length))
+        types = np.ones(n, np.int32)
+        types[rng.permutation(n)[: int(round(0.2 * n))]] = 2
+        masses = np.ones(n)
+        vel = _gaussian_velocities(rng, n, masses, temperature)
+        out.append(ReplicaSpec(
+            positions=pos, types=types,
+            box_bound=np.array([np.zeros(3), np.full(3, length)], np.float32),
+            epsilon=MIXTURE_EPS.copy(), sigma=sig, cutoff=0.9 / 0.34, dt=dt, units="reduced",
+            velocities=vel, masses=masses.astype(np.float32), shift=True, cutoff_buffer=skin,
+            max_neighbors=max_neighbors, sort_every_rebuild=10,
+            thermostat=(temperature, tau)))
+    return out
+
