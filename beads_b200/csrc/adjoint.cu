@@ -161,24 +161,58 @@ k_adj_prepare(DeviceView v, AdjView a, uint32_t m, uint32_t k, int first, int la
   }
 }
 
-__device__ __forceinline__ void add_typed(float (&acc)[kAdjTypes], int t, float v) {
+// Per type pair constants of the adjoint pair kernel.
+struct AdjCoeff {
+  float sigma2, eps4, eps24, shift;
+  float inv_eps;  // 1/eps (0 when eps = 0: the eps derivative is then 0)
+  float inv_sig;  // 1/sigma
+  float dshift;   // d(energy shift)/d(sigma)
+  float pad;
+};
+
+template <int kNt>
+__device__ __forceinline__ void add_typed(float (&acc)[kNt], int t, float v) {
 #pragma unroll
-  for (int c = 0; c < kAdjTypes; ++c) acc[c] += (c == t) ? v : 0.0f;
+  for (int c = 0; c < kNt; ++c) acc[c] += (c == t) ? v : 0.0f;
 }
 
 // Step m, part 2: x_bar += g_PE grad PE + g_W grad W + J F_bar over the LJ
 // pairs, parameter adjoints, then u_bar_m and the sum u_bar_m . v_m-1 (lane
-// `lane_out` of a.dot).  Positions in v.pos are x_m.
+// `lane_out` of a.dot).  `pos` holds x_m.  Batches of four list entries with
+// the next batch's entries requested early, as in the force kernel; kNt is
+// the LJ table side rounded up (2 or 4).
+template <int kNt>
 __global__ void __launch_bounds__(kBlock)
-k_adj_lj(DeviceView v, AdjView a, uint32_t m, uint32_t k, int first, int lane_out) {
+k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, uint32_t k,
+         int first, int lane_out) {
   const uint32_t b = blockIdx.x;
   const uint32_t r = v.block_replica[b];
   const ReplicaParams& p = v.rp[r];
   ReplicaState* st = &v.rs[r];
-  __shared__ LjCoeff table[kAdjTypes * kAdjTypes];
+  __shared__ AdjCoeff table[kNt * kNt];
   __shared__ unsigned long long theta_sh[kAdjTypes * kAdjTypes * 2 * 2];
   const int nt = p.n_types;
-  for (int t = threadIdx.x; t < nt * nt; t += kBlock) table[t] = v.lj[p.lj_offset + t];
+  const float rc2 = p.force_cut_sq;
+  const bool shift_on = a.shift_on[r] != 0;
+  for (int t = threadIdx.x; t < nt * nt; t += kBlock) {
+    const LjCoeff c = v.lj[p.lj_offset + t];
+    AdjCoeff q;
+    q.sigma2 = c.sigma2;
+    q.eps4 = c.eps4;
+    q.eps24 = c.eps24;
+    q.shift = c.shift;
+    q.inv_eps = c.eps4 != 0.0f ? 4.0f / c.eps4 : 0.0f;
+    const float sig = sqrtf(c.sigma2);
+    q.inv_sig = 1.0f / sig;
+    q.dshift = 0.0f;
+    if (shift_on) {
+      const float sc2 = c.sigma2 / rc2;
+      const float sc6 = sc2 * sc2 * sc2;
+      q.dshift = c.eps4 * (12.0f * sc6 * sc6 - 6.0f * sc6) / sig;
+    }
+    q.pad = 0.0f;
+    table[(t / nt) * kNt + (t % nt)] = q;
+  }
   for (int t = threadIdx.x; t < kAdjTypes * kAdjTypes * 4; t += kBlock) theta_sh[t] = 0ull;
   __syncthreads();
 
@@ -186,61 +220,78 @@ k_adj_lj(DeviceView v, AdjView a, uint32_t m, uint32_t k, int first, int lane_ou
   const bool real = (i - p.atom_begin) < p.n_atoms;
   const float g_pe = (float)a.obs_grad[((size_t)m * v.n_replicas + r) * 3 + 0];
   const float g_w = (float)a.obs_grad[((size_t)m * v.n_replicas + r) * 3 + 1];
-  const bool shift_on = a.shift_on[r] != 0;
+  const float h_pe = 0.5f * g_pe, h_w = 0.5f * g_w;
   float gx = 0.f, gy = 0.f, gz = 0.f;
-  float te[kAdjTypes], ts[kAdjTypes];
+  float te[kNt], ts[kNt];
 #pragma unroll
-  for (int c = 0; c < kAdjTypes; ++c) te[c] = ts[c] = 0.f;
-  const float4 xi = v.pos[i];
+  for (int c = 0; c < kNt; ++c) te[c] = ts[c] = 0.f;
+  const float4 xi = pos[i];
   const int ti = __float_as_int(xi.w);
-  if (real) {
-    const float4 fi = a.fbar[i];
-    const uint32_t n = v.nbr_count[i];
-    const uint32_t* list = v.nbr + nbr_index(i, 0, v.nbr_stride);
-    const float rc2 = p.force_cut_sq;
-    for (uint32_t q = 0; q < n; ++q) {
-      const uint32_t j = list[(size_t)q * kGroup];
-      const float4 xj = v.pos[j];
-      const float dx = acc_delta(xi.x, xj.x, p.len[0], p.half[0]);
-      const float dy = acc_delta(xi.y, xj.y, p.len[1], p.half[1]);
-      const float dz = acc_delta(xi.z, xj.z, p.len[2], p.half[2]);
-      const float r2 = norm2(dx, dy, dz);
-      if (!(r2 < rc2)) continue;
-      const int tj = __float_as_int(xj.w);
-      const LjCoeff c = table[ti * nt + tj];
-      const float inv = 1.0f / r2;
+  const AdjCoeff* row = table + ti * kNt;
+  const float4 fi = a.fbar[i];
+  const uint32_t n = real ? v.nbr_count[i] : 0u;
+  const uint32_t n_warp = __reduce_max_sync(kFull, n);
+  const float hmin = fminf(p.half[0], fminf(p.half[1], p.half[2]));
+  const float half_min_sq = hmin * hmin;
+  const uint32_t* list = v.nbr + nbr_index(i, 0, v.nbr_stride);
+  constexpr uint32_t kU = 4;
+  uint32_t jn[kU];
+#pragma unroll
+  for (uint32_t u = 0; u < kU; ++u) jn[u] = u < n ? __ldcs(list + (size_t)u * kGroup) : i;
+  for (uint32_t k0 = 0; k0 < n_warp; k0 += kU) {
+    uint32_t j[kU];
+    float4 xj[kU], fj[kU];
+#pragma unroll
+    for (uint32_t u = 0; u < kU; ++u) j[u] = jn[u];
+#pragma unroll
+    for (uint32_t u = 0; u < kU; ++u) {
+      xj[u] = __ldg(&pos[j[u]]);
+      fj[u] = __ldg(&a.fbar[j[u]]);
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < kU; ++u) {
+      jn[u] = k0 + kU + u < n ? __ldcs(list + (size_t)(k0 + kU + u) * kGroup) : i;
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < kU; ++u) {
+      float dx = xi.x - xj[u].x, dy = xi.y - xj[u].y, dz = xi.z - xj[u].z;
+      float r2 = norm2(dx, dy, dz);
+      const bool far = r2 >= half_min_sq;
+      if (__any_sync(kFull, far)) {
+        if (far) {
+          dx = acc_delta(xi.x, xj[u].x, p.len[0], p.half[0]);
+          dy = acc_delta(xi.y, xj[u].y, p.len[1], p.half[1]);
+          dz = acc_delta(xi.z, xj[u].z, p.len[2], p.half[2]);
+          r2 = norm2(dx, dy, dz);
+        }
+      }
+      const bool in = (k0 + u < n) && r2 < rc2;
+      const int tj = __float_as_int(xj[u].w);
+      const AdjCoeff c = row[tj];
+      const float rr = in ? r2 : 1.0f;
+      const float inv = __fdividef(1.0f, rr);
       const float sr2 = c.sigma2 * inv;
       const float sr6 = sr2 * sr2 * sr2;
       const float sr12 = sr6 * sr6;
-      const float phi = c.eps24 * inv * (2.0f * sr12 - sr6);
-      const float psi = 4.0f * c.eps24 * inv * inv * (2.0f * sr6 - 7.0f * sr12);
-      const float4 fj = a.fbar[j];
-      const float ddx = fi.x - fj.x, ddy = fi.y - fj.y, ddz = fi.z - fj.z;
+      const float phi = in ? c.eps24 * inv * (2.0f * sr12 - sr6) : 0.0f;
+      const float psi = in ? 4.0f * c.eps24 * inv * inv * (2.0f * sr6 - 7.0f * sr12) : 0.0f;
+      const float ddx = fi.x - fj[u].x, ddy = fi.y - fj[u].y, ddz = fi.z - fj[u].z;
       const float d_dot = dx * ddx + dy * ddy + dz * ddz;
-      const float coef = psi * d_dot - g_pe * phi + g_w * (psi * r2 + 2.0f * phi);
+      const float coef = psi * d_dot - g_pe * phi + g_w * (psi * rr + 2.0f * phi);
       gx += phi * ddx + coef * dx;
       gy += phi * ddy + coef * dy;
       gz += phi * ddz + coef * dz;
       // Parameter adjoints of this ordered pair (the pair's PE and W are
       // split half and half between its two ordered entries).
       const float fd = fi.x * dx + fi.y * dy + fi.z * dz;
-      const float eps = 0.25f * c.eps4;
-      const float sig = sqrtf(c.sigma2);
-      const float u = c.eps4 * (sr12 - sr6) - c.shift;
-      const float w = phi * r2;
-      const float d_eps = eps != 0.0f ? (phi * fd + 0.5f * g_pe * u + 0.5f * g_w * w) / eps : 0.0f;
-      float dshift = 0.0f;
-      if (shift_on) {
-        const float sc2 = c.sigma2 / rc2;
-        const float sc6 = sc2 * sc2 * sc2;
-        dshift = c.eps4 * (12.0f * sc6 * sc6 - 6.0f * sc6) / sig;
-      }
-      const float dphi = c.eps24 * inv * (24.0f * sr12 - 6.0f * sr6) / sig;
-      const float du = c.eps4 * (12.0f * sr12 - 6.0f * sr6) / sig - dshift;
-      const float dw = c.eps24 * (24.0f * sr12 - 6.0f * sr6) / sig;
-      const float d_sig = dphi * fd + 0.5f * g_pe * du + 0.5f * g_w * dw;
-      add_typed(te, tj, d_eps);
-      add_typed(ts, tj, d_sig);
+      const float uu = c.eps4 * (sr12 - sr6) - c.shift;
+      const float d_eps = (phi * fd + h_pe * uu + h_w * phi * rr) * c.inv_eps;
+      const float qq = 24.0f * sr12 - 6.0f * sr6;
+      const float dphi = c.eps24 * inv * qq * c.inv_sig;
+      const float du = c.eps4 * (12.0f * sr12 - 6.0f * sr6) * c.inv_sig - c.dshift;
+      const float d_sig = dphi * fd + h_pe * du + h_w * dphi * rr;
+      add_typed<kNt>(te, tj, in ? d_eps : 0.0f);
+      add_typed<kNt>(ts, tj, in ? d_sig : 0.0f);
     }
   }
   double dot = 0.0;
@@ -583,9 +634,6 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
         sync();
         current = wanted;
       }
-      cuda_check(cudaMemcpyAsync(v_.pos, A.seg_pos + static_cast<size_t>(k) * S,
-                                 S * sizeof(float4), cudaMemcpyDeviceToDevice, stream_),
-                 "adjoint positions");
       const int first = (m == 0) ? 1 : 0;
       const int last = (m == T) ? 1 : 0;
       const int lane_in = static_cast<int>((m + 1) & 1u);
@@ -593,8 +641,16 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
       k_adj_prepare<<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, static_cast<uint32_t>(m), k,
                                                         first, last, lane_in);
       launch_check("adjoint prepare");
-      k_adj_lj<<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, static_cast<uint32_t>(m), k, first,
-                                                   lane_out);
+      const float4* pos_m = A.seg_pos + static_cast<size_t>(k) * S;
+      if (A.max_types <= 2) {
+        k_adj_lj<2><<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, pos_m,
+                                                        static_cast<uint32_t>(m), k, first,
+                                                        lane_out);
+      } else {
+        k_adj_lj<4><<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, pos_m,
+                                                        static_cast<uint32_t>(m), k, first,
+                                                        lane_out);
+      }
       launch_check("adjoint pair");
     }
     sync();

@@ -508,6 +508,100 @@ def run_replicas(args) -> None:
         print(json.dumps(line))
 
 
+ADJOINT_METRIC = ("differentiated atom-steps/s on 1 B200 (64 x 8192-bead LJ mixture, forward "
+                  "with checkpoints + adjoint backward, FP32 pair math)")
+
+
+def run_adjoint(args) -> None:
+    """The differentiable fit workload: 64 replicas of an 8192-bead binary LJ
+    mixture (reduced units, density 0.8, T 1.0 Berendsen tau 1, dt 0.005),
+    1000 steps, loss (<PE> - PE*)^2 + (<P> - P*)^2 over the last 200 steps
+    with seeded targets, gradients w.r.t. the 3 eps, 3 sigma and the initial
+    positions by the adjoint with a checkpoint every 50 steps.  Reports the
+    cost of forward + backward against the plain forward run."""
+    import torch
+
+    from beads_b200 import workloads
+    from beads_b200.adjoint import trajectory_observables
+    from beads_b200.engine import Engine
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    steps, every = args.adj_steps, 50
+    window = min(200, steps)
+    specs = workloads.fit_mixture(n_replicas=64, n=8192, seed=21 + rank)
+    atoms = sum(s.n for s in specs)
+    vols = torch.tensor([float(np.prod(np.asarray(s.box_bound[1], np.float64) - s.box_bound[0]))
+                         for s in specs])
+    rng = np.random.default_rng(5 + rank)
+    pe_t = torch.tensor(rng.uniform(-6.0, -5.0, len(specs)) * 8192)
+    p_t = torch.tensor(rng.uniform(0.5, 1.5, len(specs)))
+    x0 = torch.tensor(np.concatenate([s.positions for s in specs]), dtype=torch.float64)
+    v0 = torch.tensor(np.concatenate([s.velocities for s in specs]), dtype=torch.float64)
+    eps = torch.tensor(workloads.MIXTURE_EPS, dtype=torch.float64, requires_grad=True)
+    sig = torch.tensor(specs[0].sigma, dtype=torch.float64, requires_grad=True)
+    x = x0.clone().requires_grad_(True)
+    with Engine(specs) as eng:
+        stream = torch.cuda.ExternalStream(eng.info()["stream"],
+                                           device=torch.device("cuda", local))
+        eng.run(max(3, args.warmup))
+        eng.run(GRAPH_WARMUP)
+        # plain forward of the same length from the same start
+        eng.upload_all(x0.numpy().astype(np.float32), v0.numpy().astype(np.float32))
+        eng.run(1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        eng.run(steps)
+        b.record(stream)
+        b.synchronize()
+        plain_s = a.elapsed_time(b) / 1e3
+        # differentiated run (wall clock: host orchestration included)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        obs = trajectory_observables(eng, eps, sig, x, v0.clone(), steps=steps,
+                                     record_from=steps - window + 1, checkpoint_every=every)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        pe = obs[:, :, 0].mean(0)
+        press = ((2.0 * obs[:, :, 2] + obs[:, :, 1]) / (3.0 * vols)).mean(0)
+        loss = ((pe - pe_t) ** 2 + (press - p_t) ** 2).sum()
+        loss.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+    fwd_s, bwd_s = t1 - t0, t2 - t1
+    line = {
+        "metric": ADJOINT_METRIC,
+        "value": atoms * steps / (fwd_s + bwd_s),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * (fwd_s + bwd_s) / steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": "64 x 8192-bead binary LJ mixture (reduced, rho 0.8, T 1, Berendsen tau 1, "
+                        f"dt 0.005), {steps} steps, loss over the last {window} steps, checkpoint "
+                        f"every {every}",
+            "plain_forward_s": plain_s,
+            "adjoint_forward_s": fwd_s,
+            "backward_s": bwd_s,
+            "backward_over_plain_forward": bwd_s / plain_s,
+            "forward_plus_backward_over_plain_forward": (fwd_s + bwd_s) / plain_s,
+            "loss": float(loss),
+            "grad_eps": eps.grad.tolist(),
+            "grad_sigma": sig.grad.tolist(),
+            "grad_x0_norm": float(x.grad.norm()),
+        },
+    }
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__)
     parser.add_argument("--gpus", type=int, default=1)
@@ -520,9 +614,12 @@ def main() -> None:
                         help="seconds of host work for the whole reference arm")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
-    parser.add_argument("--workload", default="mixture", choices=["mixture", "replicas"],
+    parser.add_argument("--adj-steps", type=int, default=1000)
+    parser.add_argument("--workload", default="mixture",
+                        choices=["mixture", "replicas", "adjoint"],
                         help="mixture: the 1M-bead mixture (default); replicas: the "
-                             "512-replica batch beside one-at-a-time runs")
+                             "512-replica batch beside one-at-a-time runs; adjoint: the "
+                             "differentiable 64-replica fit")
     parser.add_argument("--replicas", type=int, default=512)
     parser.add_argument("--beads", type=int, default=N_BEADS,
                         help="system size (same density); profiling of small cases only")
@@ -533,6 +630,8 @@ def main() -> None:
         run_reference(args)
     elif args.workload == "replicas":
         run_replicas(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_ours(args)
 
