@@ -529,6 +529,8 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
     A.seg_lam = A.alloc<double>(static_cast<size_t>(K + 1) * R);
     A.seg_kin = A.alloc<double>(static_cast<size_t>(K + 1) * R);
     A.seg_flags = A.alloc<uint32_t>(static_cast<size_t>(K + 1) * R);
+    A.seg_src = A.alloc<int>(static_cast<size_t>(K + 1) * R);
+    A.seg_changed = A.alloc<uint32_t>(static_cast<size_t>(K + 1) * R);
   }
   if (!A.xbar) {
     A.xbar = A.alloc<float4>(S);
@@ -537,18 +539,14 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
     A.ubar = A.alloc<float4>(S);
     A.theta = A.alloc<long long>(static_cast<size_t>(R) * kAdjTypes * kAdjTypes * 4);
     A.tag_xfer = A.alloc<float>(3 * n_tags_);
-    A.list_src = A.alloc<int>(R);
     A.shift_on = A.alloc<int>(R);
-    A.list_changed = A.alloc<uint32_t>(R);
     A.dot = A.alloc<long long>(static_cast<size_t>(R) * 4);
   }
   if (A.obs_capacity < (T + 1) * R * 3) {
     A.obs_capacity = (T + 1) * R * 3;
     A.obs_grad = A.alloc<double>(A.obs_capacity);
   }
-  int* d_src = A.list_src;
   int* d_shift = A.shift_on;
-  uint32_t* d_changed = A.list_changed;
   {
     std::vector<double> g((T + 1) * R * 3, 0.0);
     std::copy(obs_grad, obs_grad + (T + 1 - A.record_from) * R * 3,
@@ -580,15 +578,16 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
   av.obs_grad = A.obs_grad;
   av.theta = A.theta;
   av.ck_ref_pos = A.ck_ref_pos;
-  av.list_src = d_src;
+  av.list_src = nullptr;
   av.shift_on = d_shift;
   av.dot = A.dot;
   av.slots = A.slots;
   av.replicas = R;
 
   std::vector<uint32_t> flags;
-  std::vector<int> current(R), wanted(R);
-  std::vector<uint32_t> changed(R);
+  std::vector<int> current(R), src_all;
+  std::vector<uint32_t> chg_all;
+  std::vector<char> any_k;
   for (int s = static_cast<int>(A.segments) - 1; s >= 0; --s) {
     const uint64_t a = static_cast<uint64_t>(s) * K;
     const uint64_t b = std::min<uint64_t>(a + K, T);
@@ -603,13 +602,18 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
     flags.resize(static_cast<size_t>(b - a + 1) * R);
     cuda_check(cudaMemcpy(flags.data(), A.seg_flags, flags.size() * sizeof(uint32_t),
                           cudaMemcpyDeviceToHost), "flags");
+    // The list each forward step m used: built at the replica's last rebuild
+    // at or before m inside this segment, else the checkpoint's.  Walking
+    // backwards, a replica's list is rebuilt when that source changes; the
+    // sources and change flags of the whole segment go to the device at once.
     std::fill(current.begin(), current.end(), -2);  // list state unknown
     const uint64_t m_lo = (s == 0) ? 0 : a + 1;
+    const size_t nk = static_cast<size_t>(b - a + 1);
+    src_all.assign(nk * R, -1);
+    chg_all.assign(nk * R, 0u);
+    any_k.assign(nk, 0);
     for (uint64_t m = b + 1; m-- > m_lo;) {
       const uint32_t k = static_cast<uint32_t>(m - a);
-      // The list the forward step m used: built at the replica's last rebuild
-      // at or before m inside this segment, else the checkpoint's.
-      bool any = false;
       for (uint32_t r = 0; r < R; ++r) {
         int src = -1;
         for (uint32_t q = k; q >= 1; --q) {
@@ -618,21 +622,27 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
             break;
           }
         }
-        wanted[r] = src;
-        changed[r] = (src != current[r]) ? 1u : 0u;
-        any = any || changed[r];
+        src_all[k * R + r] = src;
+        if (src != current[r]) {
+          chg_all[k * R + r] = 1u;
+          any_k[k] = 1;
+          current[r] = src;
+        }
       }
-      if (any) {
-        cuda_check(cudaMemcpyAsync(d_src, wanted.data(), R * sizeof(int), cudaMemcpyHostToDevice,
-                                   stream_), "adjoint list");
-        cuda_check(cudaMemcpyAsync(d_changed, changed.data(), R * sizeof(uint32_t),
-                                   cudaMemcpyHostToDevice, stream_), "adjoint list");
-        k_adj_list_positions<<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, static_cast<uint32_t>(s),
-                                                                  d_changed);
+    }
+    cuda_check(cudaMemcpy(A.seg_src, src_all.data(), nk * R * sizeof(int), cudaMemcpyHostToDevice),
+               "adjoint list sources");
+    cuda_check(cudaMemcpy(A.seg_changed, chg_all.data(), nk * R * sizeof(uint32_t),
+                          cudaMemcpyHostToDevice), "adjoint list sources");
+    for (uint64_t m = b + 1; m-- > m_lo;) {
+      const uint32_t k = static_cast<uint32_t>(m - a);
+      if (any_k[k]) {
+        AdjView lv = av;
+        lv.list_src = A.seg_src + static_cast<size_t>(k) * R;
+        k_adj_list_positions<<<v_.n_blocks, kBlock, 0, stream_>>>(
+            v_, lv, static_cast<uint32_t>(s), A.seg_changed + static_cast<size_t>(k) * R);
         launch_check("adjoint list positions");
         launch_rebuild(launch_, false);
-        sync();
-        current = wanted;
       }
       const int first = (m == 0) ? 1 : 0;
       const int last = (m == T) ? 1 : 0;

@@ -42,6 +42,8 @@ struct AdjointStore {
   double* seg_lam = nullptr;     // [k * R + r] Berendsen scale after step a+k
   double* seg_kin = nullptr;     // [k * R + r] kinetic energy after step a+k
   uint32_t* seg_flags = nullptr; // [k * R + r] replica rebuilt its list at step a+k
+  int* seg_src = nullptr;        // [k * R + r] step whose positions built step a+k's list
+  uint32_t* seg_changed = nullptr;  // [k * R + r] that list differs from step a+k+1's
   uint32_t seg_capacity = 0;     // K + 1 allocated
 
   // adjoint vectors (per slot) and reductions
@@ -53,9 +55,7 @@ struct AdjointStore {
   uint64_t obs_capacity = 0;
   long long* theta = nullptr;    // [R][types^2][eps, sigma][whole, frac]
   float* tag_xfer = nullptr;     // [3 * particles] tag-order staging
-  int* list_src = nullptr;       // [R] list build source of the replayed step
   int* shift_on = nullptr;       // [R] LJ energy shift active
-  uint32_t* list_changed = nullptr;  // [R]
   long long* dot = nullptr;          // [2][R][2] sum u_bar . v (fixed point)
 
   std::vector<void*> allocations;

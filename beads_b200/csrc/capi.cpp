@@ -383,12 +383,12 @@ int beads_set_tuning(beads_ctx* ctx, const int32_t* schedule) {
 int beads_get_tuning(beads_ctx* ctx, int32_t* schedule) {
   return guarded([&] {
     require(ctx && ctx->engine && schedule, "NULL argument.");
-    int t = 0, f = 0, u = 0, pf = 0, a = 0;
-    ctx->engine->tuning(&t, &f, &u, &pf, &a);
+    int t = 0, f = 0, u = 0, nl = 0, a = 0;
+    ctx->engine->tuning(&t, &f, &u, &nl, &a);
     schedule[0] = t;
     schedule[1] = f;
     schedule[2] = u;
-    schedule[3] = pf;
+    schedule[3] = nl;
     schedule[4] = a;
   });
 }

@@ -88,7 +88,7 @@ void Engine::clear_graphs() {
   graphs_.clear();
 }
 
-void Engine::set_tuning(int tpa, int fuse_post, int unroll, int prefetch) {
+void Engine::set_tuning(int tpa, int fuse_post, int unroll, int no_l1) {
   if (tpa == 0) {
     tuning_fixed_ = false;
     tuned_ = false;
@@ -99,16 +99,16 @@ void Engine::set_tuning(int tpa, int fuse_post, int unroll, int prefetch) {
   clear_graphs();
   launch_.lj_tpa = tpa;
   launch_.lj_unroll = unroll;
-  launch_.lj_prefetch = prefetch ? 1 : 0;
+  launch_.lj_no_l1 = no_l1 ? 1 : 0;
   launch_.fuse_post = fuse_post ? 1 : 0;
   tuning_fixed_ = true;
 }
 
-void Engine::tuning(int* tpa, int* fuse_post, int* unroll, int* prefetch, int* autotuned) const {
+void Engine::tuning(int* tpa, int* fuse_post, int* unroll, int* no_l1, int* autotuned) const {
   *tpa = launch_.lj_tpa;
   *fuse_post = launch_.fuse_post;
   *unroll = launch_.lj_unroll;
-  *prefetch = launch_.lj_prefetch;
+  *no_l1 = launch_.lj_no_l1;
   *autotuned = (tuned_ && !tuning_fixed_) ? 1 : 0;
 }
 
@@ -118,7 +118,7 @@ void Engine::tuning(int* tpa, int* fuse_post, int* unroll, int* prefetch, int* a
 // BEADS_TUNE_LOG=1 the timings go to stderr.
 void Engine::autotune() {
   if (!initialized_) eval();
-  constexpr int kWarm = 2, kReps = 8;
+  constexpr int kWarm = 1, kReps = 4;
   const bool log = [] {
     const char* e = std::getenv("BEADS_TUNE_LOG");
     return e && std::string(e) == "1";
@@ -143,8 +143,8 @@ void Engine::autotune() {
     float ms = 0.f;
     cuda_check(cudaEventElapsedTime(&ms, a, b), "event elapsed");
     if (log) {
-      std::fprintf(stderr, "beads autotune: tpa %d depth %d prefetch %d fuse_post %d: %.4f ms\n",
-                   l.lj_tpa, l.lj_unroll, l.lj_prefetch, l.fuse_post, ms / kReps);
+      std::fprintf(stderr, "beads autotune: tpa %d depth %d no_l1 %d fuse_post %d: %.4f ms\n",
+                   l.lj_tpa, l.lj_unroll, l.lj_no_l1, l.fuse_post, ms / kReps);
     }
     if (best == 0.f || ms < best) {
       best = ms;
@@ -156,11 +156,11 @@ void Engine::autotune() {
     // the best shape with the kick fused.
     for (int tpa : {1, 2, 4}) {
       for (int unroll : {8, 4}) {
-        for (int prefetch : {1, 0}) {
+        for (int no_l1 : {0, 1}) {
           StepLaunch l = launch_;
           l.lj_tpa = tpa;
           l.lj_unroll = unroll;
-          l.lj_prefetch = prefetch;
+          l.lj_no_l1 = no_l1;
           l.fuse_post = 0;
           trial(l);
         }
@@ -182,12 +182,12 @@ void Engine::autotune() {
                              cudaMemcpyHostToDevice, stream_), "state restore");
   sync();
   if (chosen.lj_tpa != launch_.lj_tpa || chosen.fuse_post != launch_.fuse_post ||
-      chosen.lj_unroll != launch_.lj_unroll || chosen.lj_prefetch != launch_.lj_prefetch) {
+      chosen.lj_unroll != launch_.lj_unroll || chosen.lj_no_l1 != launch_.lj_no_l1) {
     clear_graphs();
   }
   launch_.lj_tpa = chosen.lj_tpa;
   launch_.lj_unroll = chosen.lj_unroll;
-  launch_.lj_prefetch = chosen.lj_prefetch;
+  launch_.lj_no_l1 = chosen.lj_no_l1;
   launch_.fuse_post = chosen.fuse_post;
   tuned_ = true;
 }
@@ -574,8 +574,13 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   launch_.all_regular = all_regular ? 1 : 0;
   launch_.lj_tpa = 1;
   launch_.lj_unroll = 8;
-  launch_.lj_prefetch = 1;
+  launch_.lj_no_l1 = 0;
   launch_.fuse_post = 0;
+  {
+    int max_nt = 0;
+    for (uint32_t r = 0; r < n; ++r) max_nt = std::max(max_nt, ffs[r].n_types);
+    launch_.lj_types = max_nt;
+  }
   launch_.max_atoms_per_replica = max_atoms;
   launch_.excl_cap = excl_cap;
   launch_.need_kinetic = any_thermostat ? 1 : 0;

@@ -99,13 +99,13 @@ class Engine {
   void check_status();
   // Kernel schedule of the step: threads per particle of the pair-force
   // kernel (1, 2 or 4), its batch depth (4 or 8 list entries in flight per
-  // thread), whether it requests the next batch's list entries early, and
-  // whether the second half-kick runs inside the last force kernel.  Every choice gives bit-identical results.  tpa = 0 hands
+  // thread), whether its list loads bypass L1, and whether the second
+  // half-kick runs inside the last force kernel.  Every choice gives bit-identical results.  tpa = 0 hands
   // the choice back to the autotuner, which times every candidate on this
   // batch at the first run (velocities and step state restored) and keeps
   // the fastest.
-  void set_tuning(int tpa, int fuse_post, int unroll, int prefetch);
-  void tuning(int* tpa, int* fuse_post, int* unroll, int* prefetch, int* autotuned) const;
+  void set_tuning(int tpa, int fuse_post, int unroll, int no_l1);
+  void tuning(int* tpa, int* fuse_post, int* unroll, int* no_l1, int* autotuned) const;
   void autotune();
 
   // ---- adjoint (reverse-mode gradients of a trajectory; adjoint.cu) ----

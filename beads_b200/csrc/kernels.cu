@@ -651,7 +651,165 @@ struct LjAcc {
   }
 };
 
-template <bool kObs, int kMode, int kTpa, int kUnroll, bool kPrefetch>
+// A neighbour-list entry: streamed (evict-first in L1) or not allocated in
+// L1 at all (kNoL1), so the list stream does not displace gathered positions.
+template <bool kNoL1>
+__device__ __forceinline__ uint32_t list_load(const uint32_t* p) {
+  if (kNoL1) {
+    uint32_t v;
+    asm volatile("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+  }
+  return __ldcs(p);
+}
+
+// LJ coefficients of two pairs as packed pairs.  kNt = 1 (every replica has
+// one particle type): the row is held in registers and already packed;
+// kNt = 2: the particle's two-entry row in registers, selected by the
+// neighbour's type; kNt = 0: any table, read from shared memory.
+struct PairCoeff2 {
+  float2 sigma2, eps24, eps4, neg_shift;
+};
+
+template <int kNt>
+struct CoeffRow {
+  const LjCoeff* row;
+  LjCoeff r0, r1;
+  PairCoeff2 one;
+  __device__ __forceinline__ void init(const LjCoeff* table_row) {
+    row = table_row;
+    if (kNt >= 1) r0 = table_row[0];
+    if (kNt == 2) r1 = table_row[1];
+    if (kNt == 1) {
+      one.sigma2 = make_float2(r0.sigma2, r0.sigma2);
+      one.eps24 = make_float2(r0.eps24, r0.eps24);
+      one.eps4 = make_float2(r0.eps4, r0.eps4);
+      one.neg_shift = make_float2(-r0.shift, -r0.shift);
+    }
+  }
+  __device__ __forceinline__ PairCoeff2 get(float w0, float w1) const {
+    if (kNt == 1) return one;
+    PairCoeff2 c;
+    if (kNt == 2) {
+      const bool b0 = __float_as_int(w0) != 0, b1 = __float_as_int(w1) != 0;
+      c.sigma2 = make_float2(b0 ? r1.sigma2 : r0.sigma2, b1 ? r1.sigma2 : r0.sigma2);
+      c.eps24 = make_float2(b0 ? r1.eps24 : r0.eps24, b1 ? r1.eps24 : r0.eps24);
+      c.eps4 = make_float2(b0 ? r1.eps4 : r0.eps4, b1 ? r1.eps4 : r0.eps4);
+      c.neg_shift = make_float2(b0 ? -r1.shift : -r0.shift, b1 ? -r1.shift : -r0.shift);
+      return c;
+    }
+    const LjCoeff c0 = row[__float_as_int(w0)];
+    const LjCoeff c1 = row[__float_as_int(w1)];
+    c.sigma2 = make_float2(c0.sigma2, c1.sigma2);
+    c.eps24 = make_float2(c0.eps24, c1.eps24);
+    c.eps4 = make_float2(c0.eps4, c1.eps4);
+    c.neg_shift = make_float2(-c0.shift, -c1.shift);
+    return c;
+  }
+};
+
+// The pair loop of k_lj for one particle (see k_lj).  kFar = false drops the
+// straddling-pair test: valid for warps whose particles all lie at least rc
+// inside every face, where no pair within rc can straddle the boundary.
+template <bool kObs, bool kClamp, int kTpa, int kUnroll, bool kNoL1, bool kFar, int kNt>
+__device__ __forceinline__ void lj_pairs(const DeviceView& v, const ReplicaParams& p,
+                                         const CoeffRow<kNt>& coeff, float4 xi, uint32_t i,
+                                         uint32_t sub, uint32_t n, uint32_t n_warp, float rc2,
+                                         float half_min_sq, LjAcc<kTpa>& ax, LjAcc<kTpa>& ay,
+                                         LjAcc<kTpa>& az, LjAcc<kTpa>& ae, LjAcc<kTpa>& aw) {
+  const float2 xi2x = make_float2(xi.x, xi.x);
+  const float2 xi2y = make_float2(xi.y, xi.y);
+  const float2 xi2z = make_float2(xi.z, xi.z);
+  const uint32_t* list = v.nbr + nbr_index(i, 0, v.nbr_stride) + sub * kGroup;
+  // Software-pipelined over batches of kUnroll (4 or 8) own entries: all
+  // list loads of a batch are issued, then all position gathers, then the
+  // arithmetic, so a warp keeps kUnroll independent misses in flight
+  // instead of one (8: more misses in flight, 4: fewer registers and more
+  // resident warps).  The list is streamed (evict-first) so the positions
+  // stay in L2.
+  // The list entries of the next batch are requested before the arithmetic
+  // of the current one, so the (HBM) list latency overlaps it and only the
+  // (mostly L1/L2) position gathers stay on the critical path.  kNoL1 loads
+  // list entries without allocating L1 lines, leaving L1 to the gathers.
+  constexpr uint32_t kStep = kUnroll * kTpa;
+  uint32_t jn[kUnroll];
+#pragma unroll
+  for (uint32_t u = 0; u < kUnroll; ++u) {
+    const uint32_t k = u * kTpa + sub;
+    jn[u] = k < n ? list_load<kNoL1>(list + (size_t)(u * kTpa) * kGroup) : i;
+  }
+  for (uint32_t k0 = 0; k0 < n_warp; k0 += kStep) {
+    uint32_t j[kUnroll];
+#pragma unroll
+    for (uint32_t u = 0; u < kUnroll; ++u) j[u] = jn[u];
+    float4 xj[kUnroll];
+#pragma unroll
+    for (uint32_t u = 0; u < kUnroll; ++u) xj[u] = __ldg(&v.pos[j[u]]);
+#pragma unroll
+    for (uint32_t u = 0; u < kUnroll; ++u) {
+      const uint32_t k = k0 + kStep + u * kTpa + sub;
+      jn[u] = k < n ? list_load<kNoL1>(list + (size_t)(k0 + kStep + u * kTpa) * kGroup) : i;
+    }
+    // Own entries 2h and 2h+1 of the batch run through the packed FP32x2
+    // pipe of sm_100 (__fadd2_rn / __fmul2_rn / __ffma2_rn round each lane
+    // exactly as the scalar operation would).  Pairs beyond the cutoff and
+    // padding entries get a zero force scale rather than a branch.
+#pragma unroll
+    for (uint32_t h = 0; h < kUnroll / 2; ++h) {
+      const uint32_t u0 = 2 * h, u1 = 2 * h + 1;
+      float2 dx = __fadd2_rn(xi2x, make_float2(-xj[u0].x, -xj[u1].x));
+      float2 dy = __fadd2_rn(xi2y, make_float2(-xj[u0].y, -xj[u1].y));
+      float2 dz = __fadd2_rn(xi2z, make_float2(-xj[u0].z, -xj[u1].z));
+      float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+      // Plain differences are already the once-rounded exact values unless
+      // the pair straddles the periodic boundary, which needs r^2 above
+      // (L_min/2)^2; only then (warp-uniform branch) recompute that pair
+      // with the exactly rounded minimum image.
+      const bool far0 = r2.x >= half_min_sq, far1 = r2.y >= half_min_sq;
+      if (kFar && __any_sync(kFull, far0 || far1)) {
+        if (far0) {
+          dx.x = acc_delta(xi.x, xj[u0].x, p.len[0], p.half[0]);
+          dy.x = acc_delta(xi.y, xj[u0].y, p.len[1], p.half[1]);
+          dz.x = acc_delta(xi.z, xj[u0].z, p.len[2], p.half[2]);
+          r2.x = norm2(dx.x, dy.x, dz.x);
+        }
+        if (far1) {
+          dx.y = acc_delta(xi.x, xj[u1].x, p.len[0], p.half[0]);
+          dy.y = acc_delta(xi.y, xj[u1].y, p.len[1], p.half[1]);
+          dz.y = acc_delta(xi.z, xj[u1].z, p.len[2], p.half[2]);
+          r2.y = norm2(dx.y, dy.y, dz.y);
+        }
+      }
+      const bool in0 = (k0 + u0 * kTpa + sub < n) && r2.x < rc2;
+      const bool in1 = (k0 + u1 * kTpa + sub < n) && r2.y < rc2;
+      const PairCoeff2 c = coeff.get(xj[u0].w, xj[u1].w);
+      float2 rr = make_float2(in0 ? r2.x : 1.0f, in1 ? r2.y : 1.0f);
+      if (kClamp) {
+        rr.x = fmaxf(rr.x, 0.49f * c.sigma2.x);
+        rr.y = fmaxf(rr.y, 0.49f * c.sigma2.y);
+      }
+      const float2 inv = make_float2(__fdividef(1.0f, rr.x), __fdividef(1.0f, rr.y));
+      const float2 sr2 = __fmul2_rn(c.sigma2, inv);
+      const float2 sr6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
+      const float2 sr12 = __fmul2_rn(sr6, sr6);
+      const float2 neg6 = make_float2(-sr6.x, -sr6.y);
+      const float2 g = __ffma2_rn(make_float2(2.0f, 2.0f), sr12, neg6);
+      float2 fs = __fmul2_rn(__fmul2_rn(c.eps24, inv), g);
+      fs.x = in0 ? fs.x : 0.0f;
+      fs.y = in1 ? fs.y : 0.0f;
+      ax.add_fma(h, fs, dx);
+      ay.add_fma(h, fs, dy);
+      az.add_fma(h, fs, dz);
+      if (kObs) {
+        const float2 ep = __ffma2_rn(c.eps4, __fadd2_rn(sr12, neg6), c.neg_shift);
+        ae.add(h, make_float2(in0 ? ep.x : 0.0f, in1 ? ep.y : 0.0f));
+        aw.add_fma(h, fs, rr);
+      }
+    }
+  }
+}
+
+template <bool kObs, int kMode, int kTpa, int kUnroll, bool kNoL1, int kNt>
 __global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
   constexpr bool kClamp = kMode == kForceClamp;
   constexpr bool kPost = kMode >= kForcePost;
@@ -678,113 +836,30 @@ __global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
     // Every lane of the warp (padding lanes included, with n = 0) runs the
     // same number of batches, so the warp votes below are convergent.
     const float4 xi = v.pos[i];
-    const LjCoeff* row = table + __float_as_int(xi.w) * nt;
+    CoeffRow<kNt> coeff;
+    coeff.init(table + __float_as_int(xi.w) * nt);
     const uint32_t n = real ? v.nbr_count[i] : 0u;
     const uint32_t n_warp = __reduce_max_sync(kFull, n);
     const float rc2 = p.force_cut_sq;
     const float hmin = fminf(p.half[0], fminf(p.half[1], p.half[2]));
     const float half_min_sq = hmin * hmin;
-    const float2 xi2x = make_float2(xi.x, xi.x);
-    const float2 xi2y = make_float2(xi.y, xi.y);
-    const float2 xi2z = make_float2(xi.z, xi.z);
-    const uint32_t* list = v.nbr + nbr_index(i, 0, v.nbr_stride) + sub * kGroup;
-    // Software-pipelined over batches of kUnroll (4 or 8) own entries: all
-    // list loads of a batch are issued, then all position gathers, then the
-    // arithmetic, so a warp keeps kUnroll independent misses in flight
-    // instead of one (8: more misses in flight, 4: fewer registers and more
-    // resident warps).  The list is streamed (evict-first) so the positions
-    // stay in L2.
-    // kPrefetch: the list entries of the next batch are requested before the
-    // arithmetic of the current one, so the (HBM) list latency overlaps it and
-    // only the (mostly L1/L2) position gathers stay on the critical path.
-    constexpr uint32_t kStep = kUnroll * kTpa;
-    uint32_t jn[kUnroll];
-    if (kPrefetch) {
-#pragma unroll
-      for (uint32_t u = 0; u < kUnroll; ++u) {
-        const uint32_t k = u * kTpa + sub;
-        jn[u] = k < n ? __ldcs(list + (size_t)(u * kTpa) * kGroup) : i;
-      }
-    }
-    for (uint32_t k0 = 0; k0 < n_warp; k0 += kStep) {
-      uint32_t j[kUnroll];
-#pragma unroll
-      for (uint32_t u = 0; u < kUnroll; ++u) {
-        if (kPrefetch) {
-          j[u] = jn[u];
-        } else {
-          const uint32_t k = k0 + u * kTpa + sub;
-          j[u] = k < n ? __ldcs(list + (size_t)(k0 + u * kTpa) * kGroup) : i;
-        }
-      }
-      float4 xj[kUnroll];
-#pragma unroll
-      for (uint32_t u = 0; u < kUnroll; ++u) xj[u] = __ldg(&v.pos[j[u]]);
-      if (kPrefetch) {
-#pragma unroll
-        for (uint32_t u = 0; u < kUnroll; ++u) {
-          const uint32_t k = k0 + kStep + u * kTpa + sub;
-          jn[u] = k < n ? __ldcs(list + (size_t)(k0 + kStep + u * kTpa) * kGroup) : i;
-        }
-      }
-      // Own entries 2h and 2h+1 of the batch run through the packed FP32x2
-      // pipe of sm_100 (__fadd2_rn / __fmul2_rn / __ffma2_rn round each lane
-      // exactly as the scalar operation would).  Pairs beyond the cutoff and
-      // padding entries get a zero force scale rather than a branch.
-#pragma unroll
-      for (uint32_t h = 0; h < kUnroll / 2; ++h) {
-        const uint32_t u0 = 2 * h, u1 = 2 * h + 1;
-        float2 dx = __fadd2_rn(xi2x, make_float2(-xj[u0].x, -xj[u1].x));
-        float2 dy = __fadd2_rn(xi2y, make_float2(-xj[u0].y, -xj[u1].y));
-        float2 dz = __fadd2_rn(xi2z, make_float2(-xj[u0].z, -xj[u1].z));
-        float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-        // Plain differences are already the once-rounded exact values unless
-        // the pair straddles the periodic boundary, which needs r^2 above
-        // (L_min/2)^2; only then (warp-uniform branch) recompute that pair
-        // with the exactly rounded minimum image.
-        const bool far0 = r2.x >= half_min_sq, far1 = r2.y >= half_min_sq;
-        if (__any_sync(kFull, far0 || far1)) {
-          if (far0) {
-            dx.x = acc_delta(xi.x, xj[u0].x, p.len[0], p.half[0]);
-            dy.x = acc_delta(xi.y, xj[u0].y, p.len[1], p.half[1]);
-            dz.x = acc_delta(xi.z, xj[u0].z, p.len[2], p.half[2]);
-            r2.x = norm2(dx.x, dy.x, dz.x);
-          }
-          if (far1) {
-            dx.y = acc_delta(xi.x, xj[u1].x, p.len[0], p.half[0]);
-            dy.y = acc_delta(xi.y, xj[u1].y, p.len[1], p.half[1]);
-            dz.y = acc_delta(xi.z, xj[u1].z, p.len[2], p.half[2]);
-            r2.y = norm2(dx.y, dy.y, dz.y);
-          }
-        }
-        const bool in0 = (k0 + u0 * kTpa + sub < n) && r2.x < rc2;
-        const bool in1 = (k0 + u1 * kTpa + sub < n) && r2.y < rc2;
-        const LjCoeff c0 = row[__float_as_int(xj[u0].w)];
-        const LjCoeff c1 = row[__float_as_int(xj[u1].w)];
-        float2 rr = make_float2(in0 ? r2.x : 1.0f, in1 ? r2.y : 1.0f);
-        if (kClamp) {
-          rr.x = fmaxf(rr.x, 0.49f * c0.sigma2);
-          rr.y = fmaxf(rr.y, 0.49f * c1.sigma2);
-        }
-        const float2 inv = make_float2(__fdividef(1.0f, rr.x), __fdividef(1.0f, rr.y));
-        const float2 sr2 = __fmul2_rn(make_float2(c0.sigma2, c1.sigma2), inv);
-        const float2 sr6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
-        const float2 sr12 = __fmul2_rn(sr6, sr6);
-        const float2 neg6 = make_float2(-sr6.x, -sr6.y);
-        const float2 g = __ffma2_rn(make_float2(2.0f, 2.0f), sr12, neg6);
-        float2 fs = __fmul2_rn(__fmul2_rn(make_float2(c0.eps24, c1.eps24), inv), g);
-        fs.x = in0 ? fs.x : 0.0f;
-        fs.y = in1 ? fs.y : 0.0f;
-        ax.add_fma(h, fs, dx);
-        ay.add_fma(h, fs, dy);
-        az.add_fma(h, fs, dz);
-        if (kObs) {
-          const float2 ep = __ffma2_rn(make_float2(c0.eps4, c1.eps4), __fadd2_rn(sr12, neg6),
-                                       make_float2(-c0.shift, -c1.shift));
-          ae.add(h, make_float2(in0 ? ep.x : 0.0f, in1 ? ep.y : 0.0f));
-          aw.add_fma(h, fs, rr);
-        }
-      }
+    // A warp whose particles all sit at least rc (with a margin) inside
+    // every face has no pair within rc that straddles the boundary: its plain
+    // differences are the exactly rounded minimum images, so it runs the loop
+    // without the straddling test (same bits either way).
+    const float rcm = 1.001f * sqrtf(rc2) + 1e-6f * fmaxf(p.len[0], fmaxf(p.len[1], p.len[2]));
+    const bool inside = !real ||
+        (xi.x - p.lo[0] >= rcm && p.lo[0] + p.len[0] - xi.x > rcm &&
+         xi.y - p.lo[1] >= rcm && p.lo[1] + p.len[1] - xi.y > rcm &&
+         xi.z - p.lo[2] >= rcm && p.lo[2] + p.len[2] - xi.z > rcm);
+    if (__all_sync(kFull, inside)) {
+      lj_pairs<kObs, kClamp, kTpa, kUnroll, kNoL1, false, kNt>(v, p, coeff, xi, i, sub, n,
+                                                               n_warp, rc2, half_min_sq, ax, ay,
+                                                               az, ae, aw);
+    } else {
+      lj_pairs<kObs, kClamp, kTpa, kUnroll, kNoL1, true, kNt>(v, p, coeff, xi, i, sub, n,
+                                                              n_warp, rc2, half_min_sq, ax, ay,
+                                                              az, ae, aw);
     }
   }
   const float fx = ax.total(), fy = ay.total(), fz = az.total();
@@ -1150,21 +1225,38 @@ void launch_rebuild(const StepLaunch& l, bool force_all) {
   check_launch("build");
 }
 
-template <int kTpa, int kUnroll, bool kPrefetch>
-void launch_lj_tpa(const StepLaunch& l, bool observables, int mode) {
+// Steps that need observables (thermo rows, eval) use the general-table
+// kernel at depth 4 with the tuned threads per particle; every variant sums
+// forces in the same order, so the choice never shows in the results.
+template <int kTpa>
+void launch_lj_obs(const StepLaunch& l, int mode) {
   const dim3 grid(l.v.n_blocks * kTpa);
-#define BB_LJ(obs, m) k_lj<obs, m, kTpa, kUnroll, kPrefetch><<<grid, kBlock, 0, l.stream>>>(l.v)
-  if (observables) {
-    if (mode == kForcePlain) BB_LJ(true, kForcePlain);
-    else BB_LJ(true, kForcePost);  // the kinetic total is part of the observables
-  } else {
-    switch (mode) {
-      case kForcePlain: BB_LJ(false, kForcePlain); break;
-      case kForcePost: BB_LJ(false, kForcePost); break;
-      default: BB_LJ(false, kForcePostKinetic); break;
-    }
+  if (mode == kForcePlain) {
+    k_lj<true, kForcePlain, kTpa, 4, true, 0><<<grid, kBlock, 0, l.stream>>>(l.v);
+  } else {  // the kinetic total is part of the observables
+    k_lj<true, kForcePost, kTpa, 4, true, 0><<<grid, kBlock, 0, l.stream>>>(l.v);
+  }
+}
+
+template <int kTpa, int kUnroll, bool kNoL1, int kNt>
+void launch_lj_tpa(const StepLaunch& l, int mode) {
+  const dim3 grid(l.v.n_blocks * kTpa);
+#define BB_LJ(m) k_lj<false, m, kTpa, kUnroll, kNoL1, kNt><<<grid, kBlock, 0, l.stream>>>(l.v)
+  switch (mode) {
+    case kForcePlain: BB_LJ(kForcePlain); break;
+    case kForcePost: BB_LJ(kForcePost); break;
+    default: BB_LJ(kForcePostKinetic); break;
   }
 #undef BB_LJ
+}
+
+template <int kTpa, int kUnroll, bool kNoL1>
+void launch_lj_nt(const StepLaunch& l, int mode) {
+  switch (l.lj_types) {
+    case 1: launch_lj_tpa<kTpa, kUnroll, kNoL1, 1>(l, mode); break;
+    case 2: launch_lj_tpa<kTpa, kUnroll, kNoL1, 2>(l, mode); break;
+    default: launch_lj_tpa<kTpa, kUnroll, kNoL1, 0>(l, mode); break;
+  }
 }
 
 void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post) {
@@ -1172,14 +1264,21 @@ void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post)
   const int fin = !fuse ? kForcePlain : (l.need_kinetic ? kForcePostKinetic : kForcePost);
   const bool bonded = l.v.has_bonded != 0;
   if (clamp) {
-    k_lj<false, kForceClamp, 1, 8, false><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+    k_lj<false, kForceClamp, 1, 8, false, 0><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  } else if (observables) {
+    const int mode = bonded ? kForcePlain : fin;
+    switch (l.lj_tpa) {
+      case 2: launch_lj_obs<2>(l, mode); break;
+      case 4: launch_lj_obs<4>(l, mode); break;
+      default: launch_lj_obs<1>(l, mode); break;
+    }
   } else {
     const int mode = bonded ? kForcePlain : fin;
-    // (threads per particle, batch depth, prefetch) -> one instantiation
-    const int key = l.lj_tpa * 100 + l.lj_unroll * 10 + (l.lj_prefetch ? 1 : 0);
+    // (threads per particle, batch depth, list load policy) -> one instantiation
+    const int key = l.lj_tpa * 100 + l.lj_unroll * 10 + (l.lj_no_l1 ? 1 : 0);
     switch (key) {
 #define BB_CASE(t, u, pf) \
-  case t * 100 + u * 10 + pf: launch_lj_tpa<t, u, pf != 0>(l, observables, mode); break;
+  case t * 100 + u * 10 + pf: launch_lj_nt<t, u, pf != 0>(l, mode); break;
       BB_CASE(1, 8, 0) BB_CASE(1, 8, 1) BB_CASE(1, 4, 0) BB_CASE(1, 4, 1)
       BB_CASE(2, 8, 0) BB_CASE(2, 8, 1) BB_CASE(2, 4, 0) BB_CASE(2, 4, 1)
       BB_CASE(4, 8, 0) BB_CASE(4, 8, 1) BB_CASE(4, 4, 0) BB_CASE(4, 4, 1)

@@ -20,7 +20,8 @@ struct StepLaunch {
   int all_regular;        // every replica has >= 4 cells on every axis
   int lj_tpa;             // threads per particle of the pair-force kernel: 1, 2, 4
   int lj_unroll;          // list entries in flight per thread and batch: 4 or 8
-  int lj_prefetch;        // list entries of the next batch requested one batch early
+  int lj_no_l1;           // list entries loaded without allocating L1 lines
+  int lj_types;           // largest LJ table side over the batch (1, 2: specialised)
   int fuse_post;          // second half-kick inside the last force kernel
   int need_kinetic;       // a thermostat is active in some replica
   float sd_dmax;          // descent: displacement cap

@@ -270,20 +270,21 @@ class Engine:
         return out.value
 
     def set_tuning(self, threads_per_particle: int = 0, fuse_post: bool = False,
-                   batch_depth: int = 8, prefetch: bool = True) -> None:
+                   batch_depth: int = 8, list_bypass_l1: bool = False) -> None:
         """Fix the kernel schedule (threads per particle 1, 2 or 4; fused
-        second half-kick; list entries in flight 4 or 8; early list
-        requests), or hand it back to the autotuner with threads_per_particle
-        0."""
+        second half-kick; list entries in flight 4 or 8; list loads that
+        bypass L1), or hand it back to the autotuner with
+        threads_per_particle 0."""
         sched = (ctypes.c_int32 * 4)(int(threads_per_particle), 1 if fuse_post else 0,
-                                     int(batch_depth), 1 if prefetch else 0)
+                                     int(batch_depth), 1 if list_bypass_l1 else 0)
         _lib.check(self._lib.beads_set_tuning(self._h, sched))
 
     def tuning(self) -> dict:
         out = (ctypes.c_int32 * 5)()
         _lib.check(self._lib.beads_get_tuning(self._h, out))
         return {"threads_per_particle": out[0], "fuse_post": bool(out[1]),
-                "batch_depth": out[2], "prefetch": bool(out[3]), "autotuned": bool(out[4])}
+                "batch_depth": out[2], "list_bypass_l1": bool(out[3]),
+                "autotuned": bool(out[4])}
 
     # -- differentiation ------------------------------------------------------
     def set_lj(self, replica: int, epsilon, sigma) -> None:

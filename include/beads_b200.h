@@ -271,7 +271,7 @@ BEADS_API int beads_list_stats(beads_ctx* ctx, uint64_t* total_entries,
  *   schedule[1] second half-kick inside the last force kernel (1) or as its
  *               own kernel (0)
  *   schedule[2] batch depth: neighbour-list entries in flight per thread, 4/8
- *   schedule[3] list entries of the next batch requested early (1) or not (0)
+ *   schedule[3] neighbour-list loads bypass L1 (1) or stream through it (0)
  *   schedule[4] (get only) 1 if the autotuner chose the schedule
  * The choice never changes a result (forces are summed in one canonical
  * order).  By default the first beads_run() times the candidates on the

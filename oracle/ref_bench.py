@@ -80,9 +80,11 @@ def main(argv: list[str]) -> None:
         print("replicas", json.dumps(entry))
         out_path.write_text(json.dumps({"replica_batch": entry}, indent=1))
         return
-    cases = [("lattice_4096", workloads.lj_lattice(n_side=16), 5000)]
+    # Step counts of the workloads' own specifications: the 4096-bead lattice
+    # runs 1,000 steps, the 1M-bead mixture 10,000.
+    cases = [("lattice_4096", workloads.lj_lattice(n_side=16), 1000)]
     n_mix = 131072 if quick else 1_048_576
-    cases.append((f"mixture_{n_mix}", _relaxed_mixture(n_mix), 200 if quick else 2000))
+    cases.append((f"mixture_{n_mix}", _relaxed_mixture(n_mix), 200 if quick else 10000))
     results = {}
     for name, r, steps in cases:
         spec = spec_for(r, steps, "run", forces=False, thermo_every=steps)

@@ -33,7 +33,8 @@ def test_every_schedule_gives_identical_bits(name):
             rows = [eng.run(20, 20), eng.run(20, 20)]
             states = [eng.state(r) for r in range(len(eng.sizes))]
             assert eng.tuning() == {"threads_per_particle": tpa, "fuse_post": fuse,
-                                    "batch_depth": depth, "prefetch": pf, "autotuned": False}
+                                    "batch_depth": depth, "list_bypass_l1": pf,
+                                    "autotuned": False}
         outs.append((rows, states))
     rows0, states0 = outs[0]
     for (rows, states), sched in zip(outs[1:], SCHEDULES[1:]):
