@@ -67,6 +67,13 @@ Engine::Engine(uint32_t n, const beads_system_desc* systems,
     cudaStreamDestroy(stream_);
     throw;
   }
+  // BEADS_SCHEDULE="tpa,fuse_post,depth,list_bypass_l1" fixes the kernel
+  // schedule for every context of the process (reproducible profiling, no
+  // autotuning); results do not depend on it.
+  if (const char* e = std::getenv("BEADS_SCHEDULE")) {
+    int t = 0, f = 0, u = 0, b = 0;
+    if (std::sscanf(e, "%d,%d,%d,%d", &t, &f, &u, &b) == 4 && t != 0) set_tuning(t, f, u, b);
+  }
 }
 
 void Engine::set_sort_enabled(bool on) {
