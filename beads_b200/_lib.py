@@ -163,6 +163,8 @@ EXPORTED = (
     "beads_set_lj",
     "beads_adjoint_forward",
     "beads_adjoint_backward",
+    "beads_set_bonded",
+    "beads_adjoint_bonded_grads",
     "beads_cell_sort_static",
     "beads_debug_cells",
     "beads_debug_neighbors",
@@ -212,6 +214,8 @@ def load():
     L.beads_set_lj.argtypes = [vp, ctypes.c_uint32, vp, vp]
     L.beads_adjoint_forward.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, vp]
     L.beads_adjoint_backward.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.beads_set_bonded.argtypes = [vp, ctypes.c_uint32, vp, vp, vp, vp, vp]
+    L.beads_adjoint_bonded_grads.argtypes = [vp, vp, vp, vp]
     L.beads_cell_sort_static.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float),
                                          ctypes.POINTER(ctypes.c_float), ctypes.c_double,
                                          ctypes.c_double, vp, vp, vp, ctypes.c_uint32,

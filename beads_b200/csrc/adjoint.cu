@@ -32,6 +32,7 @@
 #include <cstdio>
 #include <cstring>
 
+#include "bonded_math.cuh"
 #include "device_util.cuh"
 #include "engine.hpp"
 #include "kernels.cuh"
@@ -71,6 +72,9 @@ struct AdjView {
   const int* list_src;   // per replica: -1 checkpoint build positions, else step index
   const int* shift_on;   // per replica: LJ energy shift active
   long long* dot;        // [2 lanes][R][whole, frac]: sum u_bar . v, double-buffered
+  long long* theta_bond;      // [global bond type][k, r0][whole, frac]
+  long long* theta_angle;     // [global angle type][k, theta0 (rad)][whole, frac]
+  long long* theta_dihedral;  // [global dihedral type][k][whole, frac]
   uint32_t slots;
   uint32_t replicas;
 };
@@ -184,7 +188,7 @@ __device__ __forceinline__ void add_typed(float (&acc)[kNt], int t, float v) {
 template <int kNt>
 __global__ void __launch_bounds__(kBlock)
 k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, uint32_t k,
-         int first, int lane_out) {
+         int first, int lane_out, int finish) {
   const uint32_t b = blockIdx.x;
   const uint32_t r = v.block_replica[b];
   const ReplicaParams& p = v.rp[r];
@@ -301,7 +305,7 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
     xb.y += gy;
     xb.z += gz;
     a.xbar[i] = xb;
-    if (!first) {
+    if (!first && finish) {
       const float4 vb = a.vbar[i];
       const float4 ub = make_float4(__fmaf_rn(p.dt, xb.x, vb.x), __fmaf_rn(p.dt, xb.y, vb.y),
                                     __fmaf_rn(p.dt, xb.z, vb.z), 0.f);
@@ -310,7 +314,7 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
       dot = (double)ub.x * vp.x + (double)ub.y * vp.y + (double)ub.z * vp.z;
     }
   }
-  if (!first) {
+  if (!first && finish) {
     long long* dout = a.dot + ((size_t)lane_out * v.n_replicas + r) * 2;
     block_add_fixed<kBlock>(real ? to_fixed(dot, &st->status) : Fixed{0, 0}, dout, dout + 1);
   }
@@ -330,6 +334,155 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
       reinterpret_cast<unsigned long long*>(a.theta) + (size_t)r * kAdjTypes * kAdjTypes * 4;
   for (int t = threadIdx.x; t < kAdjTypes * kAdjTypes * 4; t += kBlock) {
     if (theta_sh[t] != 0ull) atomicAdd(&out[t], theta_sh[t]);
+  }
+}
+
+constexpr int kAdjBondedTypes = 8;  // bonded types per kind and replica the adjoint supports
+constexpr int kDirs = 4;            // dual directions: F_bar, arms, parameter a, parameter b
+
+// Minimum-image arm x_a - x_b as a dual: direction 0 carries F_bar_a -
+// F_bar_b, direction 1 the arm itself (the tangent x_m - x_me of every
+// member, differenced), directions 2-3 nothing.
+__device__ __forceinline__ V3T<Dual<kDirs>> dual_arm(const DeviceView& v, const AdjView& a,
+                                                     const ReplicaParams& p,
+                                                     const float4* pos, uint32_t ta,
+                                                     uint32_t tb) {
+  const uint32_t sa = v.slot_of_tag[ta], sb = v.slot_of_tag[tb];
+  const float4 xa = pos[sa], xb = pos[sb];
+  const float4 fa = a.fbar[sa], fb = a.fbar[sb];
+  const float dx = acc_delta(xa.x, xb.x, p.len[0], p.half[0]);
+  const float dy = acc_delta(xa.y, xb.y, p.len[1], p.half[1]);
+  const float dz = acc_delta(xa.z, xb.z, p.len[2], p.half[2]);
+  V3T<Dual<kDirs>> d;
+  d.x = dconst<kDirs>(dx);
+  d.y = dconst<kDirs>(dy);
+  d.z = dconst<kDirs>(dz);
+  d.x.d[0] = fa.x - fb.x;
+  d.y.d[0] = fa.y - fb.y;
+  d.z.d[0] = fa.z - fb.z;
+  d.x.d[1] = dx;
+  d.y.d[1] = dy;
+  d.z.d[1] = dz;
+  return d;
+}
+
+// Step m, bonded part: x_bar += J F_bar + g_PE grad PE + g_W grad W over the
+// particle's harmonic terms (forward-mode duals of the term forces), the
+// k / r0 / theta0 adjoints, then (the last kernel of the step) u_bar_m and
+// the sum u_bar_m . v_m-1.
+__global__ void __launch_bounds__(kBlock)
+k_adj_bonded(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, uint32_t k,
+             int first, int lane_out) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const ReplicaParams& p = v.rp[r];
+  ReplicaState* st = &v.rs[r];
+  __shared__ unsigned long long sh[3][kAdjBondedTypes][2][2];
+  for (int t = threadIdx.x; t < 3 * kAdjBondedTypes * 4; t += kBlock) {
+    (&sh[0][0][0][0])[t] = 0ull;
+  }
+  __syncthreads();
+  const uint32_t i = b * kBlock + threadIdx.x;
+  const bool real = (i - p.atom_begin) < p.n_atoms;
+  const float g_pe = (float)a.obs_grad[((size_t)m * v.n_replicas + r) * 3 + 0];
+  const float g_w = (float)a.obs_grad[((size_t)m * v.n_replicas + r) * 3 + 1];
+  float gx = 0.f, gy = 0.f, gz = 0.f;
+  if (real) {
+    const float4 fi = a.fbar[i];
+    const uint32_t t = v.tag[i];
+    const uint32_t e0 = v.term_off[t], e1 = v.term_off[t + 1];
+    for (uint32_t e = e0; e < e1; ++e) {
+      const uint32_t mem = v.term[e];
+      const uint32_t kind = mem >> 30;
+      const uint32_t role = (mem >> 28) & 3u;
+      const uint32_t idx = mem & 0x0fffffffu;
+      Dual<kDirs> en, vir;
+      V3T<Dual<kDirs>> f;
+      int kind_slot = 0, local = 0;
+      if (kind == kTermBond) {
+        const uint4 q = v.bonds[idx];
+        const BondCoeff c = v.bond_coeff[q.z];
+        Dual<kDirs> kk = dconst<kDirs>(c.k), r0 = dconst<kDirs>(c.r0);
+        kk.d[2] = 1.0f;
+        r0.d[3] = 1.0f;
+        f = dual_bond<kDirs>(dual_arm(v, a, p, pos, q.x, q.y), kk, r0, role, en, vir);
+        kind_slot = 0;
+        local = (int)(q.z - p.bond_type_base);
+      } else if (kind == kTermAngle) {
+        const uint4 q = v.angles[idx];
+        const AngleCoeff c = v.angle_coeff[q.w];
+        Dual<kDirs> kk = dconst<kDirs>(c.k), th = dconst<kDirs>(c.theta0);
+        kk.d[2] = 1.0f;
+        th.d[3] = 1.0f;
+        f = dual_angle<kDirs>(dual_arm(v, a, p, pos, q.x, q.y), dual_arm(v, a, p, pos, q.z, q.y),
+                              kk, th, role, en, vir);
+        kind_slot = 1;
+        local = (int)(q.w - p.angle_type_base);
+      } else {
+        const uint4 q = v.dihedrals[idx];
+        const uint32_t ty = v.dihedral_type[idx];
+        const DihedralCoeff c = v.dihedral_coeff[ty];
+        Dual<kDirs> kk = dconst<kDirs>(c.k);
+        kk.d[2] = 1.0f;
+        f = dual_dihedral<kDirs>(dual_arm(v, a, p, pos, q.x, q.y),
+                                 dual_arm(v, a, p, pos, q.z, q.y),
+                                 dual_arm(v, a, p, pos, q.z, q.w), kk, c.d, c.n, role, en, vir);
+        kind_slot = 2;
+        local = (int)(ty - p.dihedral_type_base);
+      }
+      // J F_bar (direction 0) + g_PE grad PE (= -F) + g_W grad W (= F + direction 1)
+      gx += f.x.d[0] - g_pe * f.x.v + g_w * (f.x.v + f.x.d[1]);
+      gy += f.y.d[0] - g_pe * f.y.v + g_w * (f.y.v + f.y.d[1]);
+      gz += f.z.d[0] - g_pe * f.z.v + g_w * (f.z.v + f.z.d[1]);
+      for (int q2 = 0; q2 < 2; ++q2) {
+        const int dir = 2 + q2;
+        float g = fi.x * f.x.d[dir] + fi.y * f.y.d[dir] + fi.z * f.z.d[dir];
+        if (role == 0u) g += g_pe * en.d[dir] + g_w * vir.d[dir];
+        if (g != 0.0f && local >= 0 && local < kAdjBondedTypes) {
+          const Fixed fx = to_fixed((double)g, &st->status);
+          atomicAdd(&sh[kind_slot][local][q2][0], (unsigned long long)fx.whole);
+          atomicAdd(&sh[kind_slot][local][q2][1], (unsigned long long)fx.frac);
+        }
+      }
+    }
+  }
+  double dot = 0.0;
+  if (real) {
+    float4 xb = a.xbar[i];
+    xb.x += gx;
+    xb.y += gy;
+    xb.z += gz;
+    a.xbar[i] = xb;
+    if (!first) {
+      const float4 vb = a.vbar[i];
+      const float4 ub = make_float4(__fmaf_rn(p.dt, xb.x, vb.x), __fmaf_rn(p.dt, xb.y, vb.y),
+                                    __fmaf_rn(p.dt, xb.z, vb.z), 0.f);
+      a.ubar[i] = ub;
+      const float4 vp = a.seg_vel[(size_t)(k - 1) * a.slots + i];
+      dot = (double)ub.x * vp.x + (double)ub.y * vp.y + (double)ub.z * vp.z;
+    }
+  }
+  if (!first) {
+    long long* dout = a.dot + ((size_t)lane_out * v.n_replicas + r) * 2;
+    block_add_fixed<kBlock>(real ? to_fixed(dot, &st->status) : Fixed{0, 0}, dout, dout + 1);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 3 * kAdjBondedTypes * 4; t += kBlock) {
+    const unsigned long long val = (&sh[0][0][0][0])[t];
+    if (val == 0ull) continue;
+    const int kind_slot = t / (kAdjBondedTypes * 4);
+    const int rest = t % (kAdjBondedTypes * 4);
+    const int local = rest / 4, q2 = (rest / 2) % 2, word = rest % 2;
+    long long* dst;
+    if (kind_slot == 0) {
+      dst = a.theta_bond + ((size_t)(p.bond_type_base + local) * 2 + q2) * 2 + word;
+    } else if (kind_slot == 1) {
+      dst = a.theta_angle + ((size_t)(p.angle_type_base + local) * 2 + q2) * 2 + word;
+    } else {
+      if (q2 != 0) continue;  // dihedrals have one parameter
+      dst = a.theta_dihedral + (size_t)(p.dihedral_type_base + local) * 2 + word;
+    }
+    atomicAdd(reinterpret_cast<unsigned long long*>(dst), val);
   }
 }
 
@@ -434,7 +587,11 @@ void Engine::adjoint_forward(uint64_t steps, uint64_t record_from, uint32_t ever
   if (steps == 0) throw InvalidArgument("adjoint runs need at least one step.");
   if (record_from > steps) throw InvalidArgument("record_from must not exceed steps.");
   if (every == 0) throw InvalidArgument("checkpoint interval must be positive.");
-  if (v_.has_bonded) throw InvalidArgument("the adjoint supports pair-only systems.");
+  for (const auto& h : rep_) {
+    if (h.n_bond_types > 8 || h.n_angle_types > 8 || h.n_dihedral_types > 8) {
+      throw InvalidArgument("the adjoint supports up to 8 bonded types of each kind per replica.");
+    }
+  }
   int max_types = 0;
   for (const auto& h : rep_) max_types = std::max(max_types, h.n_types);
   if (max_types > kAdjTypes) throw InvalidArgument("the adjoint supports up to 4 particle types.");
@@ -541,6 +698,9 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
     A.tag_xfer = A.alloc<float>(3 * n_tags_);
     A.shift_on = A.alloc<int>(R);
     A.dot = A.alloc<long long>(static_cast<size_t>(R) * 4);
+    A.theta_bond = A.alloc<long long>(std::max<size_t>(1, total_bond_types_) * 4);
+    A.theta_angle = A.alloc<long long>(std::max<size_t>(1, total_angle_types_) * 4);
+    A.theta_dihedral = A.alloc<long long>(std::max<size_t>(1, total_dihedral_types_) * 2);
   }
   if (A.obs_capacity < (T + 1) * R * 3) {
     A.obs_capacity = (T + 1) * R * 3;
@@ -565,6 +725,11 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
   cuda_check(cudaMemset(A.theta, 0, static_cast<size_t>(R) * kAdjTypes * kAdjTypes * 4 * 8),
              "memset");
   cuda_check(cudaMemset(A.dot, 0, static_cast<size_t>(R) * 4 * sizeof(long long)), "memset");
+  cuda_check(cudaMemset(A.theta_bond, 0, std::max<size_t>(1, total_bond_types_) * 4 * 8), "memset");
+  cuda_check(cudaMemset(A.theta_angle, 0, std::max<size_t>(1, total_angle_types_) * 4 * 8),
+             "memset");
+  cuda_check(cudaMemset(A.theta_dihedral, 0, std::max<size_t>(1, total_dihedral_types_) * 2 * 8),
+             "memset");
 
   AdjView av{};
   av.seg_pos = A.seg_pos;
@@ -581,6 +746,9 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
   av.list_src = nullptr;
   av.shift_on = d_shift;
   av.dot = A.dot;
+  av.theta_bond = A.theta_bond;
+  av.theta_angle = A.theta_angle;
+  av.theta_dihedral = A.theta_dihedral;
   av.slots = A.slots;
   av.replicas = R;
 
@@ -652,16 +820,22 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
                                                         first, last, lane_in);
       launch_check("adjoint prepare");
       const float4* pos_m = A.seg_pos + static_cast<size_t>(k) * S;
+      const int bonded = v_.has_bonded ? 1 : 0;
       if (A.max_types <= 2) {
         k_adj_lj<2><<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, pos_m,
                                                         static_cast<uint32_t>(m), k, first,
-                                                        lane_out);
+                                                        lane_out, !bonded);
       } else {
         k_adj_lj<4><<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, pos_m,
                                                         static_cast<uint32_t>(m), k, first,
-                                                        lane_out);
+                                                        lane_out, !bonded);
       }
       launch_check("adjoint pair");
+      if (bonded) {
+        k_adj_bonded<<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, pos_m, static_cast<uint32_t>(m),
+                                                         k, first, lane_out);
+        launch_check("adjoint bonded");
+      }
     }
     sync();
   }
@@ -699,6 +873,75 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
   adjoint_restore(A.segments);
   set_sort_enabled(true);
   check_status();
+}
+
+void Engine::adjoint_bonded_grads(double* grad_bond, double* grad_angle, double* grad_dihedral) {
+  if (!adj_ || !adj_->theta_bond) throw InvalidArgument("no adjoint_backward has run.");
+  AdjointStore& A = *adj_;
+  sync();
+  auto read = [&](const long long* src, size_t n_pairs, std::vector<double>& out) {
+    std::vector<long long> raw(2 * std::max<size_t>(1, n_pairs));
+    cuda_check(cudaMemcpy(raw.data(), src, raw.size() * sizeof(long long), cudaMemcpyDeviceToHost),
+               "adjoint download");
+    out.resize(n_pairs);
+    for (size_t q = 0; q < n_pairs; ++q) {
+      out[q] = static_cast<double>(raw[2 * q]) + static_cast<double>(raw[2 * q + 1]) / kFixFrac;
+    }
+  };
+  std::vector<double> b, an, d;
+  read(A.theta_bond, 2ull * total_bond_types_, b);
+  read(A.theta_angle, 2ull * total_angle_types_, an);
+  read(A.theta_dihedral, total_dihedral_types_, d);
+  constexpr double kPerDegree = 3.14159265358979323846 / 180.0;
+  if (grad_bond) std::copy(b.begin(), b.end(), grad_bond);
+  if (grad_angle) {
+    for (size_t t = 0; t < total_angle_types_; ++t) {
+      grad_angle[2 * t] = an[2 * t];
+      grad_angle[2 * t + 1] = an[2 * t + 1] * kPerDegree;
+    }
+  }
+  if (grad_dihedral) std::copy(d.begin(), d.end(), grad_dihedral);
+}
+
+void Engine::set_bonded(uint32_t replica, const double* bond_k, const double* bond_r0,
+                        const double* angle_k, const double* angle_theta0_deg,
+                        const double* dihedral_k) {
+  const ReplicaHost& h = rep_.at(replica);
+  sync();
+  if (h.n_bond_types > 0 && (bond_k || bond_r0)) {
+    std::vector<BondCoeff> c(h.n_bond_types);
+    cuda_check(cudaMemcpy(c.data(), v_.bond_coeff + h.bond_type_base,
+                          c.size() * sizeof(BondCoeff), cudaMemcpyDeviceToHost), "bonded");
+    for (int t = 0; t < h.n_bond_types; ++t) {
+      if (bond_k) c[t].k = static_cast<float>(bond_k[t]);
+      if (bond_r0) c[t].r0 = static_cast<float>(bond_r0[t]);
+    }
+    cuda_check(cudaMemcpy(const_cast<BondCoeff*>(v_.bond_coeff) + h.bond_type_base, c.data(),
+                          c.size() * sizeof(BondCoeff), cudaMemcpyHostToDevice), "bonded");
+  }
+  if (h.n_angle_types > 0 && (angle_k || angle_theta0_deg)) {
+    std::vector<AngleCoeff> c(h.n_angle_types);
+    cuda_check(cudaMemcpy(c.data(), v_.angle_coeff + h.angle_type_base,
+                          c.size() * sizeof(AngleCoeff), cudaMemcpyDeviceToHost), "bonded");
+    for (int t = 0; t < h.n_angle_types; ++t) {
+      if (angle_k) c[t].k = static_cast<float>(angle_k[t]);
+      if (angle_theta0_deg) {
+        c[t].theta0 = static_cast<float>(angle_theta0_deg[t]) * 3.14159265358979323846f / 180.0f;
+      }
+    }
+    cuda_check(cudaMemcpy(const_cast<AngleCoeff*>(v_.angle_coeff) + h.angle_type_base, c.data(),
+                          c.size() * sizeof(AngleCoeff), cudaMemcpyHostToDevice), "bonded");
+  }
+  if (h.n_dihedral_types > 0 && dihedral_k) {
+    std::vector<DihedralCoeff> c(h.n_dihedral_types);
+    cuda_check(cudaMemcpy(c.data(), v_.dihedral_coeff + h.dihedral_type_base,
+                          c.size() * sizeof(DihedralCoeff), cudaMemcpyDeviceToHost), "bonded");
+    for (int t = 0; t < h.n_dihedral_types; ++t) c[t].k = static_cast<float>(dihedral_k[t]);
+    cuda_check(cudaMemcpy(const_cast<DihedralCoeff*>(v_.dihedral_coeff) + h.dihedral_type_base,
+                          c.data(), c.size() * sizeof(DihedralCoeff), cudaMemcpyHostToDevice),
+               "bonded");
+  }
+  initialized_ = false;
 }
 
 }  // namespace bb

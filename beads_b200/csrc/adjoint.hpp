@@ -57,6 +57,9 @@ struct AdjointStore {
   float* tag_xfer = nullptr;     // [3 * particles] tag-order staging
   int* shift_on = nullptr;       // [R] LJ energy shift active
   long long* dot = nullptr;          // [2][R][2] sum u_bar . v (fixed point)
+  long long* theta_bond = nullptr;   // [bond types][k, r0][2]
+  long long* theta_angle = nullptr;  // [angle types][k, theta0][2]
+  long long* theta_dihedral = nullptr;  // [dihedral types][2]
 
   std::vector<void*> allocations;
   ~AdjointStore();

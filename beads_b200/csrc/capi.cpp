@@ -420,6 +420,24 @@ int beads_adjoint_backward(beads_ctx* ctx, const double* observables_grad, doubl
   });
 }
 
+int beads_set_bonded(beads_ctx* ctx, uint32_t replica, const double* bond_k,
+                     const double* bond_r0, const double* angle_k,
+                     const double* angle_theta0_deg, const double* dihedral_k) {
+  return guarded([&] {
+    require(ctx && ctx->engine, "NULL context.");
+    require(replica < ctx->engine->n_replicas(), "replica index out of range.");
+    ctx->engine->set_bonded(replica, bond_k, bond_r0, angle_k, angle_theta0_deg, dihedral_k);
+  });
+}
+
+int beads_adjoint_bonded_grads(beads_ctx* ctx, double* grad_bond, double* grad_angle,
+                               double* grad_dihedral) {
+  return guarded([&] {
+    require(ctx && ctx->engine, "NULL context.");
+    ctx->engine->adjoint_bonded_grads(grad_bond, grad_angle, grad_dihedral);
+  });
+}
+
 int beads_counters(beads_ctx* ctx, uint32_t replica, uint64_t* counters) {
   return guarded([&] {
     require(ctx && ctx->engine && counters, "NULL argument.");

@@ -303,6 +303,12 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
     p.bond_type_base = bond_types;
     p.angle_type_base = angle_types;
     p.dihedral_type_base = dihedral_types;
+    rep_[r].bond_type_base = bond_types;
+    rep_[r].angle_type_base = angle_types;
+    rep_[r].dihedral_type_base = dihedral_types;
+    rep_[r].n_bond_types = f.n_bond_types;
+    rep_[r].n_angle_types = f.n_angle_types;
+    rep_[r].n_dihedral_types = f.n_dihedral_types;
     bond_types += f.n_bond_types;
     angle_types += f.n_angle_types;
     dihedral_types += f.n_dihedral_types;
@@ -311,6 +317,9 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
     dihedrals += s.n_dihedrals;
   }
   n_tags_ = tags;
+  total_bond_types_ = static_cast<uint32_t>(bond_types);
+  total_angle_types_ = static_cast<uint32_t>(angle_types);
+  total_dihedral_types_ = static_cast<uint32_t>(dihedral_types);
   const uint32_t S = static_cast<uint32_t>(slots);
   const uint32_t T = static_cast<uint32_t>(tags);
   const uint32_t C = static_cast<uint32_t>(cells);

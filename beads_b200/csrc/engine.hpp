@@ -47,6 +47,8 @@ struct ReplicaHost {
   double lj_cutoff = 0;
   int lj_shift = 0;
   uint32_t sort_every = 0;       // reorder cadence in builds (0 = never)
+  int n_bond_types = 0, n_angle_types = 0, n_dihedral_types = 0;
+  uint32_t bond_type_base = 0, angle_type_base = 0, dihedral_type_base = 0;
 };
 
 struct AdjointStore;  // adjoint.cu
@@ -111,6 +113,11 @@ class Engine {
   // ---- adjoint (reverse-mode gradients of a trajectory; adjoint.cu) ----
   // Replaces the LJ eps/sigma tables of one replica (full n_types^2 tables).
   void set_lj(uint32_t replica, const double* eps, const double* sigma);
+  // Replaces one replica's harmonic bonded parameters (NULL: unchanged);
+  // angle theta0 in degrees as in beads_forcefield_desc.
+  void set_bonded(uint32_t replica, const double* bond_k, const double* bond_r0,
+                  const double* angle_k, const double* angle_theta0_deg,
+                  const double* dihedral_k);
   // Runs `steps` velocity-Verlet steps from the current state (forces and
   // the list are rebuilt first, as a fresh run), keeping a checkpoint every
   // `checkpoint_every` steps.  obs receives [step - record_from][replica]
@@ -123,6 +130,13 @@ class Engine {
   // the end-of-forward state again afterwards.
   void adjoint_backward(const double* obs_grad, double* grad_eps, double* grad_sigma,
                         float* grad_pos, float* grad_vel);
+  // Bonded parameter gradients of the last adjoint_backward, by global type
+  // (replicas' types in batch order): bonds [k, r0], angles [k, theta0 per
+  // degree], dihedrals [k].
+  void adjoint_bonded_grads(double* grad_bond, double* grad_angle, double* grad_dihedral);
+  uint32_t n_bond_types_total() const { return total_bond_types_; }
+  uint32_t n_angle_types_total() const { return total_angle_types_; }
+  uint32_t n_dihedral_types_total() const { return total_dihedral_types_; }
 
  private:
   // Switches the periodic slot reorder off (false) or back to each replica's
@@ -156,6 +170,7 @@ class Engine {
   bool initialized_ = false;
   bool use_graphs_ = true;
   bool use_conditional_ = true;
+  uint32_t total_bond_types_ = 0, total_angle_types_ = 0, total_dihedral_types_ = 0;
   bool tuning_fixed_ = false;          // set_tuning() with an explicit choice
   bool tuned_ = false;                 // autotune() has run
   cudaStream_t side_stream_ = nullptr;

@@ -297,6 +297,39 @@ class Engine:
         _lib.check(self._lib.beads_set_lj(self._h, int(replica), eps.ctypes.data,
                                           sig.ctypes.data))
 
+    def set_bonded(self, replica: int, bond_k=None, bond_r0=None, angle_k=None,
+                   angle_theta0=None, dihedral_k=None) -> None:
+        """Replace one replica's harmonic bonded parameters (per local type;
+        None leaves a parameter unchanged; theta0 in degrees)."""
+        keep = []
+
+        def ptr(x):
+            if x is None:
+                return None
+            a = np.ascontiguousarray(x, dtype=np.float64).ravel()
+            keep.append(a)
+            return a.ctypes.data
+
+        _lib.check(self._lib.beads_set_bonded(self._h, int(replica), ptr(bond_k), ptr(bond_r0),
+                                              ptr(angle_k), ptr(angle_theta0), ptr(dihedral_k)))
+
+    def adjoint_bonded_grads(self) -> dict:
+        """Bonded parameter gradients of the last adjoint_backward, one row
+        per replica type in batch order: bond (d/dk, d/dr0), angle (d/dk,
+        d/dtheta0 per degree), dihedral (d/dk)."""
+        def count(x):
+            return 0 if x is None else len(x)
+
+        nb = sum(count(s.bond_k) for s in self.replicas)
+        na = sum(count(s.angle_k) for s in self.replicas)
+        nd = sum(count(s.dihedral_k) for s in self.replicas)
+        gb = np.zeros((nb, 2), np.float64)
+        ga = np.zeros((na, 2), np.float64)
+        gd = np.zeros(nd, np.float64)
+        _lib.check(self._lib.beads_adjoint_bonded_grads(self._h, gb.ctypes.data, ga.ctypes.data,
+                                                        gd.ctypes.data))
+        return {"bond": gb, "angle": ga, "dihedral": gd}
+
     def adjoint_forward(self, steps: int, record_from: int, checkpoint_every: int) -> np.ndarray:
         """Run `steps` steps keeping checkpoints; returns [PE, virial, KE] of
         steps record_from..steps, shape (steps - record_from + 1, R, 3)."""

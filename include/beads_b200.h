@@ -293,8 +293,8 @@ BEADS_API int beads_set_lj(beads_ctx* ctx, uint32_t replica, const double* epsil
  * `checkpoint_every` steps, and writes the observables of steps
  * record_from..steps: observables[((step - record_from) * n_replicas + r) * 3
  * + {0, 1, 2}] = potential energy, virial (sum r.F), kinetic energy (as a
- * thermo row reports them).  Pair-only systems with up to 4 particle types.
- * Slots are not reordered during the run. */
+ * thermo row reports them).  Up to 4 particle types and 8 bonded types of
+ * each kind per replica.  Slots are not reordered during the run. */
 BEADS_API int beads_adjoint_forward(beads_ctx* ctx, uint64_t steps, uint64_t record_from,
                                     uint32_t checkpoint_every, double* observables);
 /* Reverse pass of the last beads_adjoint_forward(): given dL/d(observables)
@@ -308,6 +308,18 @@ BEADS_API int beads_adjoint_forward(beads_ctx* ctx, uint64_t steps, uint64_t rec
 BEADS_API int beads_adjoint_backward(beads_ctx* ctx, const double* observables_grad,
                                      double* grad_epsilon, double* grad_sigma,
                                      float* grad_positions, float* grad_velocities);
+
+/* Replaces one replica's harmonic bonded parameters, per local type (NULL
+ * arrays leave that parameter unchanged; theta0 in degrees). */
+BEADS_API int beads_set_bonded(beads_ctx* ctx, uint32_t replica, const double* bond_k,
+                               const double* bond_r0, const double* angle_k,
+                               const double* angle_theta0_deg, const double* dihedral_k);
+/* Bonded parameter gradients of the last beads_adjoint_backward(), by global
+ * type (every replica's types in batch order): grad_bond [types][2] = d/dk,
+ * d/dr0; grad_angle [types][2] = d/dk, d/dtheta0 (per degree); grad_dihedral
+ * [types] = d/dk.  NULL pointers are skipped. */
+BEADS_API int beads_adjoint_bonded_grads(beads_ctx* ctx, double* grad_bond, double* grad_angle,
+                                         double* grad_dihedral);
 
 /* Device counters of one replica, without stepping it: counters[0] completed
  * MD steps, [1] neighbour builds, [2] dangerous rebuilds (the quantities the
