@@ -103,6 +103,8 @@ def trajectory_observables(engine: Engine, epsilon: torch.Tensor, sigma: torch.T
     parameters (optional, one value per bonded type, shared by all replicas;
     angle theta0 in degrees) replace the engine's and become differentiable.
     At most 4 particle types and 8 bonded types of each kind per replica.
+    checkpoint_every = 0 keeps every step's state on the device (32 bytes per
+    particle and step) instead of replaying segments in the backward pass.
     """
     return _TrajectoryFunction.apply(epsilon, sigma, positions, velocities, bond_k, bond_r0,
                                      angle_k, angle_theta0, dihedral_k, engine, int(steps),

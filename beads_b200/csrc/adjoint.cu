@@ -185,11 +185,12 @@ __device__ __forceinline__ void add_typed(float (&acc)[kNt], int t, float v) {
 // `lane_out` of a.dot).  `pos` holds x_m.  Batches of four list entries with
 // the next batch's entries requested early, as in the force kernel; kNt is
 // the LJ table side rounded up (2 or 4).
-template <int kNt>
+template <int kNt, int kTpa>
 __global__ void __launch_bounds__(kBlock)
 k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, uint32_t k,
          int first, int lane_out, int finish) {
-  const uint32_t b = blockIdx.x;
+  constexpr uint32_t kAtoms = kBlock / kTpa;
+  const uint32_t b = blockIdx.x / kTpa;  // 128-slot block of the particles
   const uint32_t r = v.block_replica[b];
   const ReplicaParams& p = v.rp[r];
   ReplicaState* st = &v.rs[r];
@@ -220,7 +221,10 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
   for (int t = threadIdx.x; t < kAdjTypes * kAdjTypes * 4; t += kBlock) theta_sh[t] = 0ull;
   __syncthreads();
 
-  const uint32_t i = b * kBlock + threadIdx.x;
+  // kTpa threads share a particle: thread `sub` takes list entries sub,
+  // sub + kTpa, ...; their sums are combined by shuffles in a fixed order.
+  const uint32_t sub = threadIdx.x % kTpa;
+  const uint32_t i = b * kBlock + (blockIdx.x % kTpa) * kAtoms + threadIdx.x / kTpa;
   const bool real = (i - p.atom_begin) < p.n_atoms;
   const float g_pe = (float)a.obs_grad[((size_t)m * v.n_replicas + r) * 3 + 0];
   const float g_w = (float)a.obs_grad[((size_t)m * v.n_replicas + r) * 3 + 1];
@@ -233,7 +237,7 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
   const int ti = __float_as_int(xi.w);
   const AdjCoeff* row = table + ti * kNt;
   const float4 fi = a.fbar[i];
-  const uint32_t n = real ? v.nbr_count[i] : 0u;
+  const uint32_t n = real ? v.nbr_count[i] : 0u;  // every thread of the particle
   const uint32_t n_warp = __reduce_max_sync(kFull, n);
   const float hmin = fminf(p.half[0], fminf(p.half[1], p.half[2]));
   const float half_min_sq = hmin * hmin;
@@ -241,8 +245,11 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
   constexpr uint32_t kU = 4;
   uint32_t jn[kU];
 #pragma unroll
-  for (uint32_t u = 0; u < kU; ++u) jn[u] = u < n ? __ldcs(list + (size_t)u * kGroup) : i;
-  for (uint32_t k0 = 0; k0 < n_warp; k0 += kU) {
+  for (uint32_t u = 0; u < kU; ++u) {
+    const uint32_t q = u * kTpa + sub;
+    jn[u] = q < n ? __ldcs(list + (size_t)q * kGroup) : i;
+  }
+  for (uint32_t k0 = 0; k0 < n_warp; k0 += kU * kTpa) {
     uint32_t j[kU];
     float4 xj[kU], fj[kU];
 #pragma unroll
@@ -254,7 +261,8 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
     }
 #pragma unroll
     for (uint32_t u = 0; u < kU; ++u) {
-      jn[u] = k0 + kU + u < n ? __ldcs(list + (size_t)(k0 + kU + u) * kGroup) : i;
+      const uint32_t q = k0 + (kU + u) * kTpa + sub;
+      jn[u] = q < n ? __ldcs(list + (size_t)q * kGroup) : i;
     }
 #pragma unroll
     for (uint32_t u = 0; u < kU; ++u) {
@@ -269,7 +277,7 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
           r2 = norm2(dx, dy, dz);
         }
       }
-      const bool in = (k0 + u < n) && r2 < rc2;
+      const bool in = (k0 + u * kTpa + sub < n) && r2 < rc2;
       const int tj = __float_as_int(xj[u].w);
       const AdjCoeff c = row[tj];
       const float rr = in ? r2 : 1.0f;
@@ -298,8 +306,17 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
       add_typed<kNt>(ts, tj, in ? d_sig : 0.0f);
     }
   }
+  if (kTpa > 1) {
+#pragma unroll
+    for (int o = 1; o < kTpa; o <<= 1) {
+      gx += __shfl_xor_sync(kFull, gx, o);
+      gy += __shfl_xor_sync(kFull, gy, o);
+      gz += __shfl_xor_sync(kFull, gz, o);
+    }
+  }
+  const bool owner = real && sub == 0u;
   double dot = 0.0;
-  if (real) {
+  if (owner) {
     float4 xb = a.xbar[i];
     xb.x += gx;
     xb.y += gy;
@@ -316,7 +333,7 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
   }
   if (!first && finish) {
     long long* dout = a.dot + ((size_t)lane_out * v.n_replicas + r) * 2;
-    block_add_fixed<kBlock>(real ? to_fixed(dot, &st->status) : Fixed{0, 0}, dout, dout + 1);
+    block_add_fixed<kBlock>(owner ? to_fixed(dot, &st->status) : Fixed{0, 0}, dout, dout + 1);
   }
   if (real) {
     for (int c = 0; c < nt; ++c) {
@@ -541,6 +558,21 @@ void Engine::set_lj(uint32_t replica, const double* eps, const double* sigma) {
   initialized_ = false;  // forces of the current state are stale
 }
 
+void Engine::adjoint_segment_storage(uint32_t K) {
+  AdjointStore& A = *adj_;
+  const uint32_t R = A.replicas;
+  const size_t S = A.slots;
+  if (A.seg_capacity >= K + 1) return;
+  A.seg_capacity = K + 1;
+  A.seg_pos = A.alloc<float4>(static_cast<size_t>(K + 1) * S);
+  A.seg_vel = A.alloc<float4>(static_cast<size_t>(K + 1) * S);
+  A.seg_lam = A.alloc<double>(static_cast<size_t>(K + 1) * R);
+  A.seg_kin = A.alloc<double>(static_cast<size_t>(K + 1) * R);
+  A.seg_flags = A.alloc<uint32_t>(static_cast<size_t>(K + 1) * R);
+  A.seg_src = A.alloc<int>(static_cast<size_t>(K + 1) * R);
+  A.seg_changed = A.alloc<uint32_t>(static_cast<size_t>(K + 1) * R);
+}
+
 void Engine::adjoint_record(uint32_t k) {
   AdjointStore& A = *adj_;
   const size_t S = A.slots;
@@ -586,7 +618,6 @@ void Engine::adjoint_restore(uint32_t c) {
 void Engine::adjoint_forward(uint64_t steps, uint64_t record_from, uint32_t every, double* obs) {
   if (steps == 0) throw InvalidArgument("adjoint runs need at least one step.");
   if (record_from > steps) throw InvalidArgument("record_from must not exceed steps.");
-  if (every == 0) throw InvalidArgument("checkpoint interval must be positive.");
   for (const auto& h : rep_) {
     if (h.n_bond_types > 8 || h.n_angle_types > 8 || h.n_dihedral_types > 8) {
       throw InvalidArgument("the adjoint supports up to 8 bonded types of each kind per replica.");
@@ -600,6 +631,14 @@ void Engine::adjoint_forward(uint64_t steps, uint64_t record_from, uint32_t ever
   AdjointStore& A = *adj_;
   const uint32_t R = n_replicas();
   const size_t S = v_.n_slots;
+  // every == 0: keep every step's state from this forward pass (one segment,
+  // no replay in the backward pass) -- the trade of memory for compute that
+  // 180 GB of HBM usually affords: 32 bytes per slot and step.
+  A.store_all = every == 0;
+  if (A.store_all) {
+    if (steps > 0xFFFFFFF0ull) throw InvalidArgument("too many steps to store.");
+    every = static_cast<uint32_t>(steps);
+  }
   A.steps = steps;
   A.record_from = record_from;
   A.every = every;
@@ -652,10 +691,19 @@ void Engine::adjoint_forward(uint64_t steps, uint64_t record_from, uint32_t ever
   if (!tuned_ && !tuning_fixed_) autotune();
   save(0);
   if (record_from == 0) put_obs(0);
+  if (A.store_all) {
+    adjoint_segment_storage(every);
+    adjoint_record(0);
+  }
   uint64_t n = 0;
   while (n < steps) {
     const uint64_t next_ck = (n / every + 1) * every;
-    if (n + 1 >= record_from) {
+    if (A.store_all) {
+      run(1, n + 1 >= record_from ? 1 : 0);
+      n += 1;
+      adjoint_record(static_cast<uint32_t>(n));
+      if (n >= record_from) put_obs(n);
+    } else if (n + 1 >= record_from) {
       run(1, 1);
       n += 1;
       put_obs(n);
@@ -679,16 +727,7 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
   const uint64_t T = A.steps;
   const uint32_t K = A.every;
 
-  if (A.seg_capacity < K + 1) {
-    A.seg_capacity = K + 1;
-    A.seg_pos = A.alloc<float4>(static_cast<size_t>(K + 1) * S);
-    A.seg_vel = A.alloc<float4>(static_cast<size_t>(K + 1) * S);
-    A.seg_lam = A.alloc<double>(static_cast<size_t>(K + 1) * R);
-    A.seg_kin = A.alloc<double>(static_cast<size_t>(K + 1) * R);
-    A.seg_flags = A.alloc<uint32_t>(static_cast<size_t>(K + 1) * R);
-    A.seg_src = A.alloc<int>(static_cast<size_t>(K + 1) * R);
-    A.seg_changed = A.alloc<uint32_t>(static_cast<size_t>(K + 1) * R);
-  }
+  adjoint_segment_storage(K);
   if (!A.xbar) {
     A.xbar = A.alloc<float4>(S);
     A.vbar = A.alloc<float4>(S);
@@ -759,12 +798,15 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
   for (int s = static_cast<int>(A.segments) - 1; s >= 0; --s) {
     const uint64_t a = static_cast<uint64_t>(s) * K;
     const uint64_t b = std::min<uint64_t>(a + K, T);
-    // Replay the segment, recording every step.
-    adjoint_restore(static_cast<uint32_t>(s));
-    adjoint_record(0);
-    for (uint64_t k = 1; k <= b - a; ++k) {
-      launch_chunk(1, false);
-      adjoint_record(static_cast<uint32_t>(k));
+    // Replay the segment, recording every step (kept from the forward pass
+    // when it stored every step).
+    if (!A.store_all) {
+      adjoint_restore(static_cast<uint32_t>(s));
+      adjoint_record(0);
+      for (uint64_t k = 1; k <= b - a; ++k) {
+        launch_chunk(1, false);
+        adjoint_record(static_cast<uint32_t>(k));
+      }
     }
     sync();
     flags.resize(static_cast<size_t>(b - a + 1) * R);
@@ -821,14 +863,22 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
       launch_check("adjoint prepare");
       const float4* pos_m = A.seg_pos + static_cast<size_t>(k) * S;
       const int bonded = v_.has_bonded ? 1 : 0;
+      // Two threads per particle unless the step kernels run one.
+      const bool two = launch_.lj_tpa != 1;
+      const dim3 grid(v_.n_blocks * (two ? 2 : 1));
+      const uint32_t mm = static_cast<uint32_t>(m);
       if (A.max_types <= 2) {
-        k_adj_lj<2><<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, pos_m,
-                                                        static_cast<uint32_t>(m), k, first,
-                                                        lane_out, !bonded);
+        if (two) {
+          k_adj_lj<2, 2><<<grid, kBlock, 0, stream_>>>(v_, av, pos_m, mm, k, first, lane_out, !bonded);
+        } else {
+          k_adj_lj<2, 1><<<grid, kBlock, 0, stream_>>>(v_, av, pos_m, mm, k, first, lane_out, !bonded);
+        }
       } else {
-        k_adj_lj<4><<<v_.n_blocks, kBlock, 0, stream_>>>(v_, av, pos_m,
-                                                        static_cast<uint32_t>(m), k, first,
-                                                        lane_out, !bonded);
+        if (two) {
+          k_adj_lj<4, 2><<<grid, kBlock, 0, stream_>>>(v_, av, pos_m, mm, k, first, lane_out, !bonded);
+        } else {
+          k_adj_lj<4, 1><<<grid, kBlock, 0, stream_>>>(v_, av, pos_m, mm, k, first, lane_out, !bonded);
+        }
       }
       launch_check("adjoint pair");
       if (bonded) {

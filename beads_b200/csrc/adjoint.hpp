@@ -26,6 +26,7 @@ struct AdjointStore {
   uint32_t replicas = 0;      // R
   int max_types = 0;          // LJ table side of the largest replica table
   bool forward_done = false;
+  bool store_all = false;     // every step kept by the forward pass (no replay)
 
   // checkpoints: segment starts 0..segments-1, then the final state
   float4* ck_pos = nullptr;

@@ -187,6 +187,7 @@ struct DeviceView {
   const uint32_t* block_replica;
   const uint32_t* cell_replica;  // replica of each global cell
   unsigned long long* chain_launches;  // launches of the rebuild chain so far
+  long long* ke_part;            // [CUDA block][whole, frac] kinetic partials (fused kick)
   const LjCoeff* lj;
   uint32_t n_replicas;
   uint32_t n_slots;

@@ -120,7 +120,7 @@ class Engine {
                   const double* dihedral_k);
   // Runs `steps` velocity-Verlet steps from the current state (forces and
   // the list are rebuilt first, as a fresh run), keeping a checkpoint every
-  // `checkpoint_every` steps.  obs receives [step - record_from][replica]
+  // `checkpoint_every` steps (0: keep every step, no replay later).  obs receives [step - record_from][replica]
   // {pair+bonded PE, virial, thermo KE} for steps record_from..steps.
   void adjoint_forward(uint64_t steps, uint64_t record_from, uint32_t checkpoint_every,
                        double* obs);
@@ -144,6 +144,7 @@ class Engine {
   void set_sort_enabled(bool on);
   void adjoint_restore(uint32_t segment);
   void adjoint_record(uint32_t k);
+  void adjoint_segment_storage(uint32_t K);
   void adjoint_select_list(uint32_t a, uint32_t m, std::vector<int>& current,
                            const std::vector<uint32_t>& flags);
   std::unique_ptr<AdjointStore> adj_;

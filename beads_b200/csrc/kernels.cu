@@ -556,44 +556,100 @@ __device__ __forceinline__ double post_slot(const DeviceView& v, const ReplicaPa
   return ke;
 }
 
-// Block sum of the kinetic energy and, in the replica's last block, the
-// step's per-replica work.  Every block of the replica must call it.
+// The kernel that kicks (k_post, or the last force kernel when the kick is
+// fused) writes one fixed-point kinetic-energy partial per CUDA block: no
+// atomics on a shared address and no last-block handshake.  k_post_finish,
+// one block per replica, then sums that replica's partials (integer sums:
+// the order does not matter) and does the per-replica epilogue: Berendsen
+// lambda for the next step, step counter, observables.
+template <bool kKinetic>
+__device__ __forceinline__ void post_partial(const DeviceView& v, ReplicaState* st, bool real,
+                                             double ke) {
+  if (!kKinetic) return;
+  __shared__ long long part[2][kBlock / 32];
+  const Fixed f = real ? to_fixed(ke, &st->status) : Fixed{0, 0};
+  long long a = f.whole, c = f.frac;
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(kFull, a, o);
+    c += __shfl_down_sync(kFull, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    part[0][threadIdx.x >> 5] = a;
+    part[1][threadIdx.x >> 5] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long sa = 0, sc = 0;
+    for (int w = 0; w < kBlock / 32; ++w) {
+      sa += part[0][w];
+      sc += part[1][w];
+    }
+    v.ke_part[2 * (size_t)blockIdx.x] = sa;
+    v.ke_part[2 * (size_t)blockIdx.x + 1] = sc;
+  }
+}
+
+constexpr int kFinishThreads = 256;
+
 template <bool kKick, bool kObs, bool kKinetic>
-__device__ __forceinline__ void post_finish(const DeviceView& v, const ReplicaParams& p,
-                                            ReplicaState* st, uint32_t r, bool real,
-                                            double ke, uint32_t blocks_per_128 = 1) {
-  if (kKinetic) block_add_lane<kBlock>(real, ke, st, kAccKinetic);
-  const uint32_t n_blocks = p.n_pad / kBlock * blocks_per_128;
-  if (arrive_last(&st->done_post, n_blocks) && threadIdx.x == 0) {
-    const double kin = kKinetic ? take_total(st, kAccKinetic) : 0.0;
-    double lam = 1.0;
-    if (kKick && kKinetic && p.thermostat == 1 && kin > 0.0 && p.dof > 0.0) {
-      const double current = 2.0 * kin / p.dof;
-      const double arg = 1.0 + ((double)p.dt / p.tau) * (p.kt_target / current - 1.0);
-      lam = sqrt(arg > 0.0 ? arg : 0.0);
+__global__ void __launch_bounds__(kFinishThreads) k_post_finish(DeviceView v, uint32_t tpa) {
+  const uint32_t r = blockIdx.x;
+  const ReplicaParams& p = v.rp[r];
+  ReplicaState* st = &v.rs[r];
+  __shared__ long long part[2][kFinishThreads / 32];
+  long long a = 0, c = 0;
+  if (kKinetic) {
+    const uint32_t b0 = p.block_begin * tpa, b1 = (p.block_begin + p.n_pad / kBlock) * tpa;
+    for (uint32_t b = b0 + threadIdx.x; b < b1; b += kFinishThreads) {
+      a += v.ke_part[2 * (size_t)b];
+      c += v.ke_part[2 * (size_t)b + 1];
     }
-    if (kKick) {
-      st->lambda = lam;
-      st->step += 1ull;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(kFull, a, o);
+      c += __shfl_down_sync(kFull, c, o);
     }
-    if (kKinetic) st->last_kinetic = kin;
-    if (kObs) {
-      ReplicaObs o;
-      o.step = st->step;
-      o.pair_pe = take_total(st, kAccPair);
-      o.bond_pe = take_total(st, kAccBond);
-      o.angle_pe = take_total(st, kAccAngle);
-      o.dihedral_pe = take_total(st, kAccDihedral);
-      o.virial = take_total(st, kAccVirial);
-      o.ke_pre = kin;
-      o.lambda = lam;
-      o.builds = st->builds;
-      o.dangerous = st->dangerous;
-      o.status = st->status;
-      o.pad = 0;
-      v.obs[r] = o;
+    if ((threadIdx.x & 31) == 0) {
+      part[0][threadIdx.x >> 5] = a;
+      part[1][threadIdx.x >> 5] = c;
     }
-    st->done_post = 0u;
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  double kin = 0.0;
+  if (kKinetic) {
+    long long sa = 0, sc = 0;
+    for (int w = 0; w < kFinishThreads / 32; ++w) {
+      sa += part[0][w];
+      sc += part[1][w];
+    }
+    kin = from_fixed(sa, sc);
+  }
+  double lam = 1.0;
+  if (kKick && kKinetic && p.thermostat == 1 && kin > 0.0 && p.dof > 0.0) {
+    const double current = 2.0 * kin / p.dof;
+    const double arg = 1.0 + ((double)p.dt / p.tau) * (p.kt_target / current - 1.0);
+    lam = sqrt(arg > 0.0 ? arg : 0.0);
+  }
+  if (kKick) {
+    st->lambda = lam;
+    st->step += 1ull;
+  }
+  if (kKinetic) st->last_kinetic = kin;
+  if (kObs) {
+    ReplicaObs o;
+    o.step = st->step;
+    o.pair_pe = take_total(st, kAccPair);
+    o.bond_pe = take_total(st, kAccBond);
+    o.angle_pe = take_total(st, kAccAngle);
+    o.dihedral_pe = take_total(st, kAccDihedral);
+    o.virial = take_total(st, kAccVirial);
+    o.ke_pre = kin;
+    o.lambda = lam;
+    o.builds = st->builds;
+    o.dangerous = st->dangerous;
+    o.status = st->status;
+    o.pad = 0;
+    v.obs[r] = o;
   }
 }
 
@@ -783,7 +839,10 @@ __device__ __forceinline__ void lj_pairs(const DeviceView& v, const ReplicaParam
       const bool in0 = (k0 + u0 * kTpa + sub < n) && r2.x < rc2;
       const bool in1 = (k0 + u1 * kTpa + sub < n) && r2.y < rc2;
       const PairCoeff2 c = coeff.get(xj[u0].w, xj[u1].w);
-      float2 rr = make_float2(in0 ? r2.x : 1.0f, in1 ? r2.y : 1.0f);
+      // Out-of-range pairs get r^2 = 1e30: every power of sigma^2/r^2 then
+      // underflows to 0, so their force scale is exactly 0 without a select
+      // (the energy, needed only with observables, is masked explicitly).
+      float2 rr = make_float2(in0 ? r2.x : 1e30f, in1 ? r2.y : 1e30f);
       if (kClamp) {
         rr.x = fmaxf(rr.x, 0.49f * c.sigma2.x);
         rr.y = fmaxf(rr.y, 0.49f * c.sigma2.y);
@@ -795,8 +854,6 @@ __device__ __forceinline__ void lj_pairs(const DeviceView& v, const ReplicaParam
       const float2 neg6 = make_float2(-sr6.x, -sr6.y);
       const float2 g = __ffma2_rn(make_float2(2.0f, 2.0f), sr12, neg6);
       float2 fs = __fmul2_rn(__fmul2_rn(c.eps24, inv), g);
-      fs.x = in0 ? fs.x : 0.0f;
-      fs.y = in1 ? fs.y : 0.0f;
       ax.add_fma(h, fs, dx);
       ay.add_fma(h, fs, dy);
       az.add_fma(h, fs, dz);
@@ -873,7 +930,7 @@ __global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
     block_add_lane<kBlock>(owner, 0.5 * (double)e, st, kAccPair);
     block_add_lane<kBlock>(owner, 0.5 * (double)w, st, kAccVirial);
   }
-  if (kPost) post_finish<true, kObs, kKinetic>(v, p, st, r, owner, ke, kTpa);
+  if (kPost) post_partial<kKinetic>(v, st, owner, ke);
 }
 
 // ---------------------------------------------------------------------------
@@ -1065,17 +1122,15 @@ __global__ void __launch_bounds__(kBlock) k_bonded(DeviceView v) {
     block_add_lane<kBlock>(real, ed, st, kAccDihedral);
     block_add_lane<kBlock>(real, w, st, kAccVirial);
   }
-  if (kPost) post_finish<true, kObs, kKinetic>(v, p, st, r, real, ke);
+  if (kPost) post_partial<kKinetic>(v, st, real, ke);
 }
 
 // ---------------------------------------------------------------------------
-// post: second half-kick, kinetic energy (FP64 per slot, fixed-point total),
-// and per replica (last block): observables, Berendsen lambda for the next
-// step (applied lazily by pre), step counter.  The per-slot part and the
-// per-replica epilogue are shared by k_post and by the force kernels that
-// finish a step themselves (the last force kernel of a step holds the final
-// force of its slot in registers, so the kick needs no force re-read and no
-// extra launch).
+// post: second half-kick and kinetic energy (FP64 per slot, fixed-point
+// partial per block); k_post_finish then does the per-replica epilogue
+// (observables, Berendsen lambda for the next step, applied lazily by pre,
+// step counter).  The same per-slot work runs inside the last force kernel
+// when the schedule fuses the kick.
 
 template <bool kKick, bool kObs, bool kKinetic>
 __global__ void __launch_bounds__(kBlock) k_post(DeviceView v) {
@@ -1088,7 +1143,7 @@ __global__ void __launch_bounds__(kBlock) k_post(DeviceView v) {
   float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
   if (kKick && real) f = v.force[i];
   const double ke = post_slot<kKick, kKinetic || kObs>(v, p, st, i, real, f.x, f.y, f.z);
-  post_finish<kKick, kObs, kKinetic || kObs>(v, p, st, r, real, ke);
+  post_partial<kKinetic || kObs>(v, st, real, ke);
 }
 
 // Applies the pending Berendsen scale so host reads see the scaled velocities.
@@ -1302,21 +1357,38 @@ void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post)
 #undef BB_BONDED
     check_launch("bonded");
   }
+  if (fuse) {
+    const uint32_t tpa = bonded ? 1u : static_cast<uint32_t>(clamp ? 1 : l.lj_tpa);
+    const bool kin = fin == kForcePostKinetic || observables;
+    if (observables) {
+      k_post_finish<true, true, true><<<l.v.n_replicas, kFinishThreads, 0, l.stream>>>(l.v, tpa);
+    } else if (kin) {
+      k_post_finish<true, false, true><<<l.v.n_replicas, kFinishThreads, 0, l.stream>>>(l.v, tpa);
+    } else {
+      k_post_finish<true, false, false><<<l.v.n_replicas, kFinishThreads, 0, l.stream>>>(l.v, tpa);
+    }
+    check_launch("post finish");
+  }
   if (post && !fuse) launch_post(l, true, observables);
 }
 
 void launch_post(const StepLaunch& l, bool kick, bool observables) {
   const bool kin = l.need_kinetic != 0;
+  const dim3 fg(l.v.n_replicas);
   if (kick) {
     if (observables) {
       k_post<true, true, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+      k_post_finish<true, true, true><<<fg, kFinishThreads, 0, l.stream>>>(l.v, 1u);
     } else if (kin) {
       k_post<true, false, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+      k_post_finish<true, false, true><<<fg, kFinishThreads, 0, l.stream>>>(l.v, 1u);
     } else {
       k_post<true, false, false><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+      k_post_finish<true, false, false><<<fg, kFinishThreads, 0, l.stream>>>(l.v, 1u);
     }
   } else {
     k_post<false, true, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+    k_post_finish<false, true, true><<<fg, kFinishThreads, 0, l.stream>>>(l.v, 1u);
   }
   check_launch("post");
 }

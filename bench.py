@@ -362,10 +362,11 @@ def run_ours(args) -> None:
         st = eng.state()
         cpu = _cpu_baseline(st["positions"], spec, args.cpu_budget)
 
-    # Every step launches pre, the pair-force kernel and (unless the schedule
-    # fuses it) post; a step that rebuilds also runs the 7 kernels of the
+    # Every step launches pre, the pair-force kernel, post (unless the
+    # schedule fuses the kick into the force kernel) and the per-replica
+    # finish kernel; a step that rebuilds also runs the 7 kernels of the
     # rebuild chain (conditional graph node).
-    per_step = 2 if eng.tuning()["fuse_post"] else 3
+    per_step = 3 if eng.tuning()["fuse_post"] else 4
     gpu_launches = per_step * args.steps + 7 * int(timed_chains)
     line = {
         "metric": METRIC,
@@ -501,7 +502,7 @@ def run_replicas(args) -> None:
             "graph_warmup_steps": GRAPH_WARMUP,
             "schedule": schedule,
         },
-        "gpu_launches": (2 if schedule["fuse_post"] else 3) * args.steps + 7 * int(chains),
+        "gpu_launches": (3 if schedule["fuse_post"] else 4) * args.steps + 7 * int(chains),
         "clocks": clocks,
     }
     if rank == 0:
@@ -556,6 +557,7 @@ def run_adjoint(args) -> None:
         b.record(stream)
         b.synchronize()
         plain_s = a.elapsed_time(b) / 1e3
+        schedule = eng.tuning()
         # differentiated run (wall clock: host orchestration included)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -570,6 +572,27 @@ def run_adjoint(args) -> None:
         torch.cuda.synchronize()
         t2 = time.perf_counter()
     fwd_s, bwd_s = t1 - t0, t2 - t1
+    # The same gradient with every step's state kept by the forward pass
+    # (checkpoint_every = 0, no replay): the memory-for-compute trade that
+    # HBM affords at this size ((steps + 1) x 32 B per particle).
+    eps2 = eps.detach().clone().requires_grad_(True)
+    sig2 = sig.detach().clone().requires_grad_(True)
+    x2 = x0.clone().requires_grad_(True)
+    with Engine(specs) as eng2:
+        eng2.set_tuning(**{k: v for k, v in schedule.items() if k != "autotuned"})
+        eng2.run(max(3, args.warmup))
+        eng2.run(GRAPH_WARMUP)
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        obs2 = trajectory_observables(eng2, eps2, sig2, x2, v0.clone(), steps=steps,
+                                      record_from=steps - window + 1, checkpoint_every=0)
+        torch.cuda.synchronize()
+        t4 = time.perf_counter()
+        pe2 = obs2[:, :, 0].mean(0)
+        press2 = ((2.0 * obs2[:, :, 2] + obs2[:, :, 1]) / (3.0 * vols)).mean(0)
+        ((pe2 - pe_t) ** 2 + (press2 - p_t) ** 2).sum().backward()
+        torch.cuda.synchronize()
+        t5 = time.perf_counter()
     line = {
         "metric": ADJOINT_METRIC,
         "value": atoms * steps / (fwd_s + bwd_s),
@@ -592,7 +615,10 @@ def run_adjoint(args) -> None:
             "backward_s": bwd_s,
             "backward_over_plain_forward": bwd_s / plain_s,
             "forward_plus_backward_over_plain_forward": (fwd_s + bwd_s) / plain_s,
-            "loss": float(loss),
+            "stored_forward_s": t4 - t3,
+            "stored_backward_s": t5 - t4,
+            "stored_backward_over_plain_forward": (t5 - t4) / plain_s,
+            "loss": float(loss.detach()),
             "grad_eps": eps.grad.tolist(),
             "grad_sigma": sig.grad.tolist(),
             "grad_x0_norm": float(x.grad.norm()),

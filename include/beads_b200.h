@@ -290,7 +290,9 @@ BEADS_API int beads_set_lj(beads_ctx* ctx, uint32_t replica, const double* epsil
                            const double* sigma);
 /* Runs `steps` MD steps from the current state (list and forces rebuilt
  * first) keeping a checkpoint of the full step state every
- * `checkpoint_every` steps, and writes the observables of steps
+ * `checkpoint_every` steps (0: keep the state of every step, 32 bytes per
+ * particle and step, so the backward pass needs no replay), and writes the
+ * observables of steps
  * record_from..steps: observables[((step - record_from) * n_replicas + r) * 3
  * + {0, 1, 2}] = potential energy, virial (sum r.F), kinetic energy (as a
  * thermo row reports them).  Up to 4 particle types and 8 bonded types of

@@ -30,7 +30,7 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-@pytest.mark.parametrize("every", [7, 50])
+@pytest.mark.parametrize("every", [7, 50, 0])
 def test_adjoint_matches_fp64_autograd(every):
     specs = _small()
     steps, rec = 30, 12
@@ -227,3 +227,23 @@ def test_bonded_adjoint_matches_fp64_autograd():
     for key in ("x", "v", "eps", "sig", "bond_k", "bond_r0", "angle_k", "angle_theta0",
                 "dihedral_k"):
         assert _rel(ours[key].grad, ref[key].grad) < 1e-4, (key, ours[key].grad, ref[key].grad)
+
+
+def test_stored_trajectory_gives_the_replayed_gradients_bitwise():
+    """checkpoint_every = 0 keeps the forward's own states; replayed segments
+    reproduce them bit for bit, so both give the same gradients."""
+    specs = _small(n_replicas=1, seed=7)
+    grads = []
+    for every in (6, 0):
+        eps = torch.tensor(workloads.MIXTURE_EPS, requires_grad=True)
+        sig = torch.tensor(specs[0].sigma, requires_grad=True)
+        x = torch.tensor(specs[0].positions, dtype=torch.float64, requires_grad=True)
+        v = torch.tensor(specs[0].velocities, dtype=torch.float64, requires_grad=True)
+        with Engine(specs) as eng:
+            eng.set_tuning(2, False, 4, True)
+            obs = trajectory_observables(eng, eps, sig, x, v, steps=25, record_from=10,
+                                         checkpoint_every=every)
+            (obs[:, :, 0].sum() + 0.1 * obs[:, :, 1].sum()).backward()
+        grads.append((eps.grad.clone(), sig.grad.clone(), x.grad.clone(), v.grad.clone()))
+    for a, b in zip(*grads):
+        assert torch.equal(a, b)
