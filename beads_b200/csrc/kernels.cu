@@ -223,17 +223,18 @@ __global__ void __launch_bounds__(kBlock) k_scatter(DeviceView v) {
 // stable and the whole build deterministic.  One warp per cell; a bitonic
 // network in registers for <= 32 members, insertion sort otherwise.
 __global__ void __launch_bounds__(kBlock) k_cellsort(DeviceView v) {
-  const uint32_t r = blockIdx.y;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t g = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);  // global cell
+  if (g >= v.total_cells) return;                                     // warp-uniform
+  const uint32_t r = v.cell_replica[g];
   if (!v.rs[r].need_rebuild) return;
   const ReplicaParams& p = v.rp[r];
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t warps_per_block = kBlock / 32;
-  for (uint32_t c = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
-       c < p.n_cells; c += gridDim.x * warps_per_block) {
+  {
+    const uint32_t c = g - p.cell_begin;
     const uint32_t s0 = v.cell_start[p.start_base + c];
     const uint32_t s1 = v.cell_start[p.start_base + c + 1];
     const uint32_t n = s1 - s0;
-    if (n <= 1u) continue;
+    if (n <= 1u) return;
     if (n <= 32u) {
       uint32_t val = lane < n ? v.cell_atoms[s0 + lane] : 0xffffffffu;
       for (uint32_t k = 2; k <= 32; k <<= 1) {
@@ -1215,13 +1216,6 @@ void check_launch(const char* what) {
   }
 }
 
-uint32_t cell_grid_x(uint32_t max_cells) {
-  const uint32_t warps = kBlock / 32;
-  uint32_t g = (max_cells + warps - 1) / warps;
-  if (g > 1184u) g = 1184u;  // 8 blocks per SM on 148 SMs, grid-stride beyond
-  return g < 1u ? 1u : g;
-}
-
 }  // namespace
 
 void launch_pre(const StepLaunch& l, int mode, cudaGraphConditionalHandle cond, bool use_cond) {
@@ -1252,8 +1246,7 @@ void launch_rebuild(const StepLaunch& l, bool force_all) {
   check_launch("scan");
   k_scatter<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
   check_launch("scatter");
-  const dim3 cg(cell_grid_x(l.max_cells_per_replica), l.v.n_replicas);
-  k_cellsort<<<cg, kBlock, 0, l.stream>>>(l.v);
+  k_cellsort<<<(l.v.total_cells + kBlock / 32 - 1) / (kBlock / 32), kBlock, 0, l.stream>>>(l.v);
   check_launch("cellsort");
   k_reorder_gather<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
   check_launch("reorder_gather");
