@@ -526,11 +526,9 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   v.obs = dalloc<ReplicaObs>(n);
   uint32_t* d_block_replica = dalloc<uint32_t>(block_replica.size());
   std::vector<uint32_t> cell_replica(C);
-  bool all_regular = true;
   for (uint32_t r = 0; r < n; ++r) {
     std::fill(cell_replica.begin() + rp[r].cell_begin,
               cell_replica.begin() + rp[r].cell_begin + rp[r].n_cells, r);
-    for (int a = 0; a < 3; ++a) all_regular = all_regular && rp[r].nc[a] >= 4u;
   }
   uint32_t* d_cell_replica = dalloc<uint32_t>(C);
   v.chain_launches = dalloc<unsigned long long>(1);
@@ -588,7 +586,6 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   launch_.v = v;
   launch_.stream = stream_;
   launch_.max_cells_per_replica = max_cells;
-  launch_.all_regular = all_regular ? 1 : 0;
   launch_.lj_tpa = 1;
   launch_.lj_unroll = 8;
   launch_.lj_no_l1 = 0;

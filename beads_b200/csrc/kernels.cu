@@ -428,28 +428,16 @@ __device__ __forceinline__ void scan_range(const DeviceView& v, const ReplicaPar
   }
 }
 
+// The list rows of the particles of global cell g (one warp).
 template <int kCap, bool kRegular>
-__global__ void __launch_bounds__(kBlock, kCap > 16 ? 2 : 8) k_build(DeviceView v) {
-  __shared__ __align__(16) float sh_x[kBuildWarps][32];
-  __shared__ __align__(16) float sh_y[kBuildWarps][32];
-  __shared__ __align__(16) float sh_z[kBuildWarps][32];
-  __shared__ __align__(16) uint32_t sh_j[kBuildWarps][32];
-  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t g = blockIdx.x * kBuildWarps + warp;  // global cell
-  if (g >= v.total_cells) return;                      // warp-uniform exits
-  const uint32_t r = v.cell_replica[g];
-  ReplicaState* st = &v.rs[r];
-  if (!st->need_rebuild) return;
-  const ReplicaParams& p = v.rp[r];
+__device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaParams& p,
+                                           ReplicaState* st, uint32_t g, uint32_t lane,
+                                           float* sx, float* sy, float* sz, uint32_t* sj) {
   const uint32_t c = g - p.cell_begin;
   const uint32_t* start = v.cell_start + p.start_base;
   const uint32_t cs = start[c], ce = start[c + 1];
   const uint32_t nx = p.nc[0], ny = p.nc[1], nz = p.nc[2];
   const uint32_t cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
-  float* sx = sh_x[warp];
-  float* sy = sh_y[warp];
-  float* sz = sh_z[warp];
-  uint32_t* sj = sh_j[warp];
   bool any_overflow = false;
 
   for (uint32_t i0 = cs; i0 < ce; i0 += 32u) {
@@ -521,6 +509,28 @@ __global__ void __launch_bounds__(kBlock, kCap > 16 ? 2 : 8) k_build(DeviceView 
     any_overflow |= active && L.count > L.cap;
   }
   if (__any_sync(kFull, any_overflow) && lane == 0) atomicOr(&st->status, kStatusNeighborOverflow);
+}
+
+// One warp per global cell; the replica's grid decides between the
+// whole-cell shift (>= 4 cells on every axis) and the per-pair reference form.
+template <int kCap>
+__global__ void __launch_bounds__(kBlock, kCap > 16 ? 2 : 8) k_build(DeviceView v) {
+  __shared__ __align__(16) float sh_x[kBuildWarps][32];
+  __shared__ __align__(16) float sh_y[kBuildWarps][32];
+  __shared__ __align__(16) float sh_z[kBuildWarps][32];
+  __shared__ __align__(16) uint32_t sh_j[kBuildWarps][32];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t g = blockIdx.x * kBuildWarps + warp;  // global cell
+  if (g >= v.total_cells) return;                      // warp-uniform exits
+  const uint32_t r = v.cell_replica[g];
+  ReplicaState* st = &v.rs[r];
+  if (!st->need_rebuild) return;
+  const ReplicaParams& p = v.rp[r];
+  if (p.nc[0] >= 4u && p.nc[1] >= 4u && p.nc[2] >= 4u) {
+    build_cell<kCap, true>(v, p, st, g, lane, sh_x[warp], sh_y[warp], sh_z[warp], sh_j[warp]);
+  } else {
+    build_cell<kCap, false>(v, p, st, g, lane, sh_x[warp], sh_y[warp], sh_z[warp], sh_j[warp]);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1257,9 +1267,7 @@ void launch_rebuild(const StepLaunch& l, bool force_all) {
     check_launch("project_exclusions");
   }
   const uint32_t bg = (l.v.total_cells + kBuildWarps - 1) / kBuildWarps;
-#define BB_BUILD(cap)                                                          \
-  (l.all_regular ? k_build<cap, true><<<bg, kBlock, 0, l.stream>>>(l.v)        \
-                 : k_build<cap, false><<<bg, kBlock, 0, l.stream>>>(l.v))
+#define BB_BUILD(cap) k_build<cap><<<bg, kBlock, 0, l.stream>>>(l.v)
   switch (l.excl_cap) {
     case 0: BB_BUILD(0); break;
     case 4: BB_BUILD(4); break;

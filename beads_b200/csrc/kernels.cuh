@@ -17,7 +17,6 @@ struct StepLaunch {
   uint32_t max_cells_per_replica;
   uint32_t max_atoms_per_replica;
   int excl_cap;           // 0, 4, 8, 16, 32 or 64
-  int all_regular;        // every replica has >= 4 cells on every axis
   int lj_tpa;             // threads per particle of the pair-force kernel: 1, 2, 4
   int lj_unroll;          // list entries in flight per thread and batch: 4 or 8
   int lj_no_l1;           // list entries loaded without allocating L1 lines

@@ -442,15 +442,20 @@ def run_replicas(args) -> None:
     eng.run(GRAPH_WARMUP)
     builds_before = sum(eng.counters(r)["builds"] for r in range(len(specs)))
     chains_before = eng.counters()["chain_launches"]
+    profile_region = os.environ.get("BEADS_PROFILE_TIMED") == "1"
     sampler = ClockSampler(local)
     torch.cuda.synchronize()
     sampler.start()
+    if profile_region:  # lets a profiler started with capture off see only these steps
+        torch.cuda.profiler.start()
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     start.record(stream)
     eng.run(args.steps)
     stop.record(stream)
     stop.synchronize()
+    if profile_region:
+        torch.cuda.profiler.stop()
     clocks = sampler.stop()
     batch_ms = start.elapsed_time(stop)
     builds = sum(eng.counters(r)["builds"] for r in range(len(specs))) - builds_before
