@@ -365,7 +365,10 @@ struct BuildLane {
   }
 };
 
-// Tests the staged candidates [0, m) of this warp against one lane.
+// Tests the staged candidates [0, m) of this warp against one lane: the
+// distance tests of the chunk fill a 32-bit acceptance mask (two candidates
+// per packed FP32x2 step), then only the accepted candidates are walked, in
+// ascending order, for the self / exclusion checks and the append.
 template <int kCap, bool kRegular>
 __device__ __forceinline__ void test_staged(const ReplicaParams& p, BuildLane<kCap, kRegular>& L,
                                             const float* sx, const float* sy, const float* sz,
@@ -373,11 +376,13 @@ __device__ __forceinline__ void test_staged(const ReplicaParams& p, BuildLane<kC
                                             float2 s2y, float2 s2z) {
   const float2 neg1 = make_float2(-1.0f, -1.0f);
   const float cut = p.search_cut_sq;
-  for (uint32_t t = 0; t < m; t += 2) {
+  uint32_t mask = 0u;
+#pragma unroll
+  for (uint32_t t = 0; t < 32u; t += 2) {
+    if (t >= m) break;  // warp-uniform
     const float2 jx = *reinterpret_cast<const float2*>(sx + t);
     const float2 jy = *reinterpret_cast<const float2*>(sy + t);
     const float2 jz = *reinterpret_cast<const float2*>(sz + t);
-    const uint2 jj = *reinterpret_cast<const uint2*>(sj + t);
     float2 dx, dy, dz;
     if (kRegular) {
       // fl(xi - xj) (xj * -1 is exact), then fl(d + s).
@@ -393,9 +398,15 @@ __device__ __forceinline__ void test_staged(const ReplicaParams& p, BuildLane<kC
                        ref_delta(L.xi.z, jz.y, p.len[2], p.half[2]));
     }
     const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-    // The staged tail entry of an odd chunk carries slot 0xffffffff.
-    L.put(!(r2.x > cut) && jj.x != L.i && !L.excluded(jj.x), jj.x);
-    L.put(!(r2.y > cut) && jj.y != L.i && jj.y != 0xffffffffu && !L.excluded(jj.y), jj.y);
+    mask |= (!(r2.x > cut) ? 1u : 0u) << t;
+    mask |= (!(r2.y > cut) ? 2u : 0u) << t;
+  }
+  if (m < 32u) mask &= (1u << m) - 1u;  // the odd tail's pad entry and stale entries
+  while (mask != 0u) {
+    const uint32_t t = __ffs(mask) - 1;
+    mask &= mask - 1u;
+    const uint32_t j = sj[t];
+    L.put(j != L.i && !L.excluded(j), j);
   }
 }
 
@@ -514,7 +525,7 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
 // One warp per global cell; the replica's grid decides between the
 // whole-cell shift (>= 4 cells on every axis) and the per-pair reference form.
 template <int kCap>
-__global__ void __launch_bounds__(kBlock, kCap > 16 ? 2 : 8) k_build(DeviceView v) {
+__global__ void __launch_bounds__(kBlock, kCap > 16 ? 2 : (kCap >= 8 ? 4 : 8)) k_build(DeviceView v) {
   __shared__ __align__(16) float sh_x[kBuildWarps][32];
   __shared__ __align__(16) float sh_y[kBuildWarps][32];
   __shared__ __align__(16) float sh_z[kBuildWarps][32];
