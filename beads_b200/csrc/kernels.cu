@@ -77,6 +77,7 @@ k_pre(DeviceView v, float sd_dmax, float sd_fref, cudaGraphConditionalHandle con
       }
     }
     int4 im = v.img[slot];
+    bool crossed;
     {
       const float cx = floorf(__fmul_rn(__fsub_rn(x.x, p.lo[0]), p.inv_len[0]));
       const float cy = floorf(__fmul_rn(__fsub_rn(x.y, p.lo[1]), p.inv_len[1]));
@@ -87,9 +88,10 @@ k_pre(DeviceView v, float sd_dmax, float sd_fref, cudaGraphConditionalHandle con
       im.x += (int)cx;
       im.y += (int)cy;
       im.z += (int)cz;
+      crossed = cx != 0.0f || cy != 0.0f || cz != 0.0f;
     }
     v.pos[slot] = x;
-    v.img[slot] = im;
+    if (crossed) v.img[slot] = im;  // the image changes only on a boundary crossing
     if (check_step) {
       const float4 rx = v.ref_pos[slot];
       const int4 ri = v.ref_img[slot];
@@ -172,38 +174,60 @@ __global__ void __launch_bounds__(kBlock) k_bin(DeviceView v) {
 }
 
 // rebuild 2: exclusive scan of the counts of one replica (one block per
-// replica); resets the counts for the next build.
+// replica); resets the counts for the next build.  Warp w owns a contiguous
+// range of cells: it sums the range (coalesced loads), the block scans the
+// 32 warp sums, then each warp rescans its range 32 cells at a time with
+// shuffles and writes the starts.
 constexpr int kScanThreads = 1024;
+constexpr int kScanWarps = kScanThreads / 32;
 __global__ void __launch_bounds__(kScanThreads) k_scan(DeviceView v) {
   const uint32_t r = blockIdx.x;
   if (!v.rs[r].need_rebuild) return;
   const ReplicaParams& p = v.rp[r];
-  __shared__ uint32_t sums[kScanThreads];
+  __shared__ uint32_t warp_base[kScanWarps];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t n = p.n_cells;
-  const uint32_t per = (n + kScanThreads - 1) / kScanThreads;
-  const uint32_t begin = min(n, threadIdx.x * per);
+  const uint32_t per = ((n + kScanWarps - 1) / kScanWarps + 31u) & ~31u;
+  const uint32_t begin = min(n, warp * per);
   const uint32_t end = min(n, begin + per);
+  uint32_t* count = v.cell_count + p.cell_begin;
   uint32_t local = 0;
-  for (uint32_t c = begin; c < end; ++c) local += v.cell_count[p.cell_begin + c];
-  sums[threadIdx.x] = local;
+#pragma unroll 8
+  for (uint32_t c = begin + lane; c < end; c += 32u) local += count[c];
+  const uint32_t total = __reduce_add_sync(kFull, local);
+  if (lane == 0) warp_base[warp] = total;
   __syncthreads();
-  // Hillis-Steele inclusive scan over the thread sums.
-  for (int o = 1; o < kScanThreads; o <<= 1) {
-    const uint32_t add = threadIdx.x >= (uint32_t)o ? sums[threadIdx.x - o] : 0u;
-    __syncthreads();
-    sums[threadIdx.x] += add;
-    __syncthreads();
+  if (warp == 0) {
+    const uint32_t t = warp_base[lane];
+    uint32_t inc = t;
+#pragma unroll
+    for (uint32_t o = 1; o < 32u; o <<= 1) {
+      const uint32_t up = __shfl_up_sync(kFull, inc, o);
+      if (lane >= o) inc += up;
+    }
+    warp_base[lane] = inc - t;
   }
-  uint32_t run = p.atom_begin + (threadIdx.x > 0 ? sums[threadIdx.x - 1] : 0u);
-  for (uint32_t c = begin; c < end; ++c) {
-    const uint32_t g = p.cell_begin + c;
-    const uint32_t cnt = v.cell_count[g];
-    v.cell_start[p.start_base + c] = run;
-    v.cell_cursor[g] = run;
-    v.cell_count[g] = 0u;
-    run += cnt;
+  __syncthreads();
+  uint32_t run = p.atom_begin + warp_base[warp];
+  uint32_t* start = v.cell_start + p.start_base;
+  uint32_t* cursor = v.cell_cursor + p.cell_begin;
+  for (uint32_t c0 = begin; c0 < end; c0 += 32u) {
+    const uint32_t c = c0 + lane;
+    const uint32_t cnt = c < end ? count[c] : 0u;
+    uint32_t inc = cnt;
+#pragma unroll
+    for (uint32_t o = 1; o < 32u; o <<= 1) {
+      const uint32_t up = __shfl_up_sync(kFull, inc, o);
+      if (lane >= o) inc += up;
+    }
+    if (c < end) {
+      start[c] = run + inc - cnt;
+      cursor[c] = run + inc - cnt;
+      count[c] = 0u;
+    }
+    run += __shfl_sync(kFull, inc, 31);
   }
-  if (threadIdx.x == 0) v.cell_start[p.start_base + n] = p.atom_begin + p.n_atoms;
+  if (threadIdx.x == 0) start[n] = p.atom_begin + p.n_atoms;
 }
 
 // rebuild 3: scatter slots into their cells (order inside a cell is fixed by
@@ -221,7 +245,10 @@ __global__ void __launch_bounds__(kBlock) k_scatter(DeviceView v) {
 
 // rebuild 4: sort each cell's slots ascending, which makes the counting sort
 // stable and the whole build deterministic.  One warp per cell; a bitonic
-// network in registers for <= 32 members, insertion sort otherwise.
+// network in registers for <= 32 members, insertion sort otherwise.  Also
+// gathers the positions in cell order (pos2[q] = pos[cell_atoms[q]]), so the
+// list build reads its candidates with contiguous loads that do not wait on
+// the slot index; the reorder kernels find them there too.
 __global__ void __launch_bounds__(kBlock) k_cellsort(DeviceView v) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t g = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);  // global cell
@@ -234,28 +261,36 @@ __global__ void __launch_bounds__(kBlock) k_cellsort(DeviceView v) {
     const uint32_t s0 = v.cell_start[p.start_base + c];
     const uint32_t s1 = v.cell_start[p.start_base + c + 1];
     const uint32_t n = s1 - s0;
-    if (n <= 1u) return;
     if (n <= 32u) {
       uint32_t val = lane < n ? v.cell_atoms[s0 + lane] : 0xffffffffu;
-      for (uint32_t k = 2; k <= 32; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-          const uint32_t other = __shfl_xor_sync(kFull, val, j);
-          const bool up = (lane & k) == 0u;
-          const bool lower = (lane & j) == 0u;
-          val = (lower == up) ? min(val, other) : max(val, other);
+      if (n > 1u) {
+        for (uint32_t k = 2; k <= 32; k <<= 1) {
+          for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t other = __shfl_xor_sync(kFull, val, j);
+            const bool up = (lane & k) == 0u;
+            const bool lower = (lane & j) == 0u;
+            val = (lower == up) ? min(val, other) : max(val, other);
+          }
         }
       }
-      if (lane < n) v.cell_atoms[s0 + lane] = val;
-    } else if (lane == 0) {
-      for (uint32_t a = s0 + 1; a < s1; ++a) {
-        const uint32_t key = v.cell_atoms[a];
-        uint32_t q = a;
-        while (q > s0 && v.cell_atoms[q - 1] > key) {
-          v.cell_atoms[q] = v.cell_atoms[q - 1];
-          --q;
-        }
-        v.cell_atoms[q] = key;
+      if (lane < n) {
+        v.cell_atoms[s0 + lane] = val;
+        v.pos2[s0 + lane] = v.pos[val];
       }
+    } else {
+      if (lane == 0) {
+        for (uint32_t a = s0 + 1; a < s1; ++a) {
+          const uint32_t key = v.cell_atoms[a];
+          uint32_t q = a;
+          while (q > s0 && v.cell_atoms[q - 1] > key) {
+            v.cell_atoms[q] = v.cell_atoms[q - 1];
+            --q;
+          }
+          v.cell_atoms[q] = key;
+        }
+      }
+      __syncwarp();
+      for (uint32_t q = s0 + lane; q < s1; q += 32u) v.pos2[q] = v.pos[v.cell_atoms[q]];
     }
   }
 }
@@ -269,8 +304,7 @@ __global__ void __launch_bounds__(kBlock) k_reorder_gather(DeviceView v) {
   const ReplicaParams& p = v.rp[r];
   const uint32_t k = b * kBlock + threadIdx.x;
   if (k - p.atom_begin >= p.n_atoms) return;
-  const uint32_t old = v.cell_atoms[k];
-  v.pos2[k] = v.pos[old];
+  const uint32_t old = v.cell_atoms[k];  // pos2[k] is pos[old] already (k_cellsort)
   v.vel2[k] = v.vel[old];
   v.img2[k] = v.img[old];
   v.tag2[k] = v.tag[old];
@@ -322,226 +356,245 @@ k_project_exclusions(DeviceView v, int force_all) {
 // rule: skip self and excluded partners, keep r^2 <= (rc+skin)^2, count
 // overflow past max_neighbors.  Also captures the displacement reference.
 //
-// One warp per cell: lane l owns the l-th particle of the cell (cells of more
-// than 32 particles take several passes).  Candidates are staged 32 at a time
-// in shared memory (structure of arrays, so two consecutive candidates are
-// one 8-byte broadcast read per coordinate) and every lane tests them two at
-// a time on the packed FP32x2 pipe.  Candidates are visited in the
-// reference's stencil order (z, y, x cells; ascending slot inside a cell), so
-// each particle's list order is fixed.
+// One warp per cell, the candidates on the lanes.  The stencil of the cell is
+// a list of segments (contiguous runs of cell_atoms) in the reference's
+// stencil order (z, y, x cells; ascending slot inside a cell); their
+// concatenation is the candidate stream, walked 64 candidates at a time:
+// lane l holds candidates l and 32 + l of a chunk, both tested against one
+// home particle per iteration on the packed FP32x2 pipe.  Two ballots give
+// the accepted candidates in stream order; each accepted lane writes its
+// entry at the home particle's count plus its rank among the accepted, so a
+// particle's list order is the stream order under any schedule.  Every lane
+// does useful work whatever the cell occupancy, and appends never diverge.
 //
-// kRegular (every axis has >= 4 cells): a stencil cell reached across the
-// periodic boundary gets one shift s = +-L for the whole cell and the
-// difference is fl(fl(xi - xj) + s).  For any pair that can pass the search
-// cutoff this is exactly the reference's form (fl(xi - xj), then fl(d -+ L)
-// when |d| > L/2), because with >= 4 cells per axis a neighbour-cell pair
-// has |xi - xj| < L/2 unless it wraps, and a wrapped one has |xi - xj| > L/2.
-// Otherwise (small-dimension and direct paths) the reference form is applied
-// per pair.
+// Regular grids (every axis >= 4 cells): a stencil row of three x-cells is
+// one segment (two where it wraps in x), 18 segments at most.  A cell
+// reached across the periodic boundary gets one shift s = +-L for the whole
+// segment and the difference is fl(fl(xi - xj) + s).  For any pair that can
+// pass the search cutoff this is exactly the reference's form (fl(xi - xj),
+// then fl(d -+ L) when |d| > L/2), because with >= 4 cells per axis a
+// neighbour-cell pair has |xi - xj| < L/2 unless it wraps, and a wrapped one
+// has |xi - xj| > L/2.  Cells away from the boundary have no shift at all.
+// Small-dimension and direct grids: each of the min(n, 3)^3 stencil cells is
+// a segment and the reference's minimum image is applied per pair.
 constexpr int kBuildWarps = kBlock / 32;
+constexpr uint32_t kMaxSegments = 27;
 
-template <int kCap, bool kRegular>
-struct BuildLane {
-  uint32_t i;
-  float2 xx, xy, xz;  // own coordinates, duplicated for the packed pipe
-  float4 xi;
-  uint32_t* row;      // entry 0 of this particle's list; entry k at row[k * kGroup]
-  uint32_t cap;
-  uint32_t count;     // candidates accepted (may pass cap: overflow)
-  uint32_t ex[kCap > 0 ? kCap : 1];
-
-  // Branch-free append: the store is predicated, the count always advances
-  // for an accepted candidate so overflow is count > cap at the end.
-  __device__ __forceinline__ void put(bool ok, uint32_t j) {
-    if (ok && count < cap) row[count * kGroup] = j;
-    count += ok ? 1u : 0u;
-  }
-
-  __device__ __forceinline__ bool excluded(uint32_t j) const {
-    bool e = false;
-#pragma unroll
-    for (int k = 0; k < kCap; ++k) e |= (ex[k] == j);
-    return e;
-  }
+struct BuildShared {
+  uint32_t seg_end[kMaxSegments];  // stream offset one past the segment
+  uint32_t seg_q[kMaxSegments];    // cell_atoms index of the segment's stream offset 0
+  float seg_s[3][kMaxSegments];    // periodic shift of the segment (regular grids)
+  float4 home_a[32];               // {x, x, y, y} of the home particles
+  float4 home_b[32];               // {z, z, slot bits, 0}
 };
 
-// Tests the staged candidates [0, m) of this warp against one lane: the
-// distance tests of the chunk fill a 32-bit acceptance mask (two candidates
-// per packed FP32x2 step), then only the accepted candidates are walked, in
-// ascending order, for the self / exclusion checks and the append.
-template <int kCap, bool kRegular>
-__device__ __forceinline__ void test_staged(const ReplicaParams& p, BuildLane<kCap, kRegular>& L,
-                                            const float* sx, const float* sy, const float* sz,
-                                            const uint32_t* sj, uint32_t m, float2 s2x,
-                                            float2 s2y, float2 s2z) {
-  const float2 neg1 = make_float2(-1.0f, -1.0f);
+enum BuildForm : int { kBuildInterior = 0, kBuildShifted = 1, kBuildMinImage = 2 };
+
+// Tests one chunk of candidates against the home particles [0, nh) and
+// appends the accepted ones.  my_cnt: lane h holds home particle h's count.
+template <int kCap, int kForm>
+__device__ __forceinline__ void build_chunk(const DeviceView& v, const ReplicaParams& p,
+                                            const BuildShared& sh, uint32_t nh, uint32_t lane,
+                                            uint32_t jx, uint32_t jy, float2 nxj, float2 nyj,
+                                            float2 nzj, float2 s2x, float2 s2y, float2 s2z,
+                                            uint32_t& my_cnt) {
   const float cut = p.search_cut_sq;
-  uint32_t mask = 0u;
-#pragma unroll
-  for (uint32_t t = 0; t < 32u; t += 2) {
-    if (t >= m) break;  // warp-uniform
-    const float2 jx = *reinterpret_cast<const float2*>(sx + t);
-    const float2 jy = *reinterpret_cast<const float2*>(sy + t);
-    const float2 jz = *reinterpret_cast<const float2*>(sz + t);
+  const uint32_t cap = p.max_neighbors;
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll 2
+  for (uint32_t h = 0; h < nh; ++h) {
+    const float4 ha = sh.home_a[h];
+    const float4 hb = sh.home_b[h];
+    const uint32_t i = __float_as_uint(hb.z);
     float2 dx, dy, dz;
-    if (kRegular) {
-      // fl(xi - xj) (xj * -1 is exact), then fl(d + s).
-      dx = __fadd2_rn(__ffma2_rn(jx, neg1, L.xx), s2x);
-      dy = __fadd2_rn(__ffma2_rn(jy, neg1, L.xy), s2y);
-      dz = __fadd2_rn(__ffma2_rn(jz, neg1, L.xz), s2z);
+    if (kForm == kBuildMinImage) {
+      dx = make_float2(ref_delta(ha.x, -nxj.x, p.len[0], p.half[0]),
+                       ref_delta(ha.x, -nxj.y, p.len[0], p.half[0]));
+      dy = make_float2(ref_delta(ha.z, -nyj.x, p.len[1], p.half[1]),
+                       ref_delta(ha.z, -nyj.y, p.len[1], p.half[1]));
+      dz = make_float2(ref_delta(hb.x, -nzj.x, p.len[2], p.half[2]),
+                       ref_delta(hb.x, -nzj.y, p.len[2], p.half[2]));
     } else {
-      dx = make_float2(ref_delta(L.xi.x, jx.x, p.len[0], p.half[0]),
-                       ref_delta(L.xi.x, jx.y, p.len[0], p.half[0]));
-      dy = make_float2(ref_delta(L.xi.y, jy.x, p.len[1], p.half[1]),
-                       ref_delta(L.xi.y, jy.y, p.len[1], p.half[1]));
-      dz = make_float2(ref_delta(L.xi.z, jz.x, p.len[2], p.half[2]),
-                       ref_delta(L.xi.z, jz.y, p.len[2], p.half[2]));
+      // fl(xi + (-xj)) is fl(xi - xj); a zero shift leaves it unchanged.
+      dx = __fadd2_rn(make_float2(ha.x, ha.y), nxj);
+      dy = __fadd2_rn(make_float2(ha.z, ha.w), nyj);
+      dz = __fadd2_rn(make_float2(hb.x, hb.y), nzj);
+      if (kForm == kBuildShifted) {
+        dx = __fadd2_rn(dx, s2x);
+        dy = __fadd2_rn(dy, s2y);
+        dz = __fadd2_rn(dz, s2z);
+      }
     }
     const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-    mask |= (!(r2.x > cut) ? 1u : 0u) << t;
-    mask |= (!(r2.y > cut) ? 2u : 0u) << t;
-  }
-  if (m < 32u) mask &= (1u << m) - 1u;  // the odd tail's pad entry and stale entries
-  while (mask != 0u) {
-    const uint32_t t = __ffs(mask) - 1;
-    mask &= mask - 1u;
-    const uint32_t j = sj[t];
-    L.put(j != L.i && !L.excluded(j), j);
-  }
-}
-
-// Stages candidates [q0, q1) of cell_atoms 32 at a time in this warp's
-// shared arrays and tests them against every active lane.
-template <int kCap, bool kRegular>
-__device__ __forceinline__ void scan_range(const DeviceView& v, const ReplicaParams& p,
-                                           BuildLane<kCap, kRegular>& L, bool active,
-                                           uint32_t lane, uint32_t q0, uint32_t q1,
-                                           float2 s2x, float2 s2y, float2 s2z, float* sx,
-                                           float* sy, float* sz, uint32_t* sj) {
-  for (uint32_t q = q0; q < q1; q += 32u) {
-    const uint32_t m = min(32u, q1 - q);
-    __syncwarp();
-    if (lane < m) {
-      const uint32_t j = v.cell_atoms[q + lane];
-      const float4 xj = v.pos[j];
-      sx[lane] = xj.x;
-      sy[lane] = xj.y;
-      sz[lane] = xj.z;
-      sj[lane] = j;
-    } else if (lane == m) {  // pad the odd tail: tested, never appended
-      sx[lane] = 0.f;
-      sy[lane] = 0.f;
-      sz[lane] = 0.f;
-      sj[lane] = 0xffffffffu;
+    bool ax = !(r2.x > cut) && jx != i;
+    bool ay = !(r2.y > cut) && jy != i;
+    uint32_t bx = __ballot_sync(kFull, ax);
+    uint32_t by = __ballot_sync(kFull, ay);
+    if ((bx | by) == 0u) continue;  // warp-uniform
+    if (kCap > 0) {
+      // Exclusion rows are padded with 0xffffffff after the last partner.
+      const uint32_t* ex = v.excl_slot + (size_t)i * v.excl_cap;
+#pragma unroll 4
+      for (int e = 0; e < kCap; ++e) {
+        const uint32_t xe = __ldg(ex + e);
+        if (xe == 0xffffffffu) break;  // warp-uniform
+        ax = ax && jx != xe;
+        ay = ay && jy != xe;
+      }
+      bx = __ballot_sync(kFull, ax);
+      by = __ballot_sync(kFull, ay);
     }
-    __syncwarp();
-    if (active) test_staged<kCap, kRegular>(p, L, sx, sy, sz, sj, m, s2x, s2y, s2z);
+    const uint32_t cnt = __shfl_sync(kFull, my_cnt, h);
+    const uint32_t nx = __popc(bx);
+    const uint32_t kx = cnt + __popc(bx & lt);
+    const uint32_t ky = cnt + nx + __popc(by & lt);
+    uint32_t* row = v.nbr + nbr_index(i, 0, v.nbr_stride);
+    if (ax && kx < cap) row[(size_t)kx * kGroup] = jx;
+    if (ay && ky < cap) row[(size_t)ky * kGroup] = jy;
+    if (lane == h) my_cnt = cnt + nx + __popc(by);
   }
 }
 
 // The list rows of the particles of global cell g (one warp).
-template <int kCap, bool kRegular>
+template <int kCap>
 __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaParams& p,
                                            ReplicaState* st, uint32_t g, uint32_t lane,
-                                           float* sx, float* sy, float* sz, uint32_t* sj) {
+                                           BuildShared& sh) {
   const uint32_t c = g - p.cell_begin;
   const uint32_t* start = v.cell_start + p.start_base;
   const uint32_t cs = start[c], ce = start[c + 1];
+  if (cs == ce) return;
   const uint32_t nx = p.nc[0], ny = p.nc[1], nz = p.nc[2];
   const uint32_t cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+  const bool regular = nx >= 4u && ny >= 4u && nz >= 4u;
+
+  // Segment table: lane s describes segment s.
+  uint32_t q0 = 0u, q1 = 0u;
+  float shx = 0.0f, shy = 0.0f, shz = 0.0f;
+  if (regular) {
+    if (lane < 18u) {
+      const uint32_t a = lane / 6u, bb = (lane / 2u) % 3u, sg = lane & 1u;
+      const uint32_t zc = stencil_cell(cz, nz, a), yc = stencil_cell(cy, ny, bb);
+      shz = (cz == 0u && a == 0u) ? p.len[2] : (cz == nz - 1u && a == 2u) ? -p.len[2] : 0.0f;
+      shy = (cy == 0u && bb == 0u) ? p.len[1] : (cy == ny - 1u && bb == 2u) ? -p.len[1] : 0.0f;
+      // A row is [cx-1, cx+2) unless it wraps in x, where it splits in two.
+      uint32_t lo = cx - 1u, hi = cx + 2u;
+      bool used = sg == 0u;
+      if (cx == 0u) {
+        lo = sg == 0u ? nx - 1u : 0u, hi = sg == 0u ? nx : 2u, used = true;
+        shx = sg == 0u ? p.len[0] : 0.0f;
+      } else if (cx == nx - 1u) {
+        lo = sg == 0u ? nx - 2u : 0u, hi = sg == 0u ? nx : 1u, used = true;
+        shx = sg == 0u ? 0.0f : -p.len[0];
+      }
+      if (used) {
+        const uint32_t row = nx * (yc + ny * zc);
+        q0 = start[row + lo];
+        q1 = start[row + hi];
+      }
+    }
+  } else {
+    const uint32_t sxn = min(nx, 3u), syn = min(ny, 3u), szn = min(nz, 3u);
+    if (lane < sxn * syn * szn) {
+      const uint32_t k = lane % sxn, bb = (lane / sxn) % syn, a = lane / (sxn * syn);
+      const uint32_t lc = stencil_cell(cx, nx, k) +
+                          nx * (stencil_cell(cy, ny, bb) + ny * stencil_cell(cz, nz, a));
+      q0 = start[lc];
+      q1 = start[lc + 1];
+    }
+  }
+  uint32_t end = q1 - q0;  // inclusive scan of the segment lengths
+#pragma unroll
+  for (uint32_t o = 1; o < 32u; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kFull, end, o);
+    if (lane >= o) end += t;
+  }
+  const uint32_t total = __shfl_sync(kFull, end, 31);
+  __syncwarp();
+  if (lane < kMaxSegments) {
+    sh.seg_end[lane] = end;
+    sh.seg_q[lane] = q0 - (end - (q1 - q0));
+    sh.seg_s[0][lane] = shx;
+    sh.seg_s[1][lane] = shy;
+    sh.seg_s[2][lane] = shz;
+  }
+  const int form = !regular ? kBuildMinImage
+                   : (cx == 0u || cy == 0u || cz == 0u || cx == nx - 1u || cy == ny - 1u ||
+                      cz == nz - 1u)
+                       ? kBuildShifted
+                       : kBuildInterior;
+  const uint32_t nseg = regular ? 18u : kMaxSegments;
   bool any_overflow = false;
 
   for (uint32_t i0 = cs; i0 < ce; i0 += 32u) {
-    const bool active = i0 + lane < ce;
-    BuildLane<kCap, kRegular> L;
-    L.i = active ? v.cell_atoms[i0 + lane] : 0xfffffffeu;
-    L.xi = active ? v.pos[L.i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    L.xx = make_float2(L.xi.x, L.xi.x);
-    L.xy = make_float2(L.xi.y, L.xi.y);
-    L.xz = make_float2(L.xi.z, L.xi.z);
-    L.count = 0;
-    L.cap = p.max_neighbors;
-    L.row = v.nbr + nbr_index(active ? L.i : 0u, 0, v.nbr_stride);
-    if (kCap > 0) {
-      const uint32_t* row = v.excl_slot + (size_t)(active ? L.i : 0u) * v.excl_cap;
-#pragma unroll
-      for (int e = 0; e < kCap; ++e) L.ex[e] = active ? row[e] : 0xffffffffu;
+    const uint32_t nh = min(32u, ce - i0);
+    uint32_t i = 0u;
+    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncwarp();
+    if (lane < nh) {
+      i = v.cell_atoms[i0 + lane];
+      xi = v.pos2[i0 + lane];
+      sh.home_a[lane] = make_float4(xi.x, xi.x, xi.y, xi.y);
+      sh.home_b[lane] = make_float4(xi.z, xi.z, __uint_as_float(i), 0.0f);
     }
-    if (kRegular) {
-      // 9 rows of three x-cells; a row is one contiguous run of cell_atoms
-      // unless it wraps in x, where it splits at the boundary.
-      for (uint32_t a = 0; a < 3u; ++a) {
-        const uint32_t zc = stencil_cell(cz, nz, a);
-        const float sz_ = (cz == 0u && a == 0u) ? p.len[2]
-                          : (cz == nz - 1u && a == 2u) ? -p.len[2] : 0.0f;
-        for (uint32_t bb = 0; bb < 3u; ++bb) {
-          const uint32_t yc = stencil_cell(cy, ny, bb);
-          const float sy_ = (cy == 0u && bb == 0u) ? p.len[1]
-                            : (cy == ny - 1u && bb == 2u) ? -p.len[1] : 0.0f;
-          const uint32_t row = nx * (yc + ny * zc);
-          const float2 s2y = make_float2(sy_, sy_), s2z = make_float2(sz_, sz_);
-          // Up to two segments: [first run, second run) with their x shifts.
-          uint32_t c0 = cx - 1u, c1 = cx + 2u, d0 = 0u, d1 = 0u;
-          float sx0 = 0.0f, sx1 = 0.0f;
-          uint32_t nseg = 1u;
-          if (cx == 0u) {
-            c0 = nx - 1u, c1 = nx, sx0 = p.len[0], d0 = 0u, d1 = 2u, nseg = 2u;
-          } else if (cx == nx - 1u) {
-            c0 = nx - 2u, c1 = nx, d0 = 0u, d1 = 1u, sx1 = -p.len[0], nseg = 2u;
-          }
-          for (uint32_t sg = 0; sg < nseg; ++sg) {
-            const uint32_t lo = sg == 0u ? c0 : d0, hi = sg == 0u ? c1 : d1;
-            const float shx = sg == 0u ? sx0 : sx1;
-            scan_range(v, p, L, active, lane, start[row + lo], start[row + hi],
-                       make_float2(shx, shx), s2y, s2z, sx, sy, sz, sj);
-          }
-        }
+    __syncwarp();
+    uint32_t my_cnt = 0u;
+    uint32_t sa = 0u, sb = 0u;  // segment of this lane's two candidates
+    for (uint32_t base = 0; base < total; base += 64u) {
+      const uint32_t ua = base + lane, ub = base + 32u + lane;
+      while (sa < nseg && ua >= sh.seg_end[sa]) ++sa;
+      while (sb < nseg && ub >= sh.seg_end[sb]) ++sb;
+      // Past the stream: an infinite coordinate fails every distance test.
+      uint32_t jx = 0xffffffffu, jy = 0xffffffffu;
+      float4 xa = make_float4(INFINITY, 0.f, 0.f, 0.f), xb = xa;
+      if (ua < total) {
+        jx = v.cell_atoms[sh.seg_q[sa] + ua];
+        xa = v.pos2[sh.seg_q[sa] + ua];
       }
-    } else {
-      const uint32_t sxn = min(nx, 3u), syn = min(ny, 3u), szn = min(nz, 3u);
-      const float2 zero = make_float2(0.f, 0.f);
-      for (uint32_t a = 0; a < szn; ++a) {
-        const uint32_t zc = stencil_cell(cz, nz, a);
-        for (uint32_t bb = 0; bb < syn; ++bb) {
-          const uint32_t row = nx * (stencil_cell(cy, ny, bb) + ny * zc);
-          for (uint32_t k = 0; k < sxn; ++k) {
-            const uint32_t lc = row + stencil_cell(cx, nx, k);
-            scan_range(v, p, L, active, lane, start[lc], start[lc + 1], zero, zero, zero,
-                       sx, sy, sz, sj);
-          }
-        }
+      if (ub < total) {
+        jy = v.cell_atoms[sh.seg_q[sb] + ub];
+        xb = v.pos2[sh.seg_q[sb] + ub];
+      }
+      const float2 nxj = make_float2(-xa.x, -xb.x), nyj = make_float2(-xa.y, -xb.y),
+                   nzj = make_float2(-xa.z, -xb.z);
+      if (form == kBuildInterior) {
+        const float2 z = make_float2(0.f, 0.f);
+        build_chunk<kCap, kBuildInterior>(v, p, sh, nh, lane, jx, jy, nxj, nyj, nzj, z, z, z,
+                                          my_cnt);
+      } else if (form == kBuildShifted) {
+        const uint32_t ta = min(sa, kMaxSegments - 1u), tb = min(sb, kMaxSegments - 1u);
+        build_chunk<kCap, kBuildShifted>(
+            v, p, sh, nh, lane, jx, jy, nxj, nyj, nzj,
+            make_float2(sh.seg_s[0][ta], sh.seg_s[0][tb]),
+            make_float2(sh.seg_s[1][ta], sh.seg_s[1][tb]),
+            make_float2(sh.seg_s[2][ta], sh.seg_s[2][tb]), my_cnt);
+      } else {
+        const float2 z = make_float2(0.f, 0.f);
+        build_chunk<kCap, kBuildMinImage>(v, p, sh, nh, lane, jx, jy, nxj, nyj, nzj, z, z, z,
+                                          my_cnt);
       }
     }
-    if (active) {
-      v.nbr_count[L.i] = min(L.count, L.cap);
-      v.ref_pos[L.i] = L.xi;
-      v.ref_img[L.i] = v.img[L.i];
+    if (lane < nh) {
+      v.nbr_count[i] = min(my_cnt, p.max_neighbors);
+      v.ref_pos[i] = xi;
+      v.ref_img[i] = v.img[i];
     }
-    any_overflow |= active && L.count > L.cap;
+    any_overflow |= lane < nh && my_cnt > p.max_neighbors;
   }
   if (__any_sync(kFull, any_overflow) && lane == 0) atomicOr(&st->status, kStatusNeighborOverflow);
 }
 
-// One warp per global cell; the replica's grid decides between the
-// whole-cell shift (>= 4 cells on every axis) and the per-pair reference form.
+// One warp per global cell of any replica.
 template <int kCap>
-__global__ void __launch_bounds__(kBlock, kCap > 16 ? 2 : (kCap >= 8 ? 4 : 8)) k_build(DeviceView v) {
-  __shared__ __align__(16) float sh_x[kBuildWarps][32];
-  __shared__ __align__(16) float sh_y[kBuildWarps][32];
-  __shared__ __align__(16) float sh_z[kBuildWarps][32];
-  __shared__ __align__(16) uint32_t sh_j[kBuildWarps][32];
+__global__ void __launch_bounds__(kBlock, 8) k_build(DeviceView v) {
+  __shared__ BuildShared sh[kBuildWarps];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t g = blockIdx.x * kBuildWarps + warp;  // global cell
   if (g >= v.total_cells) return;                      // warp-uniform exits
   const uint32_t r = v.cell_replica[g];
   ReplicaState* st = &v.rs[r];
   if (!st->need_rebuild) return;
-  const ReplicaParams& p = v.rp[r];
-  if (p.nc[0] >= 4u && p.nc[1] >= 4u && p.nc[2] >= 4u) {
-    build_cell<kCap, true>(v, p, st, g, lane, sh_x[warp], sh_y[warp], sh_z[warp], sh_j[warp]);
-  } else {
-    build_cell<kCap, false>(v, p, st, g, lane, sh_x[warp], sh_y[warp], sh_z[warp], sh_j[warp]);
-  }
+  build_cell<kCap>(v, v.rp[r], st, g, lane, sh[warp]);
 }
 
 // ---------------------------------------------------------------------------
@@ -611,7 +664,7 @@ __device__ __forceinline__ void post_partial(const DeviceView& v, ReplicaState* 
   }
 }
 
-constexpr int kFinishThreads = 256;
+constexpr int kFinishThreads = 1024;
 
 template <bool kKick, bool kObs, bool kKinetic>
 __global__ void __launch_bounds__(kFinishThreads) k_post_finish(DeviceView v, uint32_t tpa) {
@@ -622,9 +675,11 @@ __global__ void __launch_bounds__(kFinishThreads) k_post_finish(DeviceView v, ui
   long long a = 0, c = 0;
   if (kKinetic) {
     const uint32_t b0 = p.block_begin * tpa, b1 = (p.block_begin + p.n_pad / kBlock) * tpa;
+#pragma unroll 4
     for (uint32_t b = b0 + threadIdx.x; b < b1; b += kFinishThreads) {
-      a += v.ke_part[2 * (size_t)b];
-      c += v.ke_part[2 * (size_t)b + 1];
+      const longlong2 q = reinterpret_cast<const longlong2*>(v.ke_part)[b];
+      a += q.x;
+      c += q.y;
     }
     for (int o = 16; o > 0; o >>= 1) {
       a += __shfl_down_sync(kFull, a, o);
