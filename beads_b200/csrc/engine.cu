@@ -21,7 +21,7 @@ void cuda_check(cudaError_t e, const char* what) {
 
 namespace {
 
-constexpr uint32_t kChunkMax = 64;     // steps per captured graph
+constexpr uint32_t kChunkMax = 16;     // steps per captured graph
 constexpr double kKbNmKjMol = 0.00831446261815324;
 constexpr double kPressNmKjMol = 16.60539067;
 

@@ -42,7 +42,7 @@ METRIC = "atom-steps/s on 1 B200 (1M-bead binary LJ mixture, FP32 pair math, fix
 UNIT = "atom-steps/s"
 N_BEADS = 1_048_576
 E2E_STEPS = 100  # MD steps per end-to-end call
-GRAPH_WARMUP = 127  # untimed steps that instantiate every captured step graph
+GRAPH_WARMUP = 31  # untimed steps that instantiate every captured step graph
 
 
 def _dist():
@@ -281,8 +281,8 @@ def run_ours(args) -> None:
     # the kernel-level timing below).
     for _ in range(max(3, args.warmup)):
         eng.run(1)
-    # Runs replay captured graphs of 64, 32, ..., 1 steps; one untimed run of
-    # 127 steps instantiates each of them outside the timed region.
+    # Runs replay captured graphs of 16, 8, ..., 1 steps; one untimed run of
+    # 31 steps instantiates each of them outside the timed region.
     eng.run(GRAPH_WARMUP)
     stats = eng.list_stats()
     mean_nbr = stats["entries"] / spec.n
