@@ -16,6 +16,10 @@ namespace bb {
 constexpr int kBlock = 128;          // threads per block of per-slot kernels
 constexpr int kGroup = 32;           // neighbour-list interleave width
 constexpr int kMaxTypes = 16;        // LJ type table held in shared memory
+// Coordinates of the far particle at pos[n_slots] (pads neighbour batches);
+// its squared distance to any particle is ~3e36, above kFarR2.
+constexpr float kFarCoord = 1.0e18f;
+constexpr float kFarR2 = 1.0e36f;
 // Fixed-point totals: a per-slot value v is split into floor(v) and the
 // fraction in units of 2^-32, each summed in its own 64-bit integer word.
 // Integer sums do not depend on the order of the additions, so totals are

@@ -357,7 +357,11 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   for (uint32_t r = 0; r < n; ++r) rp[r].excl_degree = max_degree;
 
   // ---- particles in input order ----
-  std::vector<float4> h_pos(S), h_vel(S);
+  // One slot past the last holds the far particle that pads neighbour
+  // batches in the pair-force kernel (its distance to every particle is
+  // beyond any cutoff).
+  std::vector<float4> h_pos(S + 1), h_vel(S);
+  h_pos[S] = make_float4(kFarCoord, kFarCoord, kFarCoord, 0.f);
   std::vector<int4> h_img(S);
   std::vector<uint32_t> h_tag(S, 0xffffffffu), h_mol(S, 0), slot_of_tag(T, 0);
   std::vector<uint32_t> block_replica(S / kBlock);
@@ -487,7 +491,7 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   v.nbr_stride = stride;
   v.excl_cap = static_cast<uint32_t>(excl_cap);
   v.has_bonded = any_bonded ? 1 : 0;
-  v.pos = dalloc<float4>(S);
+  v.pos = dalloc<float4>(S + 1);
   v.vel = dalloc<float4>(S);
   v.force = dalloc<float4>(S);
   v.img = dalloc<int4>(S);
@@ -539,7 +543,7 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   auto up = [&](void* dst, const void* src, size_t bytes) {
     if (bytes) cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_), "upload");
   };
-  up(v.pos, h_pos.data(), S * sizeof(float4));
+  up(v.pos, h_pos.data(), (S + 1) * sizeof(float4));
   up(v.vel, h_vel.data(), S * sizeof(float4));
   up(v.img, h_img.data(), S * sizeof(int4));
   up(v.tag, h_tag.data(), S * sizeof(uint32_t));

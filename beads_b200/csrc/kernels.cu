@@ -869,7 +869,7 @@ __device__ __forceinline__ void lj_pairs(const DeviceView& v, const ReplicaParam
 #pragma unroll
   for (uint32_t u = 0; u < kUnroll; ++u) {
     const uint32_t k = u * kTpa + sub;
-    jn[u] = k < n ? list_load<kNoL1>(list + (size_t)(u * kTpa) * kGroup) : i;
+    jn[u] = k < n ? list_load<kNoL1>(list + (size_t)(u * kTpa) * kGroup) : v.n_slots;
   }
   for (uint32_t k0 = 0; k0 < n_warp; k0 += kStep) {
     uint32_t j[kUnroll];
@@ -881,7 +881,8 @@ __device__ __forceinline__ void lj_pairs(const DeviceView& v, const ReplicaParam
 #pragma unroll
     for (uint32_t u = 0; u < kUnroll; ++u) {
       const uint32_t k = k0 + kStep + u * kTpa + sub;
-      jn[u] = k < n ? list_load<kNoL1>(list + (size_t)(k0 + kStep + u * kTpa) * kGroup) : i;
+      jn[u] = k < n ? list_load<kNoL1>(list + (size_t)(k0 + kStep + u * kTpa) * kGroup)
+                    : v.n_slots;
     }
     // Own entries 2h and 2h+1 of the batch run through the packed FP32x2
     // pipe of sm_100 (__fadd2_rn / __fmul2_rn / __ffma2_rn round each lane
@@ -898,7 +899,8 @@ __device__ __forceinline__ void lj_pairs(const DeviceView& v, const ReplicaParam
       // the pair straddles the periodic boundary, which needs r^2 above
       // (L_min/2)^2; only then (warp-uniform branch) recompute that pair
       // with the exactly rounded minimum image.
-      const bool far0 = r2.x >= half_min_sq, far1 = r2.y >= half_min_sq;
+      const bool far0 = r2.x >= half_min_sq && r2.x < kFarR2;
+      const bool far1 = r2.y >= half_min_sq && r2.y < kFarR2;
       if (kFar && __any_sync(kFull, far0 || far1)) {
         if (far0) {
           dx.x = acc_delta(xi.x, xj[u0].x, p.len[0], p.half[0]);
@@ -913,8 +915,9 @@ __device__ __forceinline__ void lj_pairs(const DeviceView& v, const ReplicaParam
           r2.y = norm2(dx.y, dy.y, dz.y);
         }
       }
-      const bool in0 = (k0 + u0 * kTpa + sub < n) && r2.x < rc2;
-      const bool in1 = (k0 + u1 * kTpa + sub < n) && r2.y < rc2;
+      // Entries past the particle's count are the far particle: r^2 > rc^2.
+      const bool in0 = r2.x < rc2;
+      const bool in1 = r2.y < rc2;
       const PairCoeff2 c = coeff.get(xj[u0].w, xj[u1].w);
       // Out-of-range pairs get r^2 = 1e30: every power of sigma^2/r^2 then
       // underflows to 0, so their force scale is exactly 0 without a select
