@@ -16,6 +16,7 @@ namespace bb {
 constexpr int kBlock = 128;          // threads per block of per-slot kernels
 constexpr int kGroup = 32;           // neighbour-list interleave width
 constexpr int kMaxTypes = 16;        // LJ type table held in shared memory
+constexpr uint32_t kKeBuckets = 128; // fixed-point kinetic-energy buckets per replica
 // Coordinates of the far particle at pos[n_slots] (pads neighbour batches);
 // its squared distance to any particle is ~3e36, above kFarR2.
 constexpr float kFarCoord = 1.0e18f;
@@ -191,7 +192,7 @@ struct DeviceView {
   const uint32_t* block_replica;
   const uint32_t* cell_replica;  // replica of each global cell
   unsigned long long* chain_launches;  // launches of the rebuild chain so far
-  long long* ke_part;            // [CUDA block][whole, frac] kinetic partials (fused kick)
+  long long* ke_part;            // [replica][kKeBuckets][whole, frac] kinetic-energy buckets
   const LjCoeff* lj;
   uint32_t n_replicas;
   uint32_t n_slots;

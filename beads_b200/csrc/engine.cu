@@ -536,7 +536,7 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   }
   uint32_t* d_cell_replica = dalloc<uint32_t>(C);
   v.chain_launches = dalloc<unsigned long long>(1);
-  v.ke_part = dalloc<long long>(2ull * (S / kBlock) * 4);  // up to 4 CUDA blocks per 128 slots
+  v.ke_part = dalloc<long long>(2ull * n * kKeBuckets);  // zeroed; emptied by every finish
   cuda_check(cudaMemsetAsync(v.chain_launches, 0, sizeof(unsigned long long), stream_), "memset");
   LjCoeff* d_lj = dalloc<LjCoeff>(h_lj.size());
 

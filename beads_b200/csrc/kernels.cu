@@ -607,14 +607,14 @@ enum ForceMode : int {
   kForcePostKinetic = 3,  // forces, kick and the kinetic-energy total
 };
 
-// Kick of one slot with its final force; returns its kinetic energy.
+// Kick of one slot with its final force, from its velocity vm as loaded
+// before; returns its kinetic energy.
 template <bool kKick, bool kKinetic>
-__device__ __forceinline__ double post_slot(const DeviceView& v, const ReplicaParams& p,
-                                            ReplicaState* st, uint32_t i, bool real,
-                                            float fx, float fy, float fz) {
+__device__ __forceinline__ double post_slot_vm(const DeviceView& v, const ReplicaParams& p,
+                                               ReplicaState* st, uint32_t i, bool real,
+                                               float4 vm, float fx, float fy, float fz) {
   double ke = 0.0;
   if (real) {
-    float4 vm = v.vel[i];
     if (kKick) {
       const float h = __fdiv_rn(__fmul_rn(0.5f, p.dt), vm.w);
       vm.x = __fmaf_rn(h, fx, vm.x);
@@ -631,19 +631,53 @@ __device__ __forceinline__ double post_slot(const DeviceView& v, const ReplicaPa
   return ke;
 }
 
+template <bool kKick, bool kKinetic>
+__device__ __forceinline__ double post_slot(const DeviceView& v, const ReplicaParams& p,
+                                            ReplicaState* st, uint32_t i, bool real,
+                                            float fx, float fy, float fz) {
+  const float4 vm = real ? v.vel[i] : make_float4(0.f, 0.f, 0.f, 1.f);
+  return post_slot_vm<kKick, kKinetic>(v, p, st, i, real, vm, fx, fy, fz);
+}
+
 // The kernel that kicks (k_post, or the last force kernel when the kick is
-// fused) writes one fixed-point kinetic-energy partial per CUDA block: no
-// atomics on a shared address and no last-block handshake.  k_post_finish,
-// one block per replica, then sums that replica's partials (integer sums:
-// the order does not matter) and does the per-replica epilogue: Berendsen
-// lambda for the next step, step counter, observables.
+// fused) sums each warp's kinetic energies in fixed point and adds the warp's
+// total into one of kKeBuckets buckets of its replica (warp index modulo
+// kKeBuckets): no block barrier, so a warp retires as soon as it is done,
+// and few warps share a bucket.  Integer sums do not depend on order, so the
+// total is the same bits whatever the schedule.  k_post_finish, one block
+// per replica, then sums and empties that replica's buckets and does the
+// per-replica epilogue: Berendsen lambda for the next step, step counter,
+// observables.
 template <bool kKinetic>
-__device__ __forceinline__ void post_partial(const DeviceView& v, ReplicaState* st, bool real,
-                                             double ke) {
+__device__ __forceinline__ void post_partial(const DeviceView& v, ReplicaState* st, uint32_t r,
+                                             bool real, double ke) {
+  if (!kKinetic) return;
+  const Fixed f = real ? to_fixed(ke, &st->status) : Fixed{0, 0};
+  long long a = f.whole, c = f.frac;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(kFull, a, o);
+    c += __shfl_down_sync(kFull, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    unsigned long long* bucket = reinterpret_cast<unsigned long long*>(v.ke_part) +
+                                 2 * ((size_t)r * kKeBuckets + warp % kKeBuckets);
+    if (a != 0) atomicAdd(bucket, static_cast<unsigned long long>(a));
+    if (c != 0) atomicAdd(bucket + 1, static_cast<unsigned long long>(c));
+  }
+}
+
+// Same, one bucket add per block (k_post: a short streaming kernel where the
+// block barrier costs little and fewer adds contend for the buckets).
+template <bool kKinetic>
+__device__ __forceinline__ void post_partial_block(const DeviceView& v, ReplicaState* st,
+                                                   uint32_t r, bool real, double ke) {
   if (!kKinetic) return;
   __shared__ long long part[2][kBlock / 32];
   const Fixed f = real ? to_fixed(ke, &st->status) : Fixed{0, 0};
   long long a = f.whole, c = f.frac;
+#pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     a += __shfl_down_sync(kFull, a, o);
     c += __shfl_down_sync(kFull, c, o);
@@ -659,27 +693,31 @@ __device__ __forceinline__ void post_partial(const DeviceView& v, ReplicaState* 
       sa += part[0][w];
       sc += part[1][w];
     }
-    v.ke_part[2 * (size_t)blockIdx.x] = sa;
-    v.ke_part[2 * (size_t)blockIdx.x + 1] = sc;
+    unsigned long long* bucket = reinterpret_cast<unsigned long long*>(v.ke_part) +
+                                 2 * ((size_t)r * kKeBuckets + blockIdx.x % kKeBuckets);
+    if (sa != 0) atomicAdd(bucket, static_cast<unsigned long long>(sa));
+    if (sc != 0) atomicAdd(bucket + 1, static_cast<unsigned long long>(sc));
   }
 }
 
-constexpr int kFinishThreads = 1024;
+constexpr int kFinishThreads = 128;
+static_assert(kKeBuckets <= (uint32_t)kFinishThreads, "one finish thread per bucket");
 
 template <bool kKick, bool kObs, bool kKinetic>
-__global__ void __launch_bounds__(kFinishThreads) k_post_finish(DeviceView v, uint32_t tpa) {
+__global__ void __launch_bounds__(kFinishThreads) k_post_finish(DeviceView v) {
   const uint32_t r = blockIdx.x;
   const ReplicaParams& p = v.rp[r];
   ReplicaState* st = &v.rs[r];
   __shared__ long long part[2][kFinishThreads / 32];
   long long a = 0, c = 0;
   if (kKinetic) {
-    const uint32_t b0 = p.block_begin * tpa, b1 = (p.block_begin + p.n_pad / kBlock) * tpa;
-#pragma unroll 4
-    for (uint32_t b = b0 + threadIdx.x; b < b1; b += kFinishThreads) {
-      const longlong2 q = reinterpret_cast<const longlong2*>(v.ke_part)[b];
-      a += q.x;
-      c += q.y;
+    if (threadIdx.x < kKeBuckets) {
+      longlong2* bucket = reinterpret_cast<longlong2*>(v.ke_part) + (size_t)r * kKeBuckets +
+                          threadIdx.x;
+      const longlong2 q = *bucket;
+      *bucket = make_longlong2(0, 0);
+      a = q.x;
+      c = q.y;
     }
     for (int o = 16; o > 0; o >>= 1) {
       a += __shfl_down_sync(kFull, a, o);
@@ -964,6 +1002,7 @@ __global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
   const uint32_t i = sb * kBlock + (blockIdx.x % kTpa) * kAtoms + threadIdx.x / kTpa;
   const bool real = (i - p.atom_begin) < p.n_atoms;
   LjAcc<kTpa> ax, ay, az, ae, aw;
+  float4 vm_kick = make_float4(0.f, 0.f, 0.f, 1.f);
   ax.zero();
   ay.zero();
   az.zero();
@@ -973,6 +1012,9 @@ __global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
     // Every lane of the warp (padding lanes included, with n = 0) runs the
     // same number of batches, so the warp votes below are convergent.
     const float4 xi = v.pos[i];
+    // With the kick fused, the velocity is requested before the pair loop so
+    // its latency is hidden behind it.
+    if (kPost) vm_kick = (real && sub == 0u) ? v.vel[i] : make_float4(0.f, 0.f, 0.f, 1.f);
     CoeffRow<kNt> coeff;
     coeff.init(table + __float_as_int(xi.w) * nt);
     const uint32_t n = real ? v.nbr_count[i] : 0u;
@@ -1004,13 +1046,13 @@ __global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
   if (sub == 0u) v.force[i] = make_float4(fx, fy, fz, 0.f);
   ReplicaState* st = &v.rs[r];
   double ke = 0.0;
-  if (kPost) ke = post_slot<true, kKinetic>(v, p, st, i, owner, fx, fy, fz);
+  if (kPost) ke = post_slot_vm<true, kKinetic>(v, p, st, i, owner, vm_kick, fx, fy, fz);
   if (kObs) {
     const float e = ae.total(), w = aw.total();
     block_add_lane<kBlock>(owner, 0.5 * (double)e, st, kAccPair);
     block_add_lane<kBlock>(owner, 0.5 * (double)w, st, kAccVirial);
   }
-  if (kPost) post_partial<kKinetic>(v, st, owner, ke);
+  if (kPost) post_partial<kKinetic>(v, st, r, owner, ke);
 }
 
 // ---------------------------------------------------------------------------
@@ -1202,7 +1244,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded(DeviceView v) {
     block_add_lane<kBlock>(real, ed, st, kAccDihedral);
     block_add_lane<kBlock>(real, w, st, kAccVirial);
   }
-  if (kPost) post_partial<kKinetic>(v, st, real, ke);
+  if (kPost) post_partial<kKinetic>(v, st, r, real, ke);
 }
 
 // ---------------------------------------------------------------------------
@@ -1223,7 +1265,7 @@ __global__ void __launch_bounds__(kBlock) k_post(DeviceView v) {
   float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
   if (kKick && real) f = v.force[i];
   const double ke = post_slot<kKick, kKinetic || kObs>(v, p, st, i, real, f.x, f.y, f.z);
-  post_partial<kKinetic || kObs>(v, st, real, ke);
+  post_partial_block<kKinetic || kObs>(v, st, r, real, ke);
 }
 
 // Applies the pending Berendsen scale so host reads see the scaled velocities.
@@ -1428,14 +1470,13 @@ void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post)
     check_launch("bonded");
   }
   if (fuse) {
-    const uint32_t tpa = bonded ? 1u : static_cast<uint32_t>(clamp ? 1 : l.lj_tpa);
     const bool kin = fin == kForcePostKinetic || observables;
     if (observables) {
-      k_post_finish<true, true, true><<<l.v.n_replicas, kFinishThreads, 0, l.stream>>>(l.v, tpa);
+      k_post_finish<true, true, true><<<l.v.n_replicas, kFinishThreads, 0, l.stream>>>(l.v);
     } else if (kin) {
-      k_post_finish<true, false, true><<<l.v.n_replicas, kFinishThreads, 0, l.stream>>>(l.v, tpa);
+      k_post_finish<true, false, true><<<l.v.n_replicas, kFinishThreads, 0, l.stream>>>(l.v);
     } else {
-      k_post_finish<true, false, false><<<l.v.n_replicas, kFinishThreads, 0, l.stream>>>(l.v, tpa);
+      k_post_finish<true, false, false><<<l.v.n_replicas, kFinishThreads, 0, l.stream>>>(l.v);
     }
     check_launch("post finish");
   }
@@ -1448,17 +1489,17 @@ void launch_post(const StepLaunch& l, bool kick, bool observables) {
   if (kick) {
     if (observables) {
       k_post<true, true, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
-      k_post_finish<true, true, true><<<fg, kFinishThreads, 0, l.stream>>>(l.v, 1u);
+      k_post_finish<true, true, true><<<fg, kFinishThreads, 0, l.stream>>>(l.v);
     } else if (kin) {
       k_post<true, false, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
-      k_post_finish<true, false, true><<<fg, kFinishThreads, 0, l.stream>>>(l.v, 1u);
+      k_post_finish<true, false, true><<<fg, kFinishThreads, 0, l.stream>>>(l.v);
     } else {
       k_post<true, false, false><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
-      k_post_finish<true, false, false><<<fg, kFinishThreads, 0, l.stream>>>(l.v, 1u);
+      k_post_finish<true, false, false><<<fg, kFinishThreads, 0, l.stream>>>(l.v);
     }
   } else {
     k_post<false, true, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
-    k_post_finish<false, true, true><<<fg, kFinishThreads, 0, l.stream>>>(l.v, 1u);
+    k_post_finish<false, true, true><<<fg, kFinishThreads, 0, l.stream>>>(l.v);
   }
   check_launch("post");
 }
