@@ -106,6 +106,14 @@ __global__ void k_adj_list_positions(DeviceView v, AdjView a, uint32_t segment,
                      : a.seg_pos[(size_t)src * a.slots + i];
 }
 
+// Crossing counts of restored slots: img - ref_img of the checkpoint.
+__global__ void k_adj_cross(DeviceView v) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= v.n_slots) return;
+  const int4 im = v.img[i], ri = v.ref_img[i];
+  v.cross[i] = pack_cross(im.x - ri.x, im.y - ri.y, im.z - ri.z);
+}
+
 __global__ void k_adj_mark_all(DeviceView v) {
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= v.n_replicas) return;
@@ -605,6 +613,8 @@ void Engine::adjoint_restore(uint32_t c) {
   d2d(v_.img, A.ck_img + c * S, S * sizeof(int4));
   d2d(v_.ref_pos, A.ck_ref_pos + c * S, S * sizeof(float4));
   d2d(v_.ref_img, A.ck_ref_img + c * S, S * sizeof(int4));
+  k_adj_cross<<<(static_cast<uint32_t>(S) + kBlock - 1) / kBlock, kBlock, 0, stream_>>>(v_);
+  launch_check("adjoint crossings");
   cuda_check(cudaMemcpyAsync(v_.rs, A.ck_state.data() + static_cast<size_t>(c) * A.replicas,
                              A.replicas * sizeof(ReplicaState), cudaMemcpyHostToDevice, stream_),
              "adjoint restore");

@@ -151,6 +151,7 @@ struct DeviceView {
   uint32_t* mol;
   float4* ref_pos;
   int4* ref_img;
+  uint32_t* cross;  // net boundary crossings since the last build (see pack_cross)
   // reorder scratch
   float4* pos2;
   float4* vel2;

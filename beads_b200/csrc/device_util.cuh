@@ -107,6 +107,22 @@ __device__ __forceinline__ float acc_delta(float xi, float xj, float len,
   return d;
 }
 
+// Net periodic-boundary crossings of a slot since its last list build
+// (img - ref_img), three signed 10-bit fields in one word, so the
+// displacement check reads 4 bytes per slot instead of both image vectors.
+// Bit 31 marks a field that left [-511, 511]; the check then treats the
+// slot as displaced (a crossing count that large cannot occur while the
+// rebuild policy holds).
+constexpr uint32_t kCrossSaturated = 0x80000000u;
+__device__ __forceinline__ int cross_field(uint32_t c, int k) {
+  return static_cast<int>(c << (22 - 10 * k)) >> 22;
+}
+__device__ __forceinline__ uint32_t pack_cross(int x, int y, int z) {
+  const bool sat = x < -511 || x > 511 || y < -511 || y > 511 || z < -511 || z > 511;
+  return (static_cast<uint32_t>(x) & 0x3ffu) | ((static_cast<uint32_t>(y) & 0x3ffu) << 10) |
+         ((static_cast<uint32_t>(z) & 0x3ffu) << 20) | (sat ? kCrossSaturated : 0u);
+}
+
 // |d|^2 with the contraction order fixed: fma(dz,dz, fma(dy,dy, dx*dx)).
 __device__ __forceinline__ float norm2(float dx, float dy, float dz) {
   return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));

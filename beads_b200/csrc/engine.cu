@@ -499,6 +499,7 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   v.mol = dalloc<uint32_t>(S);
   v.ref_pos = dalloc<float4>(S);
   v.ref_img = dalloc<int4>(S);
+  v.cross = dalloc<uint32_t>(S);
   v.pos2 = dalloc<float4>(S);
   v.vel2 = dalloc<float4>(S);
   v.img2 = dalloc<int4>(S);

@@ -76,32 +76,38 @@ k_pre(DeviceView v, float sd_dmax, float sd_fref, cudaGraphConditionalHandle con
         x.z = __fmaf_rn(s, f.z, x.z);
       }
     }
-    int4 im = v.img[slot];
-    bool crossed;
-    {
-      const float cx = floorf(__fmul_rn(__fsub_rn(x.x, p.lo[0]), p.inv_len[0]));
-      const float cy = floorf(__fmul_rn(__fsub_rn(x.y, p.lo[1]), p.inv_len[1]));
-      const float cz = floorf(__fmul_rn(__fsub_rn(x.z, p.lo[2]), p.inv_len[2]));
-      x.x = __fmaf_rn(-cx, p.len[0], x.x);
-      x.y = __fmaf_rn(-cy, p.len[1], x.y);
-      x.z = __fmaf_rn(-cz, p.len[2], x.z);
+    const float cx = floorf(__fmul_rn(__fsub_rn(x.x, p.lo[0]), p.inv_len[0]));
+    const float cy = floorf(__fmul_rn(__fsub_rn(x.y, p.lo[1]), p.inv_len[1]));
+    const float cz = floorf(__fmul_rn(__fsub_rn(x.z, p.lo[2]), p.inv_len[2]));
+    x.x = __fmaf_rn(-cx, p.len[0], x.x);
+    x.y = __fmaf_rn(-cy, p.len[1], x.y);
+    x.z = __fmaf_rn(-cz, p.len[2], x.z);
+    v.pos[slot] = x;
+    // Images and the crossing count change only on a boundary crossing, so
+    // a step reads neither image vector otherwise.
+    uint32_t cross = 0u;
+    const bool crossed = cx != 0.0f || cy != 0.0f || cz != 0.0f;
+    if (crossed) {
+      int4 im = v.img[slot];
       im.x += (int)cx;
       im.y += (int)cy;
       im.z += (int)cz;
-      crossed = cx != 0.0f || cy != 0.0f || cz != 0.0f;
+      v.img[slot] = im;
+      const uint32_t c0 = v.cross[slot];
+      cross = pack_cross(cross_field(c0, 0) + (int)cx, cross_field(c0, 1) + (int)cy,
+                         cross_field(c0, 2) + (int)cz) | (c0 & kCrossSaturated);
+      v.cross[slot] = cross;
     }
-    v.pos[slot] = x;
-    if (crossed) v.img[slot] = im;  // the image changes only on a boundary crossing
     if (check_step) {
       const float4 rx = v.ref_pos[slot];
-      const int4 ri = v.ref_img[slot];
-      const float dx = __fmaf_rn((float)((long long)im.x - (long long)ri.x),
-                                 p.len[0], __fsub_rn(x.x, rx.x));
-      const float dy = __fmaf_rn((float)((long long)im.y - (long long)ri.y),
-                                 p.len[1], __fsub_rn(x.y, rx.y));
-      const float dz = __fmaf_rn((float)((long long)im.z - (long long)ri.z),
-                                 p.len[2], __fsub_rn(x.z, rx.z));
-      if (norm2(dx, dy, dz) > p.disp_thr_sq) atomicExch(&st->exceeded, 1u);
+      if (!crossed) cross = v.cross[slot];
+      // (img - ref_img) L + (x - x_ref), the reference's displacement.
+      const float dx = __fmaf_rn((float)cross_field(cross, 0), p.len[0], __fsub_rn(x.x, rx.x));
+      const float dy = __fmaf_rn((float)cross_field(cross, 1), p.len[1], __fsub_rn(x.y, rx.y));
+      const float dz = __fmaf_rn((float)cross_field(cross, 2), p.len[2], __fsub_rn(x.z, rx.z));
+      if (norm2(dx, dy, dz) > p.disp_thr_sq || (cross & kCrossSaturated) != 0u) {
+        atomicExch(&st->exceeded, 1u);
+      }
     }
   }
 
@@ -578,6 +584,7 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
       v.nbr_count[i] = min(my_cnt, p.max_neighbors);
       v.ref_pos[i] = xi;
       v.ref_img[i] = v.img[i];
+      v.cross[i] = 0u;
     }
     any_overflow |= lane < nh && my_cnt > p.max_neighbors;
   }
