@@ -32,12 +32,11 @@ namespace {
 
 // ---------------------------------------------------------------------------
 // pre: Berendsen lambda of the previous step, half-kick, drift, wrap, image
-// update, displacement check; the last block of each replica decides the
-// rebuild for this step (neighbor_system.cpp:79-105).
+// update, displacement check; k_decide then takes the rebuild decision for
+// this step (neighbor_system.cpp:79-105).
 template <int kMode>
 __global__ void __launch_bounds__(kBlock)
-k_pre(DeviceView v, float sd_dmax, float sd_fref, cudaGraphConditionalHandle cond,
-      int use_cond) {
+k_pre(DeviceView v, float sd_dmax, float sd_fref) {
   const uint32_t b = blockIdx.x;
   const uint32_t r = v.block_replica[b];
   const ReplicaParams& p = v.rp[r];
@@ -106,40 +105,50 @@ k_pre(DeviceView v, float sd_dmax, float sd_fref, cudaGraphConditionalHandle con
       const float dy = __fmaf_rn((float)cross_field(cross, 1), p.len[1], __fsub_rn(x.y, rx.y));
       const float dz = __fmaf_rn((float)cross_field(cross, 2), p.len[2], __fsub_rn(x.z, rx.z));
       if (norm2(dx, dy, dz) > p.disp_thr_sq || (cross & kCrossSaturated) != 0u) {
-        atomicExch(&st->exceeded, 1u);
+        st->exceeded = 1u;  // every writer stores the same value
       }
     }
   }
+}
 
-  const uint32_t n_blocks = p.n_pad / kBlock;
-  if (arrive_last(&st->done_pre, n_blocks) && threadIdx.x == 0) {
-    const unsigned exceeded = atomicExch(&st->exceeded, 0u);
-    unsigned need = 0u;
-    if (kMode == kPreDescent || p.skin == 0.0f) {
-      need = (kMode == kPreDescent) ? exceeded : 1u;
-    } else if (check_step) {
-      const bool first = st->checks_since_build == 0u;
-      st->checks_since_build += 1u;
-      if (exceeded) {
-        need = 1u;
-        if (p.check_every > 1u && first) st->dangerous += 1ull;
-      }
+// pre, second part: one thread per replica takes the rebuild decision of
+// this step from the displacement flag k_pre's blocks set (a separate launch
+// instead of a last-block handshake: no fence and no same-address atomic in
+// each of k_pre's blocks).
+template <int kMode>
+__global__ void k_decide(DeviceView v, cudaGraphConditionalHandle cond, int use_cond) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= v.n_replicas) return;
+  const ReplicaParams& p = v.rp[r];
+  ReplicaState* st = &v.rs[r];
+  const unsigned long long phys = st->step + 1ull;
+  const bool check_step = (kMode == kPreDescent) || p.skin == 0.0f ||
+                          (phys % (unsigned long long)p.check_every) == 0ull;
+  const unsigned exceeded = st->exceeded;
+  st->exceeded = 0u;
+  unsigned need = 0u;
+  if (kMode == kPreDescent || p.skin == 0.0f) {
+    need = (kMode == kPreDescent) ? exceeded : 1u;
+  } else if (check_step) {
+    const bool first = st->checks_since_build == 0u;
+    st->checks_since_build += 1u;
+    if (exceeded) {
+      need = 1u;
+      if (p.check_every > 1u && first) st->dangerous += 1ull;
     }
-    if (need) {
-      st->builds += 1ull;
-      st->reorder_now =
-          (p.sort_every > 0u && (st->builds % p.sort_every) == 0ull) ? 1u : 0u;
-      st->checks_since_build = 0u;
-    } else {
-      st->reorder_now = 0u;
-    }
-    st->need_rebuild = need;
-    // Inside a captured step the rebuild chain is the body of a conditional
-    // graph node: any replica that rebuilds switches it on for this step.
-    if (need && use_cond) cudaGraphSetConditional(cond, 1u);
-    if (kMode == kPreVerlet) st->lambda = 1.0;
-    st->done_pre = 0u;
   }
+  if (need) {
+    st->builds += 1ull;
+    st->reorder_now = (p.sort_every > 0u && (st->builds % p.sort_every) == 0ull) ? 1u : 0u;
+    st->checks_since_build = 0u;
+  } else {
+    st->reorder_now = 0u;
+  }
+  st->need_rebuild = need;
+  // Inside a captured step the rebuild chain is the body of a conditional
+  // graph node: any replica that rebuilds switches it on for this step.
+  if (need && use_cond) cudaGraphSetConditional(cond, 1u);
+  if (kMode == kPreVerlet) st->lambda = 1.0;
 }
 
 // Marks every replica for a rebuild (initial build / explicit eval).
@@ -1347,14 +1356,17 @@ void check_launch(const char* what) {
 }  // namespace
 
 void launch_pre(const StepLaunch& l, int mode, cudaGraphConditionalHandle cond, bool use_cond) {
+  const uint32_t dg = (l.v.n_replicas + 127) / 128;
   if (mode == kPreDescent) {
-    k_pre<kPreDescent><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, l.sd_dmax, l.sd_fref, cond,
-                                                              use_cond ? 1 : 0);
+    k_pre<kPreDescent><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, l.sd_dmax, l.sd_fref);
+    check_launch("pre");
+    k_decide<kPreDescent><<<dg, 128, 0, l.stream>>>(l.v, cond, use_cond ? 1 : 0);
   } else {
-    k_pre<kPreVerlet><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, 0.f, 0.f, cond,
-                                                             use_cond ? 1 : 0);
+    k_pre<kPreVerlet><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, 0.f, 0.f);
+    check_launch("pre");
+    k_decide<kPreVerlet><<<dg, 128, 0, l.stream>>>(l.v, cond, use_cond ? 1 : 0);
   }
-  check_launch("pre");
+  check_launch("decide");
 }
 
 void launch_project_exclusions(const StepLaunch& l, bool force_all) {

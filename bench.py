@@ -362,11 +362,11 @@ def run_ours(args) -> None:
         st = eng.state()
         cpu = _cpu_baseline(st["positions"], spec, args.cpu_budget)
 
-    # Every step launches pre, the pair-force kernel, post (unless the
-    # schedule fuses the kick into the force kernel) and the per-replica
-    # finish kernel; a step that rebuilds also runs the 7 kernels of the
-    # rebuild chain (conditional graph node).
-    per_step = 3 if eng.tuning()["fuse_post"] else 4
+    # Every step launches pre, the per-replica rebuild decision, the
+    # pair-force kernel, post (unless the schedule fuses the kick into the
+    # force kernel) and the per-replica finish kernel; a step that rebuilds
+    # also runs the 7 kernels of the rebuild chain (conditional graph node).
+    per_step = 4 if eng.tuning()["fuse_post"] else 5
     gpu_launches = per_step * args.steps + 7 * int(timed_chains)
     line = {
         "metric": METRIC,
@@ -507,7 +507,7 @@ def run_replicas(args) -> None:
             "graph_warmup_steps": GRAPH_WARMUP,
             "schedule": schedule,
         },
-        "gpu_launches": (3 if schedule["fuse_post"] else 4) * args.steps + 7 * int(chains),
+        "gpu_launches": (4 if schedule["fuse_post"] else 5) * args.steps + 7 * int(chains),
         "clocks": clocks,
     }
     if rank == 0:
