@@ -878,11 +878,16 @@ struct CoeffRow {
     if (kNt == 1) return one;
     PairCoeff2 c;
     if (kNt == 2) {
-      const bool b0 = __float_as_int(w0) != 0, b1 = __float_as_int(w1) != 0;
-      c.sigma2 = make_float2(b0 ? r1.sigma2 : r0.sigma2, b1 ? r1.sigma2 : r0.sigma2);
-      c.eps24 = make_float2(b0 ? r1.eps24 : r0.eps24, b1 ? r1.eps24 : r0.eps24);
-      c.eps4 = make_float2(b0 ? r1.eps4 : r0.eps4, b1 ? r1.eps4 : r0.eps4);
-      c.neg_shift = make_float2(b0 ? -r1.shift : -r0.shift, b1 ? -r1.shift : -r0.shift);
+      // The neighbour's type t is 0 or 1, so bits(r0) + t (bits(r1) - bits(r0))
+      // picks the entry exactly, one integer multiply-add per value.
+      const int t0 = __float_as_int(w0), t1 = __float_as_int(w1);
+      auto pick = [](int t, float a, float b) {
+        return __int_as_float(__float_as_int(a) + t * (__float_as_int(b) - __float_as_int(a)));
+      };
+      c.sigma2 = make_float2(pick(t0, r0.sigma2, r1.sigma2), pick(t1, r0.sigma2, r1.sigma2));
+      c.eps24 = make_float2(pick(t0, r0.eps24, r1.eps24), pick(t1, r0.eps24, r1.eps24));
+      c.eps4 = make_float2(pick(t0, r0.eps4, r1.eps4), pick(t1, r0.eps4, r1.eps4));
+      c.neg_shift = make_float2(-pick(t0, r0.shift, r1.shift), -pick(t1, r0.shift, r1.shift));
       return c;
     }
     const LjCoeff c0 = row[__float_as_int(w0)];
