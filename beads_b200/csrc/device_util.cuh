@@ -123,6 +123,14 @@ __device__ __forceinline__ uint32_t pack_cross(int x, int y, int z) {
          ((static_cast<uint32_t>(z) & 0x3ffu) << 20) | (sat ? kCrossSaturated : 0u);
 }
 
+// Kernels launched as programmatic dependents (launch_dependent) start
+// while the previous kernel in the stream drains and wait here, before
+// their first read of its results, until it has completed and its writes
+// are visible.  Without that launch attribute this returns at once.
+__device__ __forceinline__ void wait_prior_grid() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // |d|^2 with the contraction order fixed: fma(dz,dz, fma(dy,dy, dx*dx)).
 __device__ __forceinline__ float norm2(float dx, float dy, float dz) {
   return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));

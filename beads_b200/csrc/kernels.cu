@@ -37,6 +37,7 @@ namespace {
 template <int kMode>
 __global__ void __launch_bounds__(kBlock)
 k_pre(DeviceView v, float sd_dmax, float sd_fref) {
+  wait_prior_grid();
   const uint32_t b = blockIdx.x;
   const uint32_t r = v.block_replica[b];
   const ReplicaParams& p = v.rp[r];
@@ -117,6 +118,7 @@ k_pre(DeviceView v, float sd_dmax, float sd_fref) {
 // each of k_pre's blocks).
 template <int kMode>
 __global__ void k_decide(DeviceView v, cudaGraphConditionalHandle cond, int use_cond) {
+  wait_prior_grid();
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= v.n_replicas) return;
   const ReplicaParams& p = v.rp[r];
@@ -721,6 +723,7 @@ static_assert(kKeBuckets <= (uint32_t)kFinishThreads, "one finish thread per buc
 
 template <bool kKick, bool kObs, bool kKinetic>
 __global__ void __launch_bounds__(kFinishThreads) k_post_finish(DeviceView v) {
+  wait_prior_grid();
   const uint32_t r = blockIdx.x;
   const ReplicaParams& p = v.rp[r];
   ReplicaState* st = &v.rs[r];
@@ -1277,6 +1280,7 @@ __global__ void __launch_bounds__(kBlock) k_bonded(DeviceView v) {
 
 template <bool kKick, bool kObs, bool kKinetic>
 __global__ void __launch_bounds__(kBlock) k_post(DeviceView v) {
+  wait_prior_grid();
   const uint32_t b = blockIdx.x;
   const uint32_t r = v.block_replica[b];
   const ReplicaParams& p = v.rp[r];
@@ -1358,18 +1362,45 @@ void check_launch(const char* what) {
   }
 }
 
+// Launches a kernel as a programmatic dependent of the previous work in the
+// stream (also inside a stream capture): its blocks may be scheduled while
+// that work drains, hiding the launch gap, and wait in wait_prior_grid()
+// before touching its results.  Used for the short per-step kernels that
+// follow another kernel directly.
+template <typename... P, typename... A>
+void launch_dependent(void (*kernel)(P...), dim3 grid, dim3 block, cudaStream_t stream,
+                      const char* what, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+  if (e != cudaSuccess) {
+    throw std::runtime_error(std::string("CUDA launch of ") + what +
+                             " failed: " + cudaGetErrorString(e));
+  }
+}
+
 }  // namespace
 
 void launch_pre(const StepLaunch& l, int mode, cudaGraphConditionalHandle cond, bool use_cond) {
   const uint32_t dg = (l.v.n_replicas + 127) / 128;
   if (mode == kPreDescent) {
-    k_pre<kPreDescent><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, l.sd_dmax, l.sd_fref);
-    check_launch("pre");
-    k_decide<kPreDescent><<<dg, 128, 0, l.stream>>>(l.v, cond, use_cond ? 1 : 0);
+    launch_dependent(k_pre<kPreDescent>, dim3(l.v.n_blocks), dim3(kBlock), l.stream, "pre", l.v,
+                     l.sd_dmax, l.sd_fref);
+    launch_dependent(k_decide<kPreDescent>, dim3(dg), dim3(128), l.stream, "decide", l.v, cond,
+                     use_cond ? 1 : 0);
   } else {
-    k_pre<kPreVerlet><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, 0.f, 0.f);
-    check_launch("pre");
-    k_decide<kPreVerlet><<<dg, 128, 0, l.stream>>>(l.v, cond, use_cond ? 1 : 0);
+    launch_dependent(k_pre<kPreVerlet>, dim3(l.v.n_blocks), dim3(kBlock), l.stream, "pre", l.v,
+                     0.f, 0.f);
+    launch_dependent(k_decide<kPreVerlet>, dim3(dg), dim3(128), l.stream, "decide", l.v, cond,
+                     use_cond ? 1 : 0);
   }
   check_launch("decide");
 }
@@ -1495,12 +1526,13 @@ void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post)
   }
   if (fuse) {
     const bool kin = fin == kForcePostKinetic || observables;
+    const dim3 fg(l.v.n_replicas), ft(kFinishThreads);
     if (observables) {
-      k_post_finish<true, true, true><<<l.v.n_replicas, kFinishThreads, 0, l.stream>>>(l.v);
+      launch_dependent(k_post_finish<true, true, true>, fg, ft, l.stream, "post finish", l.v);
     } else if (kin) {
-      k_post_finish<true, false, true><<<l.v.n_replicas, kFinishThreads, 0, l.stream>>>(l.v);
+      launch_dependent(k_post_finish<true, false, true>, fg, ft, l.stream, "post finish", l.v);
     } else {
-      k_post_finish<true, false, false><<<l.v.n_replicas, kFinishThreads, 0, l.stream>>>(l.v);
+      launch_dependent(k_post_finish<true, false, false>, fg, ft, l.stream, "post finish", l.v);
     }
     check_launch("post finish");
   }
@@ -1512,18 +1544,26 @@ void launch_post(const StepLaunch& l, bool kick, bool observables) {
   const dim3 fg(l.v.n_replicas);
   if (kick) {
     if (observables) {
-      k_post<true, true, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
-      k_post_finish<true, true, true><<<fg, kFinishThreads, 0, l.stream>>>(l.v);
+      launch_dependent(k_post<true, true, true>, dim3(l.v.n_blocks), dim3(kBlock), l.stream,
+                       "post", l.v);
+      launch_dependent(k_post_finish<true, true, true>, dim3(fg), dim3(kFinishThreads), l.stream,
+                       "post finish", l.v);
     } else if (kin) {
-      k_post<true, false, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
-      k_post_finish<true, false, true><<<fg, kFinishThreads, 0, l.stream>>>(l.v);
+      launch_dependent(k_post<true, false, true>, dim3(l.v.n_blocks), dim3(kBlock), l.stream,
+                       "post", l.v);
+      launch_dependent(k_post_finish<true, false, true>, dim3(fg), dim3(kFinishThreads), l.stream,
+                       "post finish", l.v);
     } else {
-      k_post<true, false, false><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
-      k_post_finish<true, false, false><<<fg, kFinishThreads, 0, l.stream>>>(l.v);
+      launch_dependent(k_post<true, false, false>, dim3(l.v.n_blocks), dim3(kBlock), l.stream,
+                       "post", l.v);
+      launch_dependent(k_post_finish<true, false, false>, dim3(fg), dim3(kFinishThreads), l.stream,
+                       "post finish", l.v);
     }
   } else {
-    k_post<false, true, true><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
-    k_post_finish<false, true, true><<<fg, kFinishThreads, 0, l.stream>>>(l.v);
+    launch_dependent(k_post<false, true, true>, dim3(l.v.n_blocks), dim3(kBlock), l.stream,
+                     "post", l.v);
+    launch_dependent(k_post_finish<false, true, true>, dim3(fg), dim3(kFinishThreads), l.stream,
+                     "post finish", l.v);
   }
   check_launch("post");
 }
