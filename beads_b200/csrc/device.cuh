@@ -152,6 +152,8 @@ struct DeviceView {
   float4* ref_pos;
   int4* ref_img;
   uint32_t* cross;  // net boundary crossings since the last build (see pack_cross)
+  uint32_t* work_start;  // [n_replicas + 1] first work item (cell) of each rebuilding
+                         // replica, then the total
   // reorder scratch
   float4* pos2;
   float4* vel2;

@@ -500,6 +500,7 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   v.ref_pos = dalloc<float4>(S);
   v.ref_img = dalloc<int4>(S);
   v.cross = dalloc<uint32_t>(S);
+  v.work_start = dalloc<uint32_t>(n + 1);
   v.pos2 = dalloc<float4>(S);
   v.vel2 = dalloc<float4>(S);
   v.img2 = dalloc<int4>(S);

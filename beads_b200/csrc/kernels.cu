@@ -199,10 +199,40 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanWarps = kScanThreads / 32;
 __global__ void __launch_bounds__(kScanThreads) k_scan(DeviceView v) {
   const uint32_t r = blockIdx.x;
-  if (!v.rs[r].need_rebuild) return;
-  const ReplicaParams& p = v.rp[r];
   __shared__ uint32_t warp_base[kScanWarps];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  {
+    // Work list of the per-cell kernels (cell sort, list build): work item
+    // w is cell w - work_start[q] of the rebuilding replica q with
+    // work_start[q] <= w < work_start[q + 1].  Every block writes its own
+    // entry (the cells of the rebuilding replicas before it), block 0 also
+    // the total.
+    uint32_t before = 0, all = 0;
+    for (uint32_t q = threadIdx.x; q < v.n_replicas; q += kScanThreads) {
+      const uint32_t c = v.rs[q].need_rebuild ? v.rp[q].n_cells : 0u;
+      all += c;
+      before += q < r ? c : 0u;
+    }
+    before = __reduce_add_sync(kFull, before);
+    all = __reduce_add_sync(kFull, all);
+    __shared__ uint32_t part[2][kScanWarps];
+    if (lane == 0) {
+      part[0][warp] = before;
+      part[1][warp] = all;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t sb = 0, sa = 0;
+      for (int w = 0; w < kScanWarps; ++w) {
+        sb += part[0][w];
+        sa += part[1][w];
+      }
+      v.work_start[r] = sb;
+      if (r == 0) v.work_start[v.n_replicas] = sa;
+    }
+  }
+  if (!v.rs[r].need_rebuild) return;
+  const ReplicaParams& p = v.rp[r];
   const uint32_t n = p.n_cells;
   const uint32_t per = ((n + kScanWarps - 1) / kScanWarps + 31u) & ~31u;
   const uint32_t begin = min(n, warp * per);
@@ -260,21 +290,32 @@ __global__ void __launch_bounds__(kBlock) k_scatter(DeviceView v) {
   v.cell_atoms[at] = slot;
 }
 
+// The replica of work item w (see k_scan); w is warp-uniform.
+__device__ __forceinline__ uint32_t work_replica(const DeviceView& v, uint32_t w) {
+  uint32_t lo = 0, hi = v.n_replicas;  // work_start[lo] <= w < work_start[hi]
+  while (hi - lo > 1u) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (v.work_start[mid] <= w) {
+      lo = mid;
+    } else {
+      hi = mid;
+    }
+  }
+  return lo;
+}
+
 // rebuild 4: sort each cell's slots ascending, which makes the counting sort
 // stable and the whole build deterministic.  One warp per cell; a bitonic
-// network in registers for <= 32 members, insertion sort otherwise.  Also
+// network in registers for <= 32 members, a rank sort in shared memory up to
+// 256, insertion sort beyond.  Also
 // gathers the positions in cell order (pos2[q] = pos[cell_atoms[q]]), so the
 // list build reads its candidates with contiguous loads that do not wait on
 // the slot index; the reorder kernels find them there too.
-__global__ void __launch_bounds__(kBlock) k_cellsort(DeviceView v) {
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t g = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);  // global cell
-  if (g >= v.total_cells) return;                                     // warp-uniform
-  const uint32_t r = v.cell_replica[g];
-  if (!v.rs[r].need_rebuild) return;
-  const ReplicaParams& p = v.rp[r];
+constexpr uint32_t kSortRankMax = 256;  // cells up to this size: rank sort in shared memory
+// Sorts cell c of replica p (one warp; keys: this warp's shared scratch).
+__device__ __forceinline__ void sort_cell(const DeviceView& v, const ReplicaParams& p,
+                                          uint32_t c, uint32_t lane, uint32_t* keys) {
   {
-    const uint32_t c = g - p.cell_begin;
     const uint32_t s0 = v.cell_start[p.start_base + c];
     const uint32_t s1 = v.cell_start[p.start_base + c + 1];
     const uint32_t n = s1 - s0;
@@ -294,6 +335,18 @@ __global__ void __launch_bounds__(kBlock) k_cellsort(DeviceView v) {
         v.cell_atoms[s0 + lane] = val;
         v.pos2[s0 + lane] = v.pos[val];
       }
+    } else if (n <= kSortRankMax) {
+      // Rank sort in shared memory: the slots are distinct, so a slot's
+      // place is the number of smaller slots in the cell.
+      for (uint32_t q = lane; q < n; q += 32u) keys[q] = v.cell_atoms[s0 + q];
+      __syncwarp();
+      for (uint32_t q = lane; q < n; q += 32u) {
+        const uint32_t key = keys[q];
+        uint32_t rank = 0;
+        for (uint32_t t = 0; t < n; ++t) rank += keys[t] < key ? 1u : 0u;
+        v.cell_atoms[s0 + rank] = key;
+        v.pos2[s0 + rank] = v.pos[key];
+      }
     } else {
       if (lane == 0) {
         for (uint32_t a = s0 + 1; a < s1; ++a) {
@@ -310,6 +363,17 @@ __global__ void __launch_bounds__(kBlock) k_cellsort(DeviceView v) {
       for (uint32_t q = s0 + lane; q < s1; q += 32u) v.pos2[q] = v.pos[v.cell_atoms[q]];
     }
   }
+}
+
+// Warp w sorts work item w (k_scan): the warps past the cells of the
+// rebuilding replicas return after one load.
+__global__ void __launch_bounds__(kBlock) k_cellsort(DeviceView v) {
+  __shared__ uint32_t sort_keys[kBlock / 32][kSortRankMax];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t w = blockIdx.x * (kBlock / 32) + warp;
+  if (w >= v.work_start[v.n_replicas]) return;  // warp-uniform
+  const uint32_t r = work_replica(v, w);
+  sort_cell(v, v.rp[r], w - v.work_start[r], lane, sort_keys[warp]);
 }
 
 // rebuild 5/6: physical reorder into cell order (every sort_every builds).
@@ -602,17 +666,17 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
   if (__any_sync(kFull, any_overflow) && lane == 0) atomicOr(&st->status, kStatusNeighborOverflow);
 }
 
-// One warp per global cell of any replica.
+// Warp w builds the lists of work item w (k_scan): the warps past the cells
+// of the rebuilding replicas return after one load.
 template <int kCap>
 __global__ void __launch_bounds__(kBlock, 8) k_build(DeviceView v) {
   __shared__ BuildShared sh[kBuildWarps];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t g = blockIdx.x * kBuildWarps + warp;  // global cell
-  if (g >= v.total_cells) return;                      // warp-uniform exits
-  const uint32_t r = v.cell_replica[g];
-  ReplicaState* st = &v.rs[r];
-  if (!st->need_rebuild) return;
-  build_cell<kCap>(v, v.rp[r], st, g, lane, sh[warp]);
+  const uint32_t w = blockIdx.x * kBuildWarps + warp;
+  if (w >= v.work_start[v.n_replicas]) return;  // warp-uniform
+  const uint32_t r = work_replica(v, w);
+  const ReplicaParams& p = v.rp[r];
+  build_cell<kCap>(v, p, &v.rs[r], p.cell_begin + (w - v.work_start[r]), lane, sh[warp]);
 }
 
 // ---------------------------------------------------------------------------
