@@ -471,47 +471,63 @@ struct BuildShared {
 
 enum BuildForm : int { kBuildInterior = 0, kBuildShifted = 1, kBuildMinImage = 2 };
 
+// Candidates of one lane in a chunk: kBuildPairs pairs, pair q holding
+// stream positions base + 64 q + lane (.x) and base + 64 q + 32 + lane (.y).
+struct CandPair {
+  uint32_t jx, jy;       // slots (0xffffffff past the stream)
+  float2 nx, ny, nz;     // minus their coordinates
+  float2 sx, sy, sz;     // periodic shifts of their segments
+};
+constexpr int kBuildPairs = 2;
+constexpr uint32_t kChunk = 64u * kBuildPairs;  // candidates per chunk
+
 // Tests one chunk of candidates against the home particles [0, nh) and
 // appends the accepted ones.  my_cnt: lane h holds home particle h's count.
 template <int kCap, int kForm>
 __device__ __forceinline__ void build_chunk(const DeviceView& v, const ReplicaParams& p,
                                             const BuildShared& sh, uint32_t nh, uint32_t lane,
-                                            uint32_t jx, uint32_t jy, float2 nxj, float2 nyj,
-                                            float2 nzj, float2 s2x, float2 s2y, float2 s2z,
+                                            const CandPair (&c)[kBuildPairs],
                                             uint32_t& my_cnt) {
   const float cut = p.search_cut_sq;
   const uint32_t cap = p.max_neighbors;
   const uint32_t lt = (1u << lane) - 1u;
-#pragma unroll 2
+#pragma unroll 1
   for (uint32_t h = 0; h < nh; ++h) {
     const float4 ha = sh.home_a[h];
     const float4 hb = sh.home_b[h];
     const uint32_t i = __float_as_uint(hb.z);
-    float2 dx, dy, dz;
-    if (kForm == kBuildMinImage) {
-      dx = make_float2(ref_delta(ha.x, -nxj.x, p.len[0], p.half[0]),
-                       ref_delta(ha.x, -nxj.y, p.len[0], p.half[0]));
-      dy = make_float2(ref_delta(ha.z, -nyj.x, p.len[1], p.half[1]),
-                       ref_delta(ha.z, -nyj.y, p.len[1], p.half[1]));
-      dz = make_float2(ref_delta(hb.x, -nzj.x, p.len[2], p.half[2]),
-                       ref_delta(hb.x, -nzj.y, p.len[2], p.half[2]));
-    } else {
-      // fl(xi + (-xj)) is fl(xi - xj); a zero shift leaves it unchanged.
-      dx = __fadd2_rn(make_float2(ha.x, ha.y), nxj);
-      dy = __fadd2_rn(make_float2(ha.z, ha.w), nyj);
-      dz = __fadd2_rn(make_float2(hb.x, hb.y), nzj);
-      if (kForm == kBuildShifted) {
-        dx = __fadd2_rn(dx, s2x);
-        dy = __fadd2_rn(dy, s2y);
-        dz = __fadd2_rn(dz, s2z);
+    bool ax[kBuildPairs], ay[kBuildPairs];
+    uint32_t bx[kBuildPairs], by[kBuildPairs];
+    uint32_t any = 0u;
+#pragma unroll
+    for (int q = 0; q < kBuildPairs; ++q) {
+      float2 dx, dy, dz;
+      if (kForm == kBuildMinImage) {
+        dx = make_float2(ref_delta(ha.x, -c[q].nx.x, p.len[0], p.half[0]),
+                         ref_delta(ha.x, -c[q].nx.y, p.len[0], p.half[0]));
+        dy = make_float2(ref_delta(ha.z, -c[q].ny.x, p.len[1], p.half[1]),
+                         ref_delta(ha.z, -c[q].ny.y, p.len[1], p.half[1]));
+        dz = make_float2(ref_delta(hb.x, -c[q].nz.x, p.len[2], p.half[2]),
+                         ref_delta(hb.x, -c[q].nz.y, p.len[2], p.half[2]));
+      } else {
+        // fl(xi + (-xj)) is fl(xi - xj); a zero shift leaves it unchanged.
+        dx = __fadd2_rn(make_float2(ha.x, ha.y), c[q].nx);
+        dy = __fadd2_rn(make_float2(ha.z, ha.w), c[q].ny);
+        dz = __fadd2_rn(make_float2(hb.x, hb.y), c[q].nz);
+        if (kForm == kBuildShifted) {
+          dx = __fadd2_rn(dx, c[q].sx);
+          dy = __fadd2_rn(dy, c[q].sy);
+          dz = __fadd2_rn(dz, c[q].sz);
+        }
       }
+      const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+      ax[q] = !(r2.x > cut) && c[q].jx != i;
+      ay[q] = !(r2.y > cut) && c[q].jy != i;
+      bx[q] = __ballot_sync(kFull, ax[q]);
+      by[q] = __ballot_sync(kFull, ay[q]);
+      any |= bx[q] | by[q];
     }
-    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-    bool ax = !(r2.x > cut) && jx != i;
-    bool ay = !(r2.y > cut) && jy != i;
-    uint32_t bx = __ballot_sync(kFull, ax);
-    uint32_t by = __ballot_sync(kFull, ay);
-    if ((bx | by) == 0u) continue;  // warp-uniform
+    if (any == 0u) continue;  // warp-uniform
     if (kCap > 0) {
       // Exclusion rows are padded with 0xffffffff after the last partner.
       const uint32_t* ex = v.excl_slot + (size_t)i * v.excl_cap;
@@ -519,20 +535,30 @@ __device__ __forceinline__ void build_chunk(const DeviceView& v, const ReplicaPa
       for (int e = 0; e < kCap; ++e) {
         const uint32_t xe = __ldg(ex + e);
         if (xe == 0xffffffffu) break;  // warp-uniform
-        ax = ax && jx != xe;
-        ay = ay && jy != xe;
+#pragma unroll
+        for (int q = 0; q < kBuildPairs; ++q) {
+          ax[q] = ax[q] && c[q].jx != xe;
+          ay[q] = ay[q] && c[q].jy != xe;
+        }
       }
-      bx = __ballot_sync(kFull, ax);
-      by = __ballot_sync(kFull, ay);
+#pragma unroll
+      for (int q = 0; q < kBuildPairs; ++q) {
+        bx[q] = __ballot_sync(kFull, ax[q]);
+        by[q] = __ballot_sync(kFull, ay[q]);
+      }
     }
-    const uint32_t cnt = __shfl_sync(kFull, my_cnt, h);
-    const uint32_t nx = __popc(bx);
-    const uint32_t kx = cnt + __popc(bx & lt);
-    const uint32_t ky = cnt + nx + __popc(by & lt);
+    uint32_t k = __shfl_sync(kFull, my_cnt, h);
     uint32_t* row = v.nbr + nbr_index(i, 0, v.nbr_stride);
-    if (ax && kx < cap) row[(size_t)kx * kGroup] = jx;
-    if (ay && ky < cap) row[(size_t)ky * kGroup] = jy;
-    if (lane == h) my_cnt = cnt + nx + __popc(by);
+#pragma unroll
+    for (int q = 0; q < kBuildPairs; ++q) {
+      const uint32_t kx = k + __popc(bx[q] & lt);
+      k += __popc(bx[q]);
+      const uint32_t ky = k + __popc(by[q] & lt);
+      k += __popc(by[q]);
+      if (ax[q] && kx < cap) row[(size_t)kx * kGroup] = c[q].jx;
+      if (ay[q] && ky < cap) row[(size_t)ky * kGroup] = c[q].jy;
+    }
+    if (lane == h) my_cnt = k;
   }
 }
 
@@ -620,39 +646,39 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
     }
     __syncwarp();
     uint32_t my_cnt = 0u;
-    uint32_t sa = 0u, sb = 0u;  // segment of this lane's two candidates
-    for (uint32_t base = 0; base < total; base += 64u) {
-      const uint32_t ua = base + lane, ub = base + 32u + lane;
-      while (sa < nseg && ua >= sh.seg_end[sa]) ++sa;
-      while (sb < nseg && ub >= sh.seg_end[sb]) ++sb;
-      // Past the stream: an infinite coordinate fails every distance test.
-      uint32_t jx = 0xffffffffu, jy = 0xffffffffu;
-      float4 xa = make_float4(INFINITY, 0.f, 0.f, 0.f), xb = xa;
-      if (ua < total) {
-        jx = v.cell_atoms[sh.seg_q[sa] + ua];
-        xa = v.pos2[sh.seg_q[sa] + ua];
+    uint32_t seg[2 * kBuildPairs] = {};  // segment walk of this lane's stream positions
+    for (uint32_t base = 0; base < total; base += kChunk) {
+      CandPair c[kBuildPairs];
+#pragma unroll
+      for (int t = 0; t < 2 * kBuildPairs; ++t) {
+        const uint32_t u = base + 32u * t + lane;
+        while (seg[t] < nseg && u >= sh.seg_end[seg[t]]) ++seg[t];
+        // Past the stream: an infinite coordinate fails every distance test.
+        uint32_t j = 0xffffffffu;
+        float4 x = make_float4(INFINITY, 0.f, 0.f, 0.f);
+        if (u < total) {
+          j = v.cell_atoms[sh.seg_q[seg[t]] + u];
+          x = v.pos2[sh.seg_q[seg[t]] + u];
+        }
+        const uint32_t st = min(seg[t], kMaxSegments - 1u);
+        const float sx = form == kBuildShifted ? sh.seg_s[0][st] : 0.f;
+        const float sy = form == kBuildShifted ? sh.seg_s[1][st] : 0.f;
+        const float sz = form == kBuildShifted ? sh.seg_s[2][st] : 0.f;
+        CandPair& cp = c[t >> 1];
+        if ((t & 1) == 0) {
+          cp.jx = j, cp.nx.x = -x.x, cp.ny.x = -x.y, cp.nz.x = -x.z;
+          cp.sx.x = sx, cp.sy.x = sy, cp.sz.x = sz;
+        } else {
+          cp.jy = j, cp.nx.y = -x.x, cp.ny.y = -x.y, cp.nz.y = -x.z;
+          cp.sx.y = sx, cp.sy.y = sy, cp.sz.y = sz;
+        }
       }
-      if (ub < total) {
-        jy = v.cell_atoms[sh.seg_q[sb] + ub];
-        xb = v.pos2[sh.seg_q[sb] + ub];
-      }
-      const float2 nxj = make_float2(-xa.x, -xb.x), nyj = make_float2(-xa.y, -xb.y),
-                   nzj = make_float2(-xa.z, -xb.z);
       if (form == kBuildInterior) {
-        const float2 z = make_float2(0.f, 0.f);
-        build_chunk<kCap, kBuildInterior>(v, p, sh, nh, lane, jx, jy, nxj, nyj, nzj, z, z, z,
-                                          my_cnt);
+        build_chunk<kCap, kBuildInterior>(v, p, sh, nh, lane, c, my_cnt);
       } else if (form == kBuildShifted) {
-        const uint32_t ta = min(sa, kMaxSegments - 1u), tb = min(sb, kMaxSegments - 1u);
-        build_chunk<kCap, kBuildShifted>(
-            v, p, sh, nh, lane, jx, jy, nxj, nyj, nzj,
-            make_float2(sh.seg_s[0][ta], sh.seg_s[0][tb]),
-            make_float2(sh.seg_s[1][ta], sh.seg_s[1][tb]),
-            make_float2(sh.seg_s[2][ta], sh.seg_s[2][tb]), my_cnt);
+        build_chunk<kCap, kBuildShifted>(v, p, sh, nh, lane, c, my_cnt);
       } else {
-        const float2 z = make_float2(0.f, 0.f);
-        build_chunk<kCap, kBuildMinImage>(v, p, sh, nh, lane, jx, jy, nxj, nyj, nzj, z, z, z,
-                                          my_cnt);
+        build_chunk<kCap, kBuildMinImage>(v, p, sh, nh, lane, c, my_cnt);
       }
     }
     if (lane < nh) {
@@ -669,7 +695,7 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
 // Warp w builds the lists of work item w (k_scan): the warps past the cells
 // of the rebuilding replicas return after one load.
 template <int kCap>
-__global__ void __launch_bounds__(kBlock, 8) k_build(DeviceView v) {
+__global__ void __launch_bounds__(kBlock, 6) k_build(DeviceView v) {
   __shared__ BuildShared sh[kBuildWarps];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t w = blockIdx.x * kBuildWarps + warp;
