@@ -213,3 +213,35 @@ def test_exclusions_remove_bonded_pairs():
             for u in (t - d, t + d):
                 if 1 <= u <= spec.n and (u - 1) // beads == chain0:
                     assert u not in row
+
+
+@pytest.mark.parametrize("density", [3.0, 10.0])
+def test_crowded_cells_sort_and_list(oracle, density):
+    """Cells far above a warp's 32 slots: ~90 per cell goes through the
+    shared-memory rank sort, ~300 through the insertion sort.  The lists
+    must equal the oracle's sets, and a second build of the same state must
+    give the same entries in the same order."""
+    rng = np.random.default_rng(int(density))
+    lens = np.array([6.2, 6.2, 6.2])
+    n = int(density * lens.prod())
+    side = int(np.ceil(n ** (1 / 3)))
+    a = 6.2 / side
+    g = np.indices((side,) * 3).reshape(3, -1).T[rng.permutation(side ** 3)[:n]]
+    # A jittered lattice: crowded cells without overlapping pairs.
+    pos = (g + 0.5 + rng.uniform(-0.1, 0.1, g.shape)) * a
+    spec = workloads.lj_lattice()
+    spec.positions = pos.astype(np.float32)
+    spec.types = np.ones(n, np.int32)
+    spec.velocities = np.zeros((n, 3), np.float32)
+    spec.masses = np.ones(n, np.float32)
+    spec.box_bound = np.array([[0, 0, 0], lens], np.float32)
+    spec.max_neighbors = 1024
+    with Engine(spec) as eng:
+        eng.eval()
+        counts, partners = eng.debug_neighbors()
+        eng.eval()
+        counts2, partners2 = eng.debug_neighbors()
+    ocounts, opartners = oracle_neighbors(spec)
+    assert np.array_equal(counts, ocounts)
+    assert neighbor_sets(counts, partners) == neighbor_sets(ocounts, opartners + 1)
+    assert np.array_equal(counts, counts2) and np.array_equal(partners, partners2)
