@@ -440,10 +440,11 @@ k_project_exclusions(DeviceView v, int force_all) {
 // One warp per cell, the candidates on the lanes.  The stencil of the cell is
 // a list of segments (contiguous runs of cell_atoms) in the reference's
 // stencil order (z, y, x cells; ascending slot inside a cell); their
-// concatenation is the candidate stream, walked 64 candidates at a time:
-// lane l holds candidates l and 32 + l of a chunk, both tested against one
-// home particle per iteration on the packed FP32x2 pipe.  Two ballots give
-// the accepted candidates in stream order; each accepted lane writes its
+// concatenation is the candidate stream, walked kChunk (128) candidates at
+// a time: lane l holds candidates l, 32 + l, 64 + l and 96 + l of a chunk
+// as two packed pairs, all tested against one home particle per iteration
+// on the packed FP32x2 pipe.  Four ballots give the accepted candidates in
+// stream order; each accepted lane writes its
 // entry at the home particle's count plus its rank among the accepted, so a
 // particle's list order is the stream order under any schedule.  Every lane
 // does useful work whatever the cell occupancy, and appends never diverge.
@@ -1362,8 +1363,8 @@ __global__ void __launch_bounds__(kBlock) k_bonded(DeviceView v) {
 }
 
 // ---------------------------------------------------------------------------
-// post: second half-kick and kinetic energy (FP64 per slot, fixed-point
-// partial per block); k_post_finish then does the per-replica epilogue
+// post: second half-kick and kinetic energy (FP64 per slot, one fixed-point
+// bucket add per block); k_post_finish then does the per-replica epilogue
 // (observables, Berendsen lambda for the next step, applied lazily by pre,
 // step counter).  The same per-slot work runs inside the last force kernel
 // when the schedule fuses the kick.
