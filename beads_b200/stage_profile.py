@@ -1,0 +1,63 @@
+"""Times one stage of the step on a named workload, for profilers.
+
+    python -m beads_b200.stage_profile --workload fit-mixture --beads 524288 \
+        --stage rebuild --reps 1
+
+Builds the workload, runs ``--warm`` MD steps, then calls
+``Engine.profile(stage, reps)`` between cudaProfilerStart and
+cudaProfilerStop, so a profiler started with ``--profile-from-start off``
+sees exactly those launches.  Prints the mean milliseconds per launch.
+Stages: forces, forces_kick, rebuild, step (see ``Engine.profile``).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+
+
+def _workload(name: str, beads: int):
+    from beads_b200 import workloads
+
+    if name == "fit-mixture":
+        return workloads.fit_mixture(n_replicas=1, n=beads, seed=3, max_neighbors=192)[0]
+    if name == "lattice":
+        side = round(beads ** (1.0 / 3.0))
+        return workloads.lj_lattice(n_side=side)
+    if name == "replicas":
+        return workloads.replica_batch(512)
+    raise ValueError(f"unknown workload {name!r}")
+
+
+def main(argv: list[str] | None = None) -> dict:
+    parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    parser.add_argument("--workload", default="fit-mixture",
+                        choices=["fit-mixture", "lattice", "replicas"])
+    parser.add_argument("--beads", type=int, default=524288)
+    parser.add_argument("--stage", default="rebuild",
+                        choices=["forces", "forces_kick", "rebuild", "step"])
+    parser.add_argument("--reps", type=int, default=1)
+    parser.add_argument("--warm", type=int, default=20)
+    parser.add_argument("--schedule", default="2,0,4,1",
+                        help="threads per particle, fused kick, depth, list bypass L1")
+    args = parser.parse_args(argv)
+
+    import torch
+
+    from beads_b200.engine import Engine
+
+    tpa, fuse, depth, bypass = (int(x) for x in args.schedule.split(","))
+    with Engine(_workload(args.workload, args.beads)) as eng:
+        eng.set_tuning(tpa, bool(fuse), depth, bool(bypass))
+        eng.run(args.warm)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        ms = eng.profile(args.stage, args.reps)
+        torch.cuda.profiler.stop()
+    out = {"workload": args.workload, "stage": args.stage, "reps": args.reps, "ms": ms}
+    print(json.dumps(out))
+    return out
+
+
+if __name__ == "__main__":
+    main()
