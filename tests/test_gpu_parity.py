@@ -245,3 +245,18 @@ def test_crowded_cells_sort_and_list(oracle, density):
     assert np.array_equal(counts, ocounts)
     assert neighbor_sets(counts, partners) == neighbor_sets(ocounts, opartners + 1)
     assert np.array_equal(counts, counts2) and np.array_equal(partners, partners2)
+
+
+@pytest.mark.parametrize("distance", [1, 3])
+def test_exclusion_distances_match_oracle(oracle, distance):
+    """Bond-graph exclusions at distance 1 (one partner row entry per bond)
+    and 3 (up to six partners along a chain): the list build's exclusion
+    check against the oracle's neighbour sets."""
+    spec = workloads.polymer_melt(n_chains=40, beads=50, seed=3, max_neighbors=96,
+                                  exclusion_distance=distance)
+    with Engine(spec) as eng:
+        eng.eval()
+        counts, partners = eng.debug_neighbors()
+    ocounts, opartners = oracle_neighbors(spec)
+    assert np.array_equal(counts, ocounts)
+    assert neighbor_sets(counts, partners) == neighbor_sets(ocounts, opartners + 1)
