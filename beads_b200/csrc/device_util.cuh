@@ -67,7 +67,7 @@ __device__ __forceinline__ void block_add_lane(bool real, double v, ReplicaState
                             &st->acc_frac[lane]);
 }
 
-// Reads and clears one fixed-point total (last block of a replica only).
+// Reads and clears one fixed-point total (one thread of the replica's finish block).
 __device__ __forceinline__ double take_total(ReplicaState* st, int lane) {
   unsigned long long* w = reinterpret_cast<unsigned long long*>(st->acc);
   unsigned long long* f = reinterpret_cast<unsigned long long*>(st->acc_frac);
