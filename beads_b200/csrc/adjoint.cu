@@ -241,6 +241,8 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
   float te[kNt], ts[kNt];
 #pragma unroll
   for (int c = 0; c < kNt; ++c) te[c] = ts[c] = 0.f;
+  float sa[2] = {0.f, 0.f}, sb[2] = {0.f, 0.f}, sc[2] = {0.f, 0.f}, sd[2] = {0.f, 0.f},
+        sn[2] = {0.f, 0.f};
   const float4 xi = pos[i];
   const int ti = __float_as_int(xi.w);
   const AdjCoeff* row = table + ti * kNt;
@@ -304,14 +306,44 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
       // Parameter adjoints of this ordered pair (the pair's PE and W are
       // split half and half between its two ordered entries).
       const float fd = fi.x * dx + fi.y * dy + fi.z * dz;
-      const float uu = c.eps4 * (sr12 - sr6) - c.shift;
-      const float d_eps = (phi * fd + h_pe * uu + h_w * phi * rr) * c.inv_eps;
-      const float qq = 24.0f * sr12 - 6.0f * sr6;
-      const float dphi = c.eps24 * inv * qq * c.inv_sig;
-      const float du = c.eps4 * (12.0f * sr12 - 6.0f * sr6) * c.inv_sig - c.dshift;
-      const float d_sig = dphi * fd + h_pe * du + h_w * dphi * rr;
-      add_typed<kNt>(te, tj, in ? d_eps : 0.0f);
-      add_typed<kNt>(ts, tj, in ? d_sig : 0.0f);
+      if constexpr (kNt == 2) {
+        // Five per-type sums; the per-type-pair constants multiply them
+        // once after the loop (see below).  With P = sr12, Q = sr6 and
+        // w = F_bar_i . d + h_W r^2:  a = inv (2P - Q) w, b = P - Q,
+        // c = inv (4P - Q) w, d = 2P - Q, n = 1, each masked to in-range.
+        const float m = in ? 1.0f : 0.0f;
+        const float tf = (float)tj, omt = 1.0f - tf;
+        const float w = fd + h_w * rr;
+        const float g2m = (2.0f * sr12 - sr6) * m;
+        const float ea = inv * g2m * w;
+        const float eb = (sr12 - sr6) * m;
+        const float ec = inv * (4.0f * sr12 - sr6) * w * m;
+        sa[0] += omt * ea, sa[1] += tf * ea;
+        sb[0] += omt * eb, sb[1] += tf * eb;
+        sc[0] += omt * ec, sc[1] += tf * ec;
+        sd[0] += omt * g2m, sd[1] += tf * g2m;
+        sn[0] += omt * m, sn[1] += tf * m;
+      } else {
+        const float uu = c.eps4 * (sr12 - sr6) - c.shift;
+        const float d_eps = (phi * fd + h_pe * uu + h_w * phi * rr) * c.inv_eps;
+        const float qq = 24.0f * sr12 - 6.0f * sr6;
+        const float dphi = c.eps24 * inv * qq * c.inv_sig;
+        const float du = c.eps4 * (12.0f * sr12 - 6.0f * sr6) * c.inv_sig - c.dshift;
+        const float d_sig = dphi * fd + h_pe * du + h_w * dphi * rr;
+        add_typed<kNt>(te, tj, in ? d_eps : 0.0f);
+        add_typed<kNt>(ts, tj, in ? d_sig : 0.0f);
+      }
+    }
+  }
+  if constexpr (kNt == 2) {
+    // d eps_t = (1/eps) [24 eps a + h_PE (4 eps b - shift n)],
+    // d sigma_t = (1/sigma) [24 eps 6 c + h_PE 4 eps 6 d] - h_PE dshift n.
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const AdjCoeff ct = row[t];
+      te[t] = ct.inv_eps * (ct.eps24 * sa[t] + h_pe * (ct.eps4 * sb[t] - ct.shift * sn[t]));
+      ts[t] = ct.inv_sig * (6.0f * ct.eps24 * sc[t] + 6.0f * h_pe * ct.eps4 * sd[t]) -
+              h_pe * ct.dshift * sn[t];
     }
   }
   if (kTpa > 1) {
