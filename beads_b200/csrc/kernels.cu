@@ -696,7 +696,7 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
 // Warp w builds the lists of work item w (k_scan): the warps past the cells
 // of the rebuilding replicas return after one load.
 template <int kCap>
-__global__ void __launch_bounds__(kBlock, 6) k_build(DeviceView v) {
+__global__ void __launch_bounds__(kBlock, 7) k_build(DeviceView v) {
   __shared__ BuildShared sh[kBuildWarps];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t w = blockIdx.x * kBuildWarps + warp;
