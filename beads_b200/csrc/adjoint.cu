@@ -603,6 +603,7 @@ void Engine::adjoint_segment_storage(uint32_t K) {
   const uint32_t R = A.replicas;
   const size_t S = A.slots;
   if (A.seg_capacity >= K + 1) return;
+  clear_replay_graphs();  // they record into the buffers replaced here
   A.seg_capacity = K + 1;
   A.seg_pos = A.alloc<float4>(static_cast<size_t>(K + 1) * S);
   A.seg_vel = A.alloc<float4>(static_cast<size_t>(K + 1) * S);
@@ -611,6 +612,40 @@ void Engine::adjoint_segment_storage(uint32_t K) {
   A.seg_flags = A.alloc<uint32_t>(static_cast<size_t>(K + 1) * R);
   A.seg_src = A.alloc<int>(static_cast<size_t>(K + 1) * R);
   A.seg_changed = A.alloc<uint32_t>(static_cast<size_t>(K + 1) * R);
+}
+
+// The replay of a segment of `steps` steps from its restored checkpoint:
+// record step 0, then each step followed by its recording, captured once
+// per length (the recording buffers and the step kernels are the same for
+// every segment) so a segment is one graph launch instead of a few host
+// calls per step.
+cudaGraphExec_t Engine::replay_graph_for(uint32_t steps) {
+  auto it = replay_graphs_.find(steps);
+  if (it != replay_graphs_.end()) return it->second.second;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+  try {
+    adjoint_record(0);
+    for (uint32_t k = 1; k <= steps; ++k) {
+      if (use_conditional_) {
+        record_step_conditional(false);
+      } else {
+        record_step(false);
+      }
+      adjoint_record(k);
+    }
+    cuda_check(cudaStreamEndCapture(stream_, &graph), "end capture");
+    cuda_check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+  } catch (...) {
+    cudaGraph_t discard = nullptr;
+    cudaStreamEndCapture(stream_, &discard);
+    if (discard) cudaGraphDestroy(discard);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  replay_graphs_[steps] = std::make_pair(graph, exec);
+  return exec;
 }
 
 void Engine::adjoint_record(uint32_t k) {
@@ -844,10 +879,15 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
     // when it stored every step).
     if (!A.store_all) {
       adjoint_restore(static_cast<uint32_t>(s));
-      adjoint_record(0);
-      for (uint64_t k = 1; k <= b - a; ++k) {
-        launch_chunk(1, false);
-        adjoint_record(static_cast<uint32_t>(k));
+      if (use_graphs_) {
+        cuda_check(cudaGraphLaunch(replay_graph_for(static_cast<uint32_t>(b - a)), stream_),
+                   "replay launch");
+      } else {
+        adjoint_record(0);
+        for (uint64_t k = 1; k <= b - a; ++k) {
+          launch_chunk(1, false);
+          adjoint_record(static_cast<uint32_t>(k));
+        }
       }
     }
     sync();

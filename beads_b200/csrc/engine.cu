@@ -93,6 +93,16 @@ void Engine::clear_graphs() {
     cudaGraphDestroy(kv.second.first);
   }
   graphs_.clear();
+  clear_replay_graphs();
+}
+
+void Engine::clear_replay_graphs() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto& kv : replay_graphs_) {
+    cudaGraphExecDestroy(kv.second.second);
+    cudaGraphDestroy(kv.second.first);
+  }
+  replay_graphs_.clear();
 }
 
 void Engine::set_tuning(int tpa, int fuse_post, int unroll, int no_l1) {
@@ -202,6 +212,10 @@ void Engine::autotune() {
 Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   for (auto& kv : graphs_) {
+    cudaGraphExecDestroy(kv.second.second);
+    cudaGraphDestroy(kv.second.first);
+  }
+  for (auto& kv : replay_graphs_) {
     cudaGraphExecDestroy(kv.second.second);
     cudaGraphDestroy(kv.second.first);
   }

@@ -158,6 +158,10 @@ class Engine {
   void record_step(bool observables);
   void record_step_conditional(bool observables);
   cudaGraphExec_t graph_for(uint32_t steps, bool obs_last);
+  // Adjoint: one captured graph per segment length replays the segment's
+  // steps with their recording (adjoint.cu).
+  cudaGraphExec_t replay_graph_for(uint32_t steps);
+  void clear_replay_graphs();
   void launch_chunk(uint32_t steps, bool obs_last);
   void sync();
 
@@ -176,6 +180,7 @@ class Engine {
   bool tuned_ = false;                 // autotune() has run
   cudaStream_t side_stream_ = nullptr;
   std::map<std::pair<uint32_t, bool>, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs_;
+  std::map<uint32_t, std::pair<cudaGraph_t, cudaGraphExec_t>> replay_graphs_;
   ReplicaObs* h_obs_ = nullptr;        // pinned
   ReplicaState* h_state_ = nullptr;    // pinned
   float* d_xfer_pos_ = nullptr;        // tag-order staging (lazily allocated)
