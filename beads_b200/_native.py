@@ -29,18 +29,33 @@ def _get(mapping: Mapping, key: str, path: str):
     if not isinstance(mapping, Mapping):
         raise TypeError(f"{path} must be a dict.")
     if key not in mapping:
-        raise ValueError(f"{path}.{key} is required.")
+        raise ValueError(f'{path} is missing required field "{key}".')
     return mapping[key]
 
 
+def _uint(value, path: str) -> int:
+    """Non-negative integer, refused as the reference's value reader does
+    (native/src/bindings/native_spec_value_reader.hpp:18-44)."""
+    if isinstance(value, (bool, np.bool_)) or not isinstance(value, (int, np.integer)):
+        raise TypeError(f"{path} must be an integer.")
+    if value < 0:
+        raise ValueError(f"{path} must be non-negative.")
+    if value > np.iinfo(np.uint64).max:
+        raise ValueError(f"{path} contains values outside the supported uint64 range.")
+    return int(value)
+
+
 def _array(value, dtype, shape, path: str) -> np.ndarray:
+    # Order and wording of native/src/bindings/ndarray_reader.hpp:38-72.
     if not isinstance(value, np.ndarray):
-        raise TypeError(f"{path} must be a numpy.ndarray.")
+        raise TypeError(f"{path} must be a numpy array.")
     if value.dtype != np.dtype(dtype):
         raise TypeError(f"{path} must have dtype {np.dtype(dtype).name}.")
     if tuple(value.shape) != tuple(shape):
         raise ValueError(f"{path} must have shape {tuple(shape)}.")
-    return np.ascontiguousarray(value)
+    if not value.flags.c_contiguous:
+        raise ValueError(f"{path} must be C-contiguous.")
+    return value
 
 
 def _real(params: Mapping, key: str, context: str, *, required=True, default=None,
@@ -96,14 +111,12 @@ class _Parsed:
 
     def __init__(self, spec: Mapping[str, Any]):
         self.keep = _lib.Keep()
-        system = _get(spec, "system", "spec")
-        ff = _get(spec, "forcefield", "spec")
-        dyn = _get(spec, "dynamics", "spec")
-        nbr = _get(spec, "neighbor", "spec")
-        out = _get(spec, "output", "spec")
-        self.runsteps = int(_get(spec, "runsteps", "spec"))
-        if self.runsteps < 0:
-            raise ValueError("spec.runsteps must be non-negative.")
+        system = _get(spec, "system", "native spec")
+        ff = _get(spec, "forcefield", "native spec")
+        dyn = _get(spec, "dynamics", "native spec")
+        nbr = _get(spec, "neighbor", "native spec")
+        out = _get(spec, "output", "native spec")
+        self.runsteps = _uint(_get(spec, "runsteps", "native spec"), "runsteps")
         self._system(system)
         self._forcefield(ff)
         self._dynamics(dyn)
@@ -168,25 +181,31 @@ class _Parsed:
         pair = _get(f, "pair_style", "forcefield")
         if pair is None:
             raise ValueError("forcefield.pair_style is required.")
+        pair_name = _get(pair, "style", "forcefield.pair_style")
+        coeffs = _get(f, "pair_coeffs", "forcefield")
+        # The style agreement is checked before the style itself is looked up
+        # (native/src/input/native_spec_validation.hpp:484-488, then
+        # native/src/forcefield/pair/pair_factory.cpp:44-46).
+        for c in coeffs:
+            if _get(c, "style", "pair_coeff") != pair_name:
+                raise ValueError("forcefield.pair_coeff style must match active pair_style.")
         params = _style(pair, "forcefield.pair_style", "lj", "pair")
-        _only(params, {"cutoff", "shift"}, "pair_style")
-        cutoff = _real(params, "cutoff", "pair_style", positive=True)
+        _only(params, {"cutoff", "shift"}, 'Pair("lj") pair_style')
+        cutoff = _real(params, "cutoff", 'Pair("lj") pair_style', positive=True)
         shift = params.get("shift", False)
         if not isinstance(shift, (bool, np.bool_)):
-            raise ValueError("pair_style.shift must be a boolean.")
+            raise ValueError('Pair("lj") pair_style.shift must be a boolean.')
         nt = self.n_types
         eps = np.full((nt, nt), np.nan)
         sig = np.full((nt, nt), np.nan)
-        for c in _get(f, "pair_coeffs", "forcefield"):
-            if _get(c, "style", "pair_coeff") != "lj":
-                raise ValueError('unsupported pair style "{}".'.format(c["style"]))
+        for c in coeffs:
             a, b = int(_get(c, "type_i", "pair_coeff")), int(_get(c, "type_j", "pair_coeff"))
             if not (1 <= a <= nt and 1 <= b <= nt):
                 raise ValueError("Pair(\"lj\") pair_coeff type id is outside active type range.")
             p = dict(_get(c, "params", "pair_coeff"))
-            _exact(p, {"epsilon", "sigma"}, "pair_coeff")
-            e = _real(p, "epsilon", "pair_coeff", positive=True)
-            s = _real(p, "sigma", "pair_coeff", positive=True)
+            _exact(p, {"epsilon", "sigma"}, 'Pair("lj") pair_coeff')
+            e = _real(p, "epsilon", 'Pair("lj") pair_coeff', positive=True)
+            s = _real(p, "sigma", 'Pair("lj") pair_coeff', positive=True)
             if not np.isnan(eps[a - 1, b - 1]):
                 raise ValueError("Pair(\"lj\") pair_coeff duplicate coeff for type pair.")
             eps[a - 1, b - 1] = eps[b - 1, a - 1] = e
@@ -274,7 +293,7 @@ class _Parsed:
     # dynamics / neighbour / output ------------------------------------------------
     def _dynamics(self, d) -> None:
         if _get(d, "style", "dynamics") != "velocity_verlet":
-            raise ValueError('dynamics.style must be "velocity_verlet".')
+            raise ValueError("dynamics.style must be velocity_verlet.")
         params = dict(_get(d, "params", "dynamics"))
         if set(params) != {"dt"}:
             raise ValueError('dynamics.params for style "velocity_verlet" requires exactly '
@@ -298,11 +317,27 @@ class _Parsed:
         self.dd = dd
 
     def _neighbor(self, nb) -> None:
+        # Checks and wording of native/src/input/native_spec_validation.hpp:649-669.
         nd = _lib.NeighborDesc()
-        nd.cutoff_buffer = _real(nb, "cutoff_buffer", "neighbor", nonnegative=True)
-        nd.rebuild_check_every = int(_get(nb, "rebuild_check_every", "neighbor"))
-        nd.sort_every_rebuild = int(_get(nb, "sort_every_rebuild", "neighbor"))
-        nd.max_neighbors = int(_get(nb, "max_neighbors", "neighbor"))
+        buffer = _real(nb, "cutoff_buffer", "neighbor")
+        if not np.isfinite(buffer):
+            raise ValueError("neighbor.cutoff_buffer must be finite.")
+        if buffer < 0.0:
+            raise ValueError("neighbor.cutoff_buffer must be non-negative.")
+        counts = {}
+        for key in ("rebuild_check_every", "sort_every_rebuild", "max_neighbors"):
+            counts[key] = _uint(_get(nb, key, "neighbor"), f"neighbor.{key}")
+            if counts[key] == 0:
+                raise ValueError(f"neighbor.{key} must be positive.")
+            if counts[key] > np.iinfo(np.uint32).max:
+                raise ValueError(f"neighbor.{key} contains values outside the supported "
+                                 "uint32 range.")
+        if buffer == 0.0 and counts["rebuild_check_every"] != 1:
+            raise ValueError("neighbor.cutoff_buffer=0 requires neighbor.rebuild_check_every=1.")
+        nd.cutoff_buffer = buffer
+        nd.rebuild_check_every = counts["rebuild_check_every"]
+        nd.sort_every_rebuild = counts["sort_every_rebuild"]
+        nd.max_neighbors = counts["max_neighbors"]
         self.nd = nd
 
     def _output(self, out) -> None:

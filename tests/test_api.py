@@ -190,6 +190,10 @@ def test_native_rejects_bad_spec_values():
         _native._Parsed(spec)
     spec = load_spec("mixture")
     spec["forcefield"]["pair_style"]["style"] = "morse"
+    with pytest.raises(ValueError, match="pair_coeff style must match active pair_style"):
+        _native._Parsed(spec)
+    for coeff in spec["forcefield"]["pair_coeffs"]:
+        coeff["style"] = "morse"
     with pytest.raises(ValueError, match='unsupported pair style "morse"'):
         _native._Parsed(spec)
     spec = load_spec("chains")
