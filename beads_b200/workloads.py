@@ -99,15 +99,10 @@ def lj_mixture(n: int = 1_048_576, box: float | None = 37.2, density: float | No
         sort_every_rebuild=sort_every_rebuild, thermostat=(temperature, tau))
 
 
-def polymer_melt(n_chains: int = 2000, beads: int = 200, density: float = 0.85, seed: int = 5,
-                 step: float = 0.97, reject: float = 0.8, temperature: float = 1.0,
-                 tau: float = 1.0, dt: float = 0.005, skin: float = 0.3,
-                 exclusion_distance: int = 2, dihedrals: bool = True,
-                 max_neighbors: int = 128) -> ReplicaSpec:
-    """Bead-spring melt from seeded self-avoiding random walks."""
+def _sequential_walks(rng, n_chains: int, beads: int, length: float, step: float,
+                      reject: float) -> np.ndarray:
+    """Chains grown one after another, bead by bead (pure Python; small melts)."""
     n = n_chains * beads
-    length = (n / density) ** (1.0 / 3.0)
-    rng = np.random.default_rng(seed)
     cell = reject
     ncell = max(1, int(length // cell))
     grid: dict[tuple[int, int, int], list[int]] = {}
@@ -164,6 +159,160 @@ def polymer_melt(n_chains: int = 2000, beads: int = 200, density: float = 0.85, 
                 for _k in range(back):
                     idx -= 1
                     unplace(idx)
+    return pos
+
+
+# Offsets of a cell's 27-cell neighbourhood.
+_STENCIL = np.array([(dx, dy, dz) for dx in (-1, 0, 1) for dy in (-1, 0, 1)
+                     for dz in (-1, 0, 1)], np.int64)
+
+
+def _lockstep_walks(rng, n_chains: int, beads: int, length: float, step: float,
+                    reject: float) -> np.ndarray:
+    """All chains grown together, at most one bead per chain per round (vectorised).
+
+    Same acceptance rule as the sequential walk: a bead keeps at least
+    ``reject`` from every bead already placed.  In a round, each unfinished
+    chain proposes one bead (a uniform point for a chain's first bead, else a
+    step of length ``step`` in a uniform direction from its last bead); a
+    proposal is kept when it clears the placed beads and every proposal of a
+    lower-numbered chain in the same round.  A chain makes several proposals a
+    round (more as fewer chains remain) and keeps its first clear one.  A chain
+    refused 200 times in a row backs off up to 4 beads, and after 50 back-offs
+    it starts again.
+    """
+    from scipy.spatial import cKDTree
+
+    n = n_chains * beads
+    ncell = max(1, int(length // reject))
+    csize = length / ncell
+    # Points at least `reject` apart in a cube of side below 2 * reject / sqrt(3)
+    # number at most 8 (one per octant); coarser grids (tiny boxes) get room for 64.
+    cap = 8 if csize < 2.0 * reject / math.sqrt(3.0) else 64
+    members = np.full((ncell ** 3, cap), -1, np.int64)
+    fill = np.zeros(ncell ** 3, np.int64)
+    cell_of = np.full(n, -1, np.int64)
+    pos = np.zeros((n, 3))
+    size = np.zeros(n_chains, np.int64)
+    refused = np.zeros(n_chains, np.int64)
+    backoffs = np.zeros(n_chains, np.int64)
+    r2 = reject * reject
+
+    def cell_index(p):
+        k = np.floor(p / csize).astype(np.int64) % ncell
+        return k, (k[:, 2] * ncell + k[:, 1]) * ncell + k[:, 0]
+
+    def unplace(at: int) -> None:
+        c = cell_of[at]
+        row = members[c]
+        j = int(np.nonzero(row == at)[0][0])
+        last = fill[c] - 1
+        row[j] = row[last]
+        row[last] = -1
+        fill[c] = last
+        cell_of[at] = -1
+
+    while True:
+        active = np.nonzero(size < beads)[0]
+        if active.size == 0:
+            break
+        m = active.size
+        tries = int(min(64, max(2, 8192 // m)))  # proposals per chain this round
+        first = size[active] == 0
+        cand = np.empty((m, tries, 3))
+        cand[first] = rng.uniform(0.0, length, (int(first.sum()), tries, 3))
+        grow = ~first
+        if grow.any():
+            u = rng.standard_normal((int(grow.sum()), tries, 3))
+            u /= np.linalg.norm(u, axis=2)[..., None]
+            prev = active[grow] * beads + size[active[grow]] - 1
+            cand[grow] = pos[prev][:, None, :] + step * u
+        cand = np.mod(cand, length).reshape(m * tries, 3)
+        cand[cand >= length] = 0.0
+        k, flat = cell_index(cand)
+        near = (k[:, None, :] + _STENCIL[None, :, :]) % ncell
+        near = (near[..., 2] * ncell + near[..., 1]) * ncell + near[..., 0]
+        who = members[near].reshape(m * tries, -1)
+        row, col = np.nonzero(who >= 0)
+        d = cand[row] - pos[who[row, col]]
+        d -= length * np.round(d / length)
+        hit = row[np.einsum("ij,ij->i", d, d) < r2]
+        free = np.ones(m * tries, bool)
+        free[hit] = False
+        free = free.reshape(m, tries)
+        # Each chain takes its first free proposal; `used` counts the attempts.
+        pick = np.argmax(free, axis=1)
+        found = free[np.arange(m), pick]
+        used = np.where(found, pick + 1, tries)
+        choice = np.arange(m) * tries + pick
+        clash = ~found
+        ok = np.nonzero(found)[0]
+        if ok.size > 1:
+            pts = cand[choice[ok]]
+            pairs = cKDTree(pts, boxsize=length).query_pairs(reject, output_type="ndarray")
+            if len(pairs):
+                # Every proposal in a close pair but the lowest-numbered chain's
+                # one is refused (proposals are in chain order).
+                keep = np.ones(ok.size, bool)
+                order = np.argsort(pairs[:, 0], kind="stable")
+                for a, b in pairs[order]:
+                    if keep[a]:
+                        keep[b] = False
+                clash[ok[~keep]] = True
+                ok = ok[keep]
+        if ok.size:
+            chains = active[ok]
+            at = chains * beads + size[chains]
+            pos[at] = cand[choice[ok]]
+            cells = flat[choice[ok]]
+            srt = np.argsort(cells, kind="stable")
+            cells_s = cells[srt]
+            starts = np.r_[0, np.nonzero(np.diff(cells_s))[0] + 1]
+            rank = np.arange(cells_s.size) - np.repeat(starts, np.diff(np.r_[starts,
+                                                                            cells_s.size]))
+            slot = fill[cells_s] + rank
+            if slot.max() >= cap:
+                raise RuntimeError("polymer_melt: cell capacity exceeded")
+            members[cells_s, slot] = at[srt]
+            np.add.at(fill, cells_s, 1)
+            cell_of[at] = cells
+            size[chains] += 1
+            refused[chains] = 0
+        bad = active[clash]
+        refused[bad] += used[clash]
+        for c in bad[refused[bad] >= 200]:
+            refused[c] = 0
+            backoffs[c] += 1
+            if backoffs[c] > 50:
+                back, backoffs[c] = int(size[c]), 0
+            else:
+                back = int(min(size[c] - 1, 4))
+            for _k in range(back):
+                size[c] -= 1
+                unplace(int(c * beads + size[c]))
+    return pos
+
+
+def polymer_melt(n_chains: int = 2000, beads: int = 200, density: float = 0.85, seed: int = 5,
+                 step: float = 0.97, reject: float = 0.8, temperature: float = 1.0,
+                 tau: float = 1.0, dt: float = 0.005, skin: float = 0.3,
+                 exclusion_distance: int = 2, dihedrals: bool = True,
+                 max_neighbors: int = 128, growth: str = "sequential") -> ReplicaSpec:
+    """Bead-spring melt from seeded self-avoiding random walks.
+
+    ``growth="sequential"`` grows the chains one after another (the layout
+    the small test melts are pinned on); ``"lockstep"`` grows them all
+    together, vectorised, for melts of hundreds of thousands of beads.
+    """
+    n = n_chains * beads
+    length = (n / density) ** (1.0 / 3.0)
+    rng = np.random.default_rng(seed)
+    if growth == "sequential":
+        pos = _sequential_walks(rng, n_chains, beads, length, step, reject)
+    elif growth == "lockstep":
+        pos = _lockstep_walks(rng, n_chains, beads, length, step, reject)
+    else:
+        raise ValueError(f"unknown growth {growth!r}")
     lo = np.zeros(3)
     hi = np.full(3, length)
     posf = _inside(pos, lo, hi)

@@ -514,6 +514,79 @@ def run_replicas(args) -> None:
         print(json.dumps(line))
 
 
+CHAINS_METRIC = ("atom-steps/s on 1 B200 (400,000-bead bead-spring melt: WCA pairs, harmonic "
+                 "bonds, angles and dihedrals, 1-2/1-3 exclusions)")
+
+
+def run_chains(args) -> None:
+    """The bead-spring melt: 2000 chains of 200 beads grown as seeded
+    self-avoiding walks (step 0.97, rejection radius 0.8) at rho 0.85,
+    reduced units; LJ rc 2^(1/6) shifted, skin 0.3; bonds k 500 r0 0.97,
+    angles k 5 theta0 150, dihedrals k 1 d 1 n 1; pairs within two bonds
+    excluded; Berendsen T 1 tau 1, dt 0.005.  One engine on one GPU,
+    device-timed."""
+    import torch
+
+    from beads_b200 import workloads
+    from beads_b200.engine import Engine
+
+    world, rank, local = _dist()
+    if world > 1:
+        raise SystemExit("--workload chains runs on one GPU")
+    torch.cuda.set_device(local)
+    spec = workloads.polymer_melt(seed=5, growth="lockstep")
+    eng = Engine(spec)
+    stream = torch.cuda.ExternalStream(eng.info()["stream"], device=torch.device("cuda", local))
+    eng.run(max(3, args.warmup))
+    eng.run(GRAPH_WARMUP)
+    builds_before = eng.counters(0)["builds"]
+    chains_before = eng.counters()["chain_launches"]
+    sampler = ClockSampler(local)
+    torch.cuda.synchronize()
+    sampler.start()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    eng.run(args.steps)
+    stop.record(stream)
+    stop.synchronize()
+    clocks = sampler.stop()
+    ms = start.elapsed_time(stop)
+    builds = eng.counters(0)["builds"] - builds_before
+    chains = eng.counters()["chain_launches"] - chains_before
+    schedule = eng.tuning()
+    eng.close()
+    line = {
+        "metric": CHAINS_METRIC,
+        "value": spec.n * args.steps / (ms / 1e3),
+        "unit": UNIT,
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": "bead-spring melt, 2000 chains x 200 beads, rho 0.85, WCA rc 2^(1/6), "
+                        "skin 0.3, bonds/angles/dihedrals, exclusions within 2 bonds, "
+                        "Berendsen T 1 tau 1, dt 0.005",
+            "parallelism": "none",
+            "neighbor_builds_timed": int(builds),
+            "graph_warmup_steps": GRAPH_WARMUP,
+            "schedule": schedule,
+        },
+        # pre, decide, pair forces, bonded forces (+ half-kick), [post,] post finish
+        # per step; bin, scan, scatter, cellsort, two reorder passes, exclusion
+        # projection and list build per rebuild chain.
+        "gpu_launches": (5 if schedule["fuse_post"] else 6) * args.steps + 8 * int(chains),
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+
+
 ADJOINT_METRIC = ("differentiated atom-steps/s on 1 B200 (64 x 8192-bead LJ mixture, forward "
                   "with checkpoints + adjoint backward, FP32 pair math)")
 
@@ -647,10 +720,11 @@ def main() -> None:
     parser.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     parser.add_argument("--adj-steps", type=int, default=1000)
     parser.add_argument("--workload", default="mixture",
-                        choices=["mixture", "replicas", "adjoint"],
+                        choices=["mixture", "replicas", "adjoint", "chains"],
                         help="mixture: the 1M-bead mixture (default); replicas: the "
                              "512-replica batch beside one-at-a-time runs; adjoint: the "
-                             "differentiable 64-replica fit")
+                             "differentiable 64-replica fit; chains: the 400,000-bead "
+                             "bead-spring melt")
     parser.add_argument("--replicas", type=int, default=512)
     parser.add_argument("--beads", type=int, default=N_BEADS,
                         help="system size (same density); profiling of small cases only")
@@ -663,6 +737,8 @@ def main() -> None:
         run_replicas(args)
     elif args.workload == "adjoint":
         run_adjoint(args)
+    elif args.workload == "chains":
+        run_chains(args)
     else:
         run_ours(args)
 

@@ -6,7 +6,7 @@ initial neighbour build and every step).
 
 TEST INFRASTRUCTURE ONLY (needs a GPU and oracle/build_ref.py's output).
 
-    python -m oracle.ref_bench <out.json> [--quick] [--replicas]
+    python -m oracle.ref_bench <out.json> [--quick] [--replicas | --chains]
 """
 
 from __future__ import annotations
@@ -81,10 +81,15 @@ def main(argv: list[str]) -> None:
         out_path.write_text(json.dumps({"replica_batch": entry}, indent=1))
         return
     # Step counts of the workloads' own specifications: the 4096-bead lattice
-    # runs 1,000 steps, the 1M-bead mixture 10,000.
-    cases = [("lattice_4096", workloads.lj_lattice(n_side=16), 1000)]
-    n_mix = 131072 if quick else 1_048_576
-    cases.append((f"mixture_{n_mix}", _relaxed_mixture(n_mix), 200 if quick else 10000))
+    # runs 1,000 steps, the 1M-bead mixture 10,000, the 400,000-bead melt 20,000.
+    if "--chains" in argv:
+        n_chains = 250 if quick else 2000
+        melt = workloads.polymer_melt(n_chains=n_chains, growth="lockstep")
+        cases = [(f"chains_{melt.n}", melt, 1000 if quick else 20000)]
+    else:
+        cases = [("lattice_4096", workloads.lj_lattice(n_side=16), 1000)]
+        n_mix = 131072 if quick else 1_048_576
+        cases.append((f"mixture_{n_mix}", _relaxed_mixture(n_mix), 200 if quick else 10000))
     results = {}
     for name, r, steps in cases:
         spec = spec_for(r, steps, "run", forces=False, thermo_every=steps)
