@@ -190,6 +190,32 @@ def _cpu_baseline(positions, spec, budget_s: float):
                       f"{wall:.1f} s of host work, FP64 oracle with OpenMP"}
 
 
+def _cpu_baseline_melt(spec, budget_s: float):
+    """Times the CPU oracle port (OpenMP, FP64) on the whole bead-spring melt
+    (pairs, bonds, angles, dihedrals, exclusions, Berendsen) for a bounded
+    number of MD steps (about budget_s of host work)."""
+    from oracle import oracle as O
+
+    ff = O.ForceField(epsilon=np.asarray(spec.epsilon, np.float64).ravel(),
+                      sigma=np.asarray(spec.sigma, np.float64).ravel(), cutoff=spec.cutoff,
+                      shift=spec.shift, bond_k=spec.bond_k, bond_r0=spec.bond_r0,
+                      angle_k=spec.angle_k, angle_theta0=spec.angle_theta0,
+                      dihedral_k=spec.dihedral_k, dihedral_d=spec.dihedral_d,
+                      dihedral_n=spec.dihedral_n, exclusion_distance=spec.exclusion_distance)
+    # reduced units: k_B T is the target temperature itself
+    sim = O.Sim(spec.positions, spec.velocities, spec.masses, spec.types, spec.box_bound, ff,
+                dt=spec.dt, skin=spec.cutoff_buffer, check_every=spec.rebuild_check_every,
+                bonds=spec.bonds, angles=spec.angles, dihedrals=spec.dihedrals,
+                thermostat=True, kt_target=spec.thermostat[0], tau=spec.thermostat[1])
+    rate, wall = _cpu_rate(sim, spec.n, 1)
+    steps = max(1, int(budget_s / max(wall, 1e-3)))
+    rate, wall = _cpu_rate(sim, spec.n, steps)
+    sim.close()
+    return {"value": rate, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+            "sample": f"{steps} MD steps of the full {spec.n}-bead melt (after one untimed "
+                      f"step), {wall:.1f} s of host work, FP64 oracle with OpenMP"}
+
+
 def _lattice_mixture(n_side: int):
     """The workload's mixture (same density, composition, parameters) on a
     jittered n_side^3 simple-cubic lattice: no overlaps, so the CPU arm needs
@@ -584,6 +610,8 @@ def run_chains(args) -> None:
         "gpu_launches": (5 if schedule["fuse_post"] else 6) * args.steps + 8 * int(chains),
         "clocks": clocks,
     }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = _cpu_baseline_melt(spec, args.cpu_budget)
     print(json.dumps(line))
 
 
