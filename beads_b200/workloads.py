@@ -189,8 +189,15 @@ def _lockstep_walks(rng, n_chains: int, beads: int, length: float, step: float,
     # Points at least `reject` apart in a cube of side below 2 * reject / sqrt(3)
     # number at most 8 (one per octant); coarser grids (tiny boxes) get room for 64.
     cap = 8 if csize < 2.0 * reject / math.sqrt(3.0) else 64
-    members = np.full((ncell ** 3, cap), -1, np.int64)
+    members = np.full((ncell ** 3, cap), -1, np.int32)
     fill = np.zeros(ncell ** 3, np.int64)
+    # flat ids of every cell's 27-cell neighbourhood, periodic
+    axis = np.arange(ncell)
+    kk = np.stack(np.meshgrid(axis, axis, axis, indexing="ij"), -1).reshape(-1, 3)[:, ::-1]
+    around = (kk[:, None, :] + _STENCIL[None, :, :]) % ncell
+    stencil_of = ((around[..., 2] * ncell + around[..., 1]) * ncell
+                  + around[..., 0]).astype(np.int32)
+    del kk, around
     cell_of = np.full(n, -1, np.int64)
     pos = np.zeros((n, 3))
     size = np.zeros(n_chains, np.int64)
@@ -200,7 +207,7 @@ def _lockstep_walks(rng, n_chains: int, beads: int, length: float, step: float,
 
     def cell_index(p):
         k = np.floor(p / csize).astype(np.int64) % ncell
-        return k, (k[:, 2] * ncell + k[:, 1]) * ncell + k[:, 0]
+        return (k[:, 2] * ncell + k[:, 1]) * ncell + k[:, 0]
 
     def unplace(at: int) -> None:
         c = cell_of[at]
@@ -229,10 +236,8 @@ def _lockstep_walks(rng, n_chains: int, beads: int, length: float, step: float,
             cand[grow] = pos[prev][:, None, :] + step * u
         cand = np.mod(cand, length).reshape(m * tries, 3)
         cand[cand >= length] = 0.0
-        k, flat = cell_index(cand)
-        near = (k[:, None, :] + _STENCIL[None, :, :]) % ncell
-        near = (near[..., 2] * ncell + near[..., 1]) * ncell + near[..., 0]
-        who = members[near].reshape(m * tries, -1)
+        flat = cell_index(cand)
+        who = members[stencil_of[flat]].reshape(m * tries, -1)
         row, col = np.nonzero(who >= 0)
         d = cand[row] - pos[who[row, col]]
         d -= length * np.round(d / length)
