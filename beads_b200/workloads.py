@@ -12,6 +12,7 @@ fixed seeds.
                       rejection radius 0.8) with harmonic bonds, angles and
                       dihedrals, reduced units, rho 0.85.
 * ``replica_batch``   many independent single-type LJ boxes of uneven size.
+* ``relaxed``         a spec moved by capped steepest descent on the GPU.
 
 Each function returns ``ReplicaSpec`` objects for ``beads_b200.engine.Engine``.
 """
@@ -346,6 +347,30 @@ def polymer_melt(n_chains: int = 2000, beads: int = 200, density: float = 0.85, 
         dihedral_k=[1.0] if dihedrals else None, dihedral_d=[1] if dihedrals else None,
         dihedral_n=[1] if dihedrals else None, exclusion_distance=exclusion_distance,
         cutoff_buffer=skin, max_neighbors=max_neighbors, thermostat=(temperature, tau))
+
+
+def relaxed(spec: ReplicaSpec, iterations: int = 500, dmax: float = 0.01,
+            fref: float = 100.0, capacity: int = 256) -> ReplicaSpec:
+    """A copy of ``spec`` moved by ``iterations`` capped steepest-descent
+    steps on the GPU (``Engine.minimize``: every bead moves dmax * F /
+    max(|F|, fref), all force terms included), with positions wrapped into
+    the box and images carried.  The descent runs with a list capacity of at
+    least ``capacity``; the copy keeps the spec's own.  A start grown with a
+    rejection radius below the pair minimum (the polymer melt: 0.8 against
+    2^(1/6)) needs it before MD: from the raw start the overlapping pairs
+    heat the melt until its neighbour lists overflow."""
+    import dataclasses
+
+    from .engine import Engine
+
+    work = dataclasses.replace(spec, max_neighbors=max(capacity, spec.max_neighbors))
+    with Engine(work) as eng:
+        eng.minimize(iterations, dmax, fref)
+        st = eng.state()
+    box = np.asarray(spec.box_bound, np.float64)
+    return dataclasses.replace(spec, positions=_inside(st["positions"].astype(np.float64),
+                                                       box[0], box[1]),
+                               images=st["images"].copy())
 
 
 def replica_batch(n_replicas: int = 512, n_min: int = 256, n_max: int = 32768, seed: int = 7,

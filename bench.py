@@ -546,11 +546,11 @@ CHAINS_METRIC = ("atom-steps/s on 1 B200 (400,000-bead bead-spring melt: WCA pai
 
 def run_chains(args) -> None:
     """The bead-spring melt: 2000 chains of 200 beads grown as seeded
-    self-avoiding walks (step 0.97, rejection radius 0.8) at rho 0.85,
-    reduced units; LJ rc 2^(1/6) shifted, skin 0.3; bonds k 500 r0 0.97,
-    angles k 5 theta0 150, dihedrals k 1 d 1 n 1; pairs within two bonds
-    excluded; Berendsen T 1 tau 1, dt 0.005.  One engine on one GPU,
-    device-timed."""
+    self-avoiding walks (step 0.97, rejection radius 0.8) at rho 0.85 and
+    relaxed by 500 capped steepest-descent steps, reduced units; LJ rc
+    2^(1/6) shifted, skin 0.3; bonds k 500 r0 0.97, angles k 5 theta0 150,
+    dihedrals k 1 d 1 n 1; pairs within two bonds excluded; Berendsen T 1
+    tau 1, dt 0.005.  One engine on one GPU, device-timed."""
     import torch
 
     from beads_b200 import workloads
@@ -560,7 +560,7 @@ def run_chains(args) -> None:
     if world > 1:
         raise SystemExit("--workload chains runs on one GPU")
     torch.cuda.set_device(local)
-    spec = workloads.polymer_melt(seed=5, growth="lockstep")
+    spec = workloads.relaxed(workloads.polymer_melt(seed=5, growth="lockstep"))
     eng = Engine(spec)
     stream = torch.cuda.ExternalStream(eng.info()["stream"], device=torch.device("cuda", local))
     eng.run(max(3, args.warmup))
@@ -596,7 +596,8 @@ def run_chains(args) -> None:
         "dtype": "f32",
         "data": "synthetic",
         "config": {
-            "workload": "bead-spring melt, 2000 chains x 200 beads, rho 0.85, WCA rc 2^(1/6), "
+            "workload": "bead-spring melt, 2000 chains x 200 beads, rho 0.85 (relaxed start), "
+                        "WCA rc 2^(1/6), "
                         "skin 0.3, bonds/angles/dihedrals, exclusions within 2 bonds, "
                         "Berendsen T 1 tau 1, dt 0.005",
             "parallelism": "none",

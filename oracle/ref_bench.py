@@ -84,7 +84,7 @@ def main(argv: list[str]) -> None:
     # runs 1,000 steps, the 1M-bead mixture 10,000, the 400,000-bead melt 20,000.
     if "--chains" in argv:
         n_chains = 250 if quick else 2000
-        melt = workloads.polymer_melt(n_chains=n_chains, growth="lockstep")
+        melt = workloads.relaxed(workloads.polymer_melt(n_chains=n_chains, growth="lockstep"))
         cases = [(f"chains_{melt.n}", melt, 1000 if quick else 20000)]
     else:
         cases = [("lattice_4096", workloads.lj_lattice(n_side=16), 1000)]
