@@ -58,3 +58,44 @@ def test_lockstep_melt_crowded_small_box():
 def test_unknown_growth_refused():
     with pytest.raises(ValueError, match="unknown growth"):
         workloads.polymer_melt(n_chains=2, beads=4, growth="spiral")
+
+
+def test_relaxed_carries_positions_images_and_capacity(monkeypatch):
+    # Engine stand-in (the descent itself runs on the GPU): records the list
+    # capacity it was built with and returns moved, partly wrapped positions.
+    import beads_b200.engine as engine_mod
+
+    seen = {}
+
+    class FakeEngine:
+        def __init__(self, spec):
+            seen["capacity"] = spec.max_neighbors
+            self.n = spec.n
+            self.hi = float(spec.box_bound[1][0])
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *exc):
+            return False
+
+        def minimize(self, iterations, dmax, fref):
+            seen["args"] = (iterations, dmax, fref)
+
+        def state(self):
+            pos = np.full((self.n, 3), 0.5, np.float32)
+            pos[0, 0] = self.hi  # a coordinate that rounded onto the upper bound
+            img = np.zeros((self.n, 3), np.int32)
+            img[1] = (1, 0, -1)
+            return {"positions": pos, "images": img}
+
+    monkeypatch.setattr(engine_mod, "Engine", FakeEngine)
+    spec = workloads.polymer_melt(n_chains=3, beads=6, seed=1, max_neighbors=64)
+    out = workloads.relaxed(spec, iterations=7, dmax=0.02, fref=50.0)
+    assert seen == {"capacity": 256, "args": (7, 0.02, 50.0)}
+    assert out.max_neighbors == 64 and spec.max_neighbors == 64
+    assert out.positions.dtype == np.float32
+    assert (out.positions < np.float32(spec.box_bound[1][0])).all()
+    assert tuple(out.images[1]) == (1, 0, -1)
+    assert np.array_equal(out.bonds, spec.bonds)
+    assert out is not spec and not np.array_equal(out.positions, spec.positions)
