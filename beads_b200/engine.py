@@ -109,6 +109,8 @@ def _descriptors(spec: ReplicaSpec, keep: _lib.Keep):
     sd = _lib.SystemDesc()
     n = spec.n
     sd.n_particles = n
+    if spec.units not in _lib.UNITS:
+        raise ValueError('system.units must be "reduced" or "nm_kjmol".')
     sd.units = _lib.UNITS[spec.units]
     bb = np.asarray(spec.box_bound, dtype=np.float32).reshape(2, 3)
     sd.box_lo[:] = [float(x) for x in bb[0]]
