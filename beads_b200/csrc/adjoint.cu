@@ -36,6 +36,7 @@
 #include "device_util.cuh"
 #include "engine.hpp"
 #include "kernels.cuh"
+#include "trace.hpp"
 
 namespace bb {
 
@@ -693,6 +694,7 @@ void Engine::adjoint_restore(uint32_t c) {
 }
 
 void Engine::adjoint_forward(uint64_t steps, uint64_t record_from, uint32_t every, double* obs) {
+  TraceRange trace("beads.adjoint_forward");
   if (steps == 0) throw InvalidArgument("adjoint runs need at least one step.");
   if (record_from > steps) throw InvalidArgument("record_from must not exceed steps.");
   for (const auto& h : rep_) {
@@ -797,6 +799,7 @@ void Engine::adjoint_forward(uint64_t steps, uint64_t record_from, uint32_t ever
 
 void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* grad_sigma,
                               float* grad_pos, float* grad_vel) {
+  TraceRange trace("beads.adjoint_backward");
   if (!adj_ || !adj_->forward_done) throw InvalidArgument("adjoint_backward needs a forward run.");
   AdjointStore& A = *adj_;
   const uint32_t R = A.replicas;

@@ -10,6 +10,7 @@
 
 #include "engine.hpp"
 #include "outputs.hpp"
+#include "trace.hpp"
 
 struct beads_ctx {
   bb::Engine* engine = nullptr;
@@ -75,6 +76,7 @@ std::string str(const T& v) {
 // 113-244): initial build + forces (step 0 outputs), then runsteps steps with
 // outputs on multiples of each output's `every`, then the final state.
 void execute_run(const beads_run_desc& run) {
+  bb::TraceRange trace("beads.execute");
   require(run.system && run.forcefield && run.neighbor && run.dynamics,
           "run description is incomplete.");
   const beads_system_desc& sys = *run.system;

@@ -2,6 +2,7 @@
 // tables, the captured step loop and host transfers.
 #include "engine.hpp"
 #include "adjoint.hpp"
+#include "trace.hpp"
 
 #include <cstdio>
 
@@ -134,6 +135,7 @@ void Engine::tuning(int* tpa, int* fuse_post, int* unroll, int* no_l1, int* auto
 // keeps the fastest.  The kicks of the trial launches are undone.  With
 // BEADS_TUNE_LOG=1 the timings go to stderr.
 void Engine::autotune() {
+  TraceRange trace("beads.autotune");
   if (!initialized_) eval();
   constexpr int kWarm = 1, kReps = 4;
   const bool log = [] {
@@ -657,6 +659,7 @@ void Engine::check_status() {
 }
 
 void Engine::eval() {
+  TraceRange trace("beads.eval");
   launch_apply_lambda(launch_);
   launch_rebuild(launch_, true);
   launch_forces(launch_, true, false);
@@ -770,6 +773,7 @@ void Engine::launch_chunk(uint32_t steps, bool obs_last) {
 }
 
 bool Engine::run(uint64_t steps, uint64_t obs_every) {
+  TraceRange trace("beads.run");
   if (!initialized_) eval();
   if (!tuned_ && !tuning_fixed_ && steps > 0) autotune();
   bool last_obs = false;
@@ -802,6 +806,7 @@ bool Engine::run(uint64_t steps, uint64_t obs_every) {
 }
 
 void Engine::minimize(uint32_t iterations, float dmax, float fref) {
+  TraceRange trace("beads.minimize");
   StepLaunch l = launch_;
   l.sd_dmax = dmax;
   l.sd_fref = fref;
