@@ -35,7 +35,8 @@ def _system_from(spec_like) -> beads.System:
     s = beads.System(positions=spec_like.positions, types=spec_like.types,
                      box_bound=spec_like.box_bound, velocities=spec_like.velocities,
                      masses=spec_like.masses, tags=spec_like.tags,
-                     molecule_ids=spec_like.molecule_ids, units=spec_like.units)
+                     molecule_ids=spec_like.molecule_ids, images=spec_like.images,
+                     units=spec_like.units)
     if spec_like.bonds is not None:
         s.set_topology(bonds=[tuple(map(int, b)) for b in spec_like.bonds],
                        angles=None if spec_like.angles is None
