@@ -1,7 +1,8 @@
 """The seeded workload generators (CPU): the polymer melt's two growth
 orders keep the same invariants (no two beads closer than the rejection
 radius, every bond of the step length, chains of the asked size) and are
-reproducible from the seed."""
+reproducible from the seed; ``relaxed`` hands the descent a roomy list and
+carries its positions and images back (engine stood in by a fake)."""
 
 from __future__ import annotations
 
