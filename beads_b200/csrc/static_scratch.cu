@@ -17,7 +17,6 @@
 
 #include <cstdint>
 #include <cstring>
-#include <mutex>
 
 #include "../../include/beads_b200.h"
 #include "setup.hpp"
@@ -31,13 +30,9 @@ namespace {
 constexpr uint32_t kStaticMaxCells = BEADS_STATIC_MAX_CELLS;
 constexpr int kStaticThreads = 256;
 constexpr int kStaticScanThreads = 1024;
-constexpr int kMaxDevices = 64;
 
 // Shared by every call on a device; contents survive from the previous call.
 static __device__ __align__(256) uint32_t g_static_scratch[2 * kStaticMaxCells];
-
-std::mutex g_setup_mutex;
-uint32_t* g_scratch_ptr[kMaxDevices] = {};
 
 __device__ __forceinline__ uint32_t static_axis_cell(float x, float lo, float inv, uint32_t n) {
   const float scaled = __fmul_rn(__fsub_rn(x, lo), inv);
@@ -108,8 +103,9 @@ __global__ void k_static_scatter(const uint32_t* cell_of, uint32_t n, uint32_t* 
   order[atomicAdd(&cursor[cell_of[i]], 1u)] = i;
 }
 
-// Ascending particle index inside every cell: one warp per cell, a register
-// bitonic network up to 32 members, insertion sort by one lane above that.
+// Ascending particle index inside every cell.  Cells of up to 32 members:
+// one warp each, a bitonic network in registers.  Larger cells: one block
+// each (k_static_cellsort_big), so no cell is ever sorted by a single thread.
 __global__ void k_static_cellsort(const uint32_t* cell_start, uint32_t n_cells, uint32_t* order) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warps = blockDim.x / 32u;
@@ -117,29 +113,70 @@ __global__ void k_static_cellsort(const uint32_t* cell_start, uint32_t n_cells, 
     const uint32_t s0 = cell_start[c];
     const uint32_t s1 = cell_start[c + 1];
     const uint32_t m = s1 - s0;
-    if (m <= 1u) continue;
-    if (m <= 32u) {
-      uint32_t val = lane < m ? order[s0 + lane] : 0xffffffffu;
-      for (uint32_t k = 2; k <= 32; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-          const uint32_t other = __shfl_xor_sync(0xffffffffu, val, j);
-          const bool up = (lane & k) == 0u;
-          const bool lower = (lane & j) == 0u;
-          val = (lower == up) ? min(val, other) : max(val, other);
-        }
-      }
-      if (lane < m) order[s0 + lane] = val;
-    } else if (lane == 0) {
-      for (uint32_t a = s0 + 1; a < s1; ++a) {
-        const uint32_t key = order[a];
-        uint32_t q = a;
-        while (q > s0 && order[q - 1] > key) {
-          order[q] = order[q - 1];
-          --q;
-        }
-        order[q] = key;
+    if (m <= 1u || m > 32u) continue;  // warp-uniform
+    uint32_t val = lane < m ? order[s0 + lane] : 0xffffffffu;
+    for (uint32_t k = 2; k <= 32; k <<= 1) {
+      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+        const uint32_t other = __shfl_xor_sync(0xffffffffu, val, j);
+        const bool up = (lane & k) == 0u;
+        const bool lower = (lane & j) == 0u;
+        val = (lower == up) ? min(val, other) : max(val, other);
       }
     }
+    if (lane < m) order[s0 + lane] = val;
+  }
+}
+
+// Cells of more than 32 members, one block per cell at a time: an ascending
+// bitonic network over the m members in place (the form without direction
+// flips: the first exchange of a stage of width k pairs i with the mirror
+// i ^ (k - 1), the later ones i with i ^ j; a partner at or past m stands
+// for +infinity, so that exchange is skipped).  O(m log^2 m) compare-exchanges
+// spread over the block, with a block barrier between passes; members are
+// staged in shared memory when they fit, otherwise sorted where they lie.
+constexpr uint32_t kStaticBigThreads = 1024;
+constexpr uint32_t kStaticSmemKeys = 8192;  // 32 KiB of shared memory
+
+__device__ __forceinline__ void static_exchange(uint32_t* a, uint32_t i, uint32_t partner,
+                                                uint32_t m) {
+  if (partner > i && partner < m) {
+    const uint32_t x = a[i], y = a[partner];
+    if (y < x) {
+      a[i] = y;
+      a[partner] = x;
+    }
+  }
+}
+
+__device__ void static_bitonic(uint32_t* a, uint32_t m) {
+  for (uint32_t k = 2; k < 2u * m; k <<= 1) {
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+      static_exchange(a, i, i ^ (k - 1u), m);
+    }
+    __syncthreads();
+    for (uint32_t j = k >> 2; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) static_exchange(a, i, i ^ j, m);
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kStaticBigThreads)
+k_static_cellsort_big(const uint32_t* cell_start, uint32_t n_cells, uint32_t* order) {
+  __shared__ uint32_t keys[kStaticSmemKeys];
+  for (uint32_t c = blockIdx.x; c < n_cells; c += gridDim.x) {
+    const uint32_t s0 = cell_start[c];
+    const uint32_t m = cell_start[c + 1] - s0;
+    if (m <= 32u) continue;  // block-uniform
+    if (m <= kStaticSmemKeys) {
+      for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) keys[i] = order[s0 + i];
+      __syncthreads();
+      static_bitonic(keys, m);
+      for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) order[s0 + i] = keys[i];
+    } else {
+      static_bitonic(order + s0, m);
+    }
+    __syncthreads();
   }
 }
 
@@ -148,25 +185,18 @@ int static_fail(int code, const char* message) {
   return code;
 }
 
-// Address of the static array on the current device, looked up once per
-// device (cudaGetSymbolAddress; the host-side symbol is not a device address).
+// Device address of the static array on the current device.  The host-side
+// symbol is only a stand-in, never a device address; the address is looked up
+// on every call (cheap), so a module reloaded after cudaDeviceReset is seen.
 int scratch_for_current_device(uint32_t** out) {
-  int device = -1;
-  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) {
-    return static_fail(BEADS_ERR_CUDA, "beads_cell_sort_static: no usable current CUDA device.");
+  void* ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+  if (e != cudaSuccess || ptr == nullptr) {
+    return static_fail(BEADS_ERR_CUDA,
+                       "beads_cell_sort_static: cudaGetSymbolAddress of the static scratch "
+                       "array failed.");
   }
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (g_scratch_ptr[device] == nullptr) {
-    void* ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
-    if (e != cudaSuccess || ptr == nullptr) {
-      return static_fail(BEADS_ERR_CUDA,
-                         "beads_cell_sort_static: cudaGetSymbolAddress of the static scratch "
-                         "array failed.");
-    }
-    g_scratch_ptr[device] = static_cast<uint32_t*>(ptr);
-  }
-  *out = g_scratch_ptr[device];
+  *out = static_cast<uint32_t*>(ptr);
   return BEADS_OK;
 }
 
@@ -219,6 +249,9 @@ extern "C" int beads_cell_sort_static(const float* d_positions, uint32_t n, cons
   k_static_scatter<<<blocks, kStaticThreads, 0, s>>>(d_cell_of, n, cursor, d_order);
   const uint32_t sort_blocks = (plan.n_cells + (kStaticThreads / 32) - 1) / (kStaticThreads / 32);
   k_static_cellsort<<<sort_blocks, kStaticThreads, 0, s>>>(d_cell_start, plan.n_cells, d_order);
+  const uint32_t big_blocks = plan.n_cells < 592u ? plan.n_cells : 592u;  // 4 per SM at most
+  k_static_cellsort_big<<<big_blocks, kStaticBigThreads, 0, s>>>(d_cell_start, plan.n_cells,
+                                                                 d_order);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return static_fail(BEADS_ERR_CUDA, cudaGetErrorString(e));
   if (n_cells_out) *n_cells_out = plan.n_cells;

@@ -6,7 +6,11 @@ Its cell ids are compared bit for bit with those the engine reports through
 beads_debug_cells for the same positions, on two calls in a row with
 different systems (the second call also shows that the shared static counters
 are cleared between calls); the sorted order is checked for being the stable
-counting sort of those ids.
+counting sort of those ids.  Grids the engine comparison does not reach are
+checked against the oracle's cell ids (the reference's rule, clamps
+included): crowded cells (~100 members, and more than the 8192 members the
+block sort stages in shared memory), 2 cells per axis, and beads just
+outside [lo, hi).
 """
 
 from __future__ import annotations
@@ -73,6 +77,42 @@ def test_static_cell_sort_matches_engine_on_two_calls():
     for spec, (cell_of, order, cell_start, nc) in zip((first, second), results):
         assert np.array_equal(cell_of, _engine_cells(spec))
         _check_sorted(cell_of, order, cell_start, nc)
+
+
+def _uniform_spec(n, box, seed, cutoff=2.5, skin=0.3):
+    spec = workloads.lj_lattice()
+    rng = np.random.default_rng(seed)
+    spec.positions = (rng.uniform(0.0, 1.0, (n, 3)) * np.asarray(box)).astype(np.float32)
+    spec.box_bound = np.array([[0.0, 0.0, 0.0], box], np.float32)
+    spec.cutoff, spec.cutoff_buffer = cutoff, skin
+    return spec
+
+
+@pytest.mark.parametrize("case", ["crowded_3", "two_cells", "outside", "huge_cells"])
+def test_static_cell_sort_matches_oracle_on_edge_grids(oracle, case):
+    if case == "crowded_3":
+        spec = _uniform_spec(2700, (8.5, 8.5, 8.5), 3)      # 3^3 cells, ~100 per cell
+    elif case == "two_cells":
+        spec = _uniform_spec(500, (6.0, 6.0, 6.0), 4)       # 2^3 cells (direct grid)
+    elif case == "outside":
+        spec = _uniform_spec(3000, (12.0, 12.0, 12.0), 5)
+        lo, hi = np.float32(0.0), np.float32(12.0)
+        # beads just below lo and at or just above hi on each axis (clamped)
+        spec.positions[:6, 0] = [np.nextafter(lo, np.float32(-1)), -1e-3, hi,
+                                 np.nextafter(hi, np.float32(13)), 12.5, -0.7]
+        spec.positions[6:12, 1] = spec.positions[:6, 0]
+        spec.positions[12:18, 2] = spec.positions[:6, 0]
+    else:
+        spec = _uniform_spec(80000, (6.0, 6.0, 6.0), 6)     # 2^3 cells of ~10,000
+    cell_of, order, cell_start, nc = _static_sort(spec)
+    expect = oracle.cell_ids(spec.positions, spec.box_bound, spec.cutoff, spec.cutoff_buffer)
+    assert np.array_equal(cell_of, expect)
+    _check_sorted(cell_of, order, cell_start, nc)
+    if case in ("crowded_3", "huge_cells"):
+        assert np.diff(cell_start).max() > (8192 if case == "huge_cells" else 32)
+    # a second call on the same input gives the same bits (counters cleared)
+    again = _static_sort(spec)
+    assert all(np.array_equal(a, b) for a, b in zip((cell_of, order, cell_start), again[:3]))
 
 
 def test_static_cell_sort_rejects_grids_beyond_the_maximum():
