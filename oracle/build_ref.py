@@ -14,13 +14,23 @@ sm_100a, in two precisions, and links
 Each module exposes the reference's ``build_info()`` and
 ``execute_simulation(spec)``; load it with ``oracle.ref.load(precision)``.
 
-    python oracle/build_ref.py <reference checkout> [--jobs 8]
+Beside each module it links ``_ref_neighbors`` from ``oracle/ref_neighbors.cu``
+(a checker of this repository) with the same reference objects, minus the
+reference's PYBIND11_MODULE translation unit: ``neighbor_dump(spec)`` returns
+the list the reference's own NeighborSystem builds for a spec.
+
+    python oracle/build_ref.py [<reference checkout>] [--jobs 8]
+
+Without an argument the checkout is $BEADS_REFERENCE_SRC, else the path this
+recipe was written against (/root/reference); when neither exists the recipe
+prints why and builds nothing.
 """
 
 from __future__ import annotations
 
 import argparse
 import concurrent.futures
+import os
 import pathlib
 import subprocess
 import sys
@@ -74,15 +84,54 @@ def build(ref: pathlib.Path, precision: str, jobs: int) -> pathlib.Path:
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(r.stderr[-4000:])
+    build_harness(ref, precision, objdir, [o for o in objs if o.name != "bindings__module.cpp.o"])
     return target
+
+
+def build_harness(ref: pathlib.Path, precision: str, objdir: pathlib.Path,
+                  objs: list[pathlib.Path]) -> pathlib.Path:
+    """Links oracle/ref_neighbors.cu against the reference's objects."""
+    defines = ["-DBEADS_REAL64"] if precision == "f64" else []
+    src = HERE / "ref_neighbors.cu"
+    obj = objdir / "harness__ref_neighbors.cu.o"
+    suffix = sysconfig.get_config_var("EXT_SUFFIX") or ".so"
+    target = OUT / precision / f"_ref_neighbors{suffix}"
+    if not (obj.exists() and obj.stat().st_mtime >= src.stat().st_mtime):
+        cmd = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
+               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", *defines, *includes(ref),
+               "-c", str(src), "-o", str(obj)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"{src}:\n{r.stderr[-4000:]}")
+    cmd = ["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler",
+           "-fPIC", str(obj), *map(str, objs), "-lpthread", "-o", str(target)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-4000:])
+    return target
+
+
+def default_reference() -> pathlib.Path:
+    return pathlib.Path(os.environ.get("BEADS_REFERENCE_SRC", "/root/reference"))
+
+
+def built() -> bool:
+    """True when both precisions' _native and _ref_neighbors modules exist."""
+    return all(list((OUT / p).glob(f"{m}*.so")) for p in ("f32", "f64")
+               for m in ("_native", "_ref_neighbors"))
 
 
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__)
-    parser.add_argument("reference", type=pathlib.Path)
+    parser.add_argument("reference", type=pathlib.Path, nargs="?", default=None)
     parser.add_argument("--jobs", type=int, default=8)
     parser.add_argument("--precision", choices=["f32", "f64", "both"], default="both")
     args = parser.parse_args()
+    if args.reference is None:
+        args.reference = default_reference()
+        if not (args.reference / "native" / "src").is_dir():
+            print(f"reference checkout not found at {args.reference}; checker modules not built")
+            return
     for p in (["f32", "f64"] if args.precision == "both" else [args.precision]):
         print(build(args.reference.resolve(), p, args.jobs))
     sys.stdout.flush()

@@ -6,6 +6,7 @@ so each run happens in a fresh subprocess that loads exactly one of them.
 
     python -m oracle.ref <f32|f64> <spec.json> <spec.npz> <workdir>
     python -m oracle.ref <f32|f64> --many <root> <count>
+    python -m oracle.ref <f32|f64> --neighbors <spec.json> <spec.npz> <out.npz>
 
 runs ``_native.execute_simulation(spec)`` with ``workdir`` as the current
 directory (the spec's output prefixes are relative to it); ``--many`` runs
@@ -96,6 +97,31 @@ def run(precision: str, spec: dict, workdir: pathlib.Path, timeout: float = 1800
                     str(workdir)], check=True, env=env, timeout=timeout)
 
 
+def harness_path(precision: str) -> pathlib.Path:
+    found = glob.glob(str(HERE / "_ref" / precision / "_ref_neighbors*.so"))
+    if not found:
+        raise FileNotFoundError(f"reference neighbour harness for {precision} is not built "
+                                "(python oracle/build_ref.py <reference checkout>)")
+    return pathlib.Path(found[0])
+
+
+def neighbors(precision: str, spec: dict, workdir: pathlib.Path,
+              timeout: float = 1800.0) -> dict:
+    """The reference engine's own neighbour list after its initial build for
+    `spec` (oracle/ref_neighbors.cu), computed in a subprocess: counts[n] and
+    partners[n][max_neighbors] in tag order, overflow, path, excluded_pairs."""
+    workdir = pathlib.Path(workdir)
+    workdir.mkdir(parents=True, exist_ok=True)
+    jp, npz, out = workdir / "spec.json", workdir / "spec.npz", workdir / "neighbors.npz"
+    save_spec(spec, jp, npz)
+    env = dict(os.environ)
+    env["PYTHONPATH"] = str(ROOT) + os.pathsep + env.get("PYTHONPATH", "")
+    subprocess.run([sys.executable, "-m", "oracle.ref", precision, "--neighbors", str(jp),
+                    str(npz), str(out)], check=True, env=env, timeout=timeout)
+    with np.load(out) as data:
+        return {k: data[k] for k in data.files}
+
+
 def run_many(precision: str, specs: list[dict], workdir: pathlib.Path,
              timeout: float = 3600.0) -> list[pathlib.Path]:
     """Runs every spec in turn in ONE subprocess (one module load); spec k runs
@@ -123,6 +149,17 @@ def _prepare(spec: dict, precision: str) -> dict:
 
 
 def main(argv: list[str]) -> None:
+    if len(argv) == 5 and argv[1] == "--neighbors":
+        precision, _, jp, npz, out = argv
+        spec = _prepare(load_spec(pathlib.Path(jp), pathlib.Path(npz)), precision)
+        hs = importlib.util.spec_from_file_location("_ref_neighbors", harness_path(precision))
+        mod = importlib.util.module_from_spec(hs)
+        hs.loader.exec_module(mod)
+        d = mod.neighbor_dump(spec)
+        np.savez(out, counts=d["counts"], partners=d["partners"], overflow=d["overflow"],
+                 path=np.array(d["path"]), excluded_pairs=d["excluded_pairs"],
+                 builds=d["builds"])
+        return
     if len(argv) == 4 and argv[1] == "--many":
         precision, _, root, count = argv
         mod = _load(precision)
