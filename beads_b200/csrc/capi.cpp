@@ -3,6 +3,7 @@
 #include <chrono>
 #include <memory>
 #include <cstring>
+#include <functional>
 #include <iomanip>
 #include <sstream>
 #include <string>
@@ -175,8 +176,13 @@ void execute_run(const beads_run_desc& run) {
 
   engine.eval();
   emit(0, true);
+  // The reference polls for an interrupt every max(1, 100000 / N) steps
+  // (simulation_run.cpp:92); here the poll runs at the first chunk boundary
+  // (chunks hold at most 16 steps) at or after each such interval, inside
+  // Engine::run, and once before the final outputs.
   const uint64_t check_interval = std::max<uint64_t>(1, 100000 / std::max<uint32_t>(1, sys.n_particles));
-  uint64_t last_check = 0;
+  std::function<bool()> poll;
+  if (run.interrupt) poll = [&] { return run.interrupt(run.interrupt_user) != 0; };
   while (engine.step() < run.runsteps) {
     const uint64_t s = engine.step();
     uint64_t next = run.runsteps;
@@ -184,15 +190,14 @@ void execute_run(const beads_run_desc& run) {
     if (traj) next = std::min(next, (s / run.trajectory_every + 1) * run.trajectory_every);
     const uint64_t target = next;
     const bool obs_at_target = thermo && target % run.thermo_every == 0;
-    // Interrupt polling between chunks.
-    if (run.interrupt && (s - last_check) >= check_interval) {
-      last_check = s;
-      if (run.interrupt(run.interrupt_user)) throw std::runtime_error("interrupted");
-    }
-    engine.run(target - s, obs_at_target ? target : 0);
+    engine.run(target - s, obs_at_target ? target : 0, run.interrupt ? &poll : nullptr,
+               check_interval);
     emit(target, obs_at_target);
+    if (run.interrupt && engine.step() < run.runsteps && poll()) {
+      throw std::runtime_error("interrupted");
+    }
   }
-  if (run.interrupt && run.runsteps > 0 && run.interrupt(run.interrupt_user)) {
+  if (run.interrupt && run.runsteps > 0 && poll()) {
     throw std::runtime_error("interrupted");
   }
   if (final_state) {

@@ -224,6 +224,10 @@ Engine::~Engine() {
   for (void* p : allocations_) cudaFree(p);
   if (h_obs_) cudaFreeHost(h_obs_);
   if (h_state_) cudaFreeHost(h_state_);
+  if (h_chunk_status_) cudaFreeHost(h_chunk_status_);
+  for (cudaEvent_t e : chunk_event_) {
+    if (e) cudaEventDestroy(e);
+  }
   if (side_stream_) cudaStreamDestroy(side_stream_);
   if (stream_) cudaStreamDestroy(stream_);
 }
@@ -604,6 +608,10 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
 
   cuda_check(cudaMallocHost(&h_obs_, n * sizeof(ReplicaObs)), "cudaMallocHost");
   cuda_check(cudaMallocHost(&h_state_, n * sizeof(ReplicaState)), "cudaMallocHost");
+  cuda_check(cudaMallocHost(&h_chunk_status_, 2 * n * sizeof(unsigned)), "cudaMallocHost");
+  for (cudaEvent_t& e : chunk_event_) {
+    cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event create");
+  }
 
   launch_.v = v;
   launch_.stream = stream_;
@@ -772,12 +780,25 @@ void Engine::launch_chunk(uint32_t steps, bool obs_last) {
   }
 }
 
-bool Engine::run(uint64_t steps, uint64_t obs_every) {
+bool Engine::run(uint64_t steps, uint64_t obs_every, const std::function<bool()>* poll,
+                 uint64_t poll_every) {
   TraceRange trace("beads.run");
   if (!initialized_) eval();
   if (!tuned_ && !tuning_fixed_ && steps > 0) autotune();
+  const uint32_t n = n_replicas();
   bool last_obs = false;
   uint64_t remaining = steps;
+  uint64_t chunks = 0;
+  uint64_t last_poll = step_;
+  // Status words of a finished chunk: any bit set means the step that set it
+  // failed; check_status() (full download, reference message) then throws.
+  auto chunk_failed = [&](uint64_t k) {
+    const unsigned* w = h_chunk_status_ + (k & 1u) * n;
+    for (uint32_t r = 0; r < n; ++r) {
+      if (w[r] != 0u) return true;
+    }
+    return false;
+  };
   while (remaining > 0) {
     uint64_t chunk = std::min<uint64_t>(remaining, kChunkMax);
     bool obs = false;
@@ -797,9 +818,29 @@ bool Engine::run(uint64_t steps, uint64_t obs_every) {
       obs = false;
     }
     launch_chunk(static_cast<uint32_t>(chunk), obs);
+    // This chunk's status words, gathered from the replica states (one
+    // strided copy), land in its half of the pinned ring.
+    const uint64_t k = chunks++;
+    cuda_check(cudaMemcpy2DAsync(h_chunk_status_ + (k & 1u) * n, sizeof(unsigned), &v_.rs->status,
+                                 sizeof(ReplicaState), sizeof(unsigned), n,
+                                 cudaMemcpyDeviceToHost, stream_),
+               "status copy");
+    cuda_check(cudaEventRecord(chunk_event_[k & 1u], stream_), "event record");
     step_ += chunk;
     remaining -= chunk;
     last_obs = obs;
+    if (k > 0) {
+      cuda_check(cudaEventSynchronize(chunk_event_[(k - 1) & 1u]), "status wait");
+      if (chunk_failed(k - 1)) check_status();
+    }
+    if (poll != nullptr && remaining > 0 && step_ - last_poll >= poll_every) {
+      last_poll = step_;
+      if ((*poll)()) {
+        sync();
+        check_status();
+        throw std::runtime_error("interrupted");  // BEADS_ERR_INTERRUPTED
+      }
+    }
   }
   check_status();
   return last_obs;

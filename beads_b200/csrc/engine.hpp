@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -71,7 +72,18 @@ class Engine {
   void eval();
   // Advance `steps`; observables on multiples of obs_every (0 = never).
   // Returns true if the last step was an observable step.
-  bool run(uint64_t steps, uint64_t obs_every);
+  //
+  // The steps run as captured chunks of at most 16.  After launching chunk
+  // k the host reads the status words that chunk k - 1 left (a pinned copy
+  // queued behind it, so the device keeps chunk k to work on) and raises the
+  // error of a replica whose list overflowed, whose energy left the
+  // fixed-point range or whose velocities became non-finite: at most one
+  // chunk after the step that failed.  `poll`, when given, is called at the
+  // first chunk boundary at or after every `poll_every` steps; a true return
+  // stops the run with std::runtime_error("interrupted") once the queued
+  // chunks have drained.
+  bool run(uint64_t steps, uint64_t obs_every, const std::function<bool()>* poll = nullptr,
+           uint64_t poll_every = 1);
   void minimize(uint32_t iterations, float dmax, float fref);
 
   void observables(std::vector<beads_observables>& out);
@@ -183,6 +195,8 @@ class Engine {
   std::map<uint32_t, std::pair<cudaGraph_t, cudaGraphExec_t>> replay_graphs_;
   ReplicaObs* h_obs_ = nullptr;        // pinned
   ReplicaState* h_state_ = nullptr;    // pinned
+  unsigned* h_chunk_status_ = nullptr; // pinned, [2][n_replicas]: status words after a chunk
+  cudaEvent_t chunk_event_[2] = {nullptr, nullptr};
   float* d_xfer_pos_ = nullptr;        // tag-order staging (lazily allocated)
   float* d_xfer_vel_ = nullptr;
   std::vector<uint32_t> host_row_tag_;  // per replica concatenated (global tag idx)
