@@ -16,7 +16,15 @@ Arms:
   default            the CUDA engine through its C ABI.
   --impl reference   the reference's algorithm on the host cores (the CPU
                      oracle port: the reference has no CPU implementation of
-                     this path), bounded sample of the same workload.
+                     this path) on the same workload, relaxed the same way on
+                     the host; its line also carries the reference's own CUDA
+                     build timed on the same relaxed input (`reference_cuda`).
+
+`--gpus N` (N > 1) without a launcher re-executes this script under
+torch.distributed.run with N local ranks on 127.0.0.1.  The mixture then runs
+one replica per GPU ("weak"); `--workload replicas` and `--workload adjoint`
+split one replica batch over the ranks by atom count ("strong"), the adjoint
+summing its parameter gradients and loss over the ranks (NCCL all-reduce).
 """
 
 from __future__ import annotations
@@ -38,11 +46,21 @@ ROOT = pathlib.Path(__file__).resolve().parent
 if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
-METRIC = "atom-steps/s on 1 B200 (1M-bead binary LJ mixture, FP32 pair math, fixed-point totals)"
 UNIT = "atom-steps/s"
 N_BEADS = 1_048_576
 E2E_STEPS = 100  # MD steps per end-to-end call
 GRAPH_WARMUP = 31  # untimed steps that instantiate every captured step graph
+CLOCK_WINDOW_S = 0.6  # shortest stretch of load the clock sampler sees
+WORKLOAD = ("binary LJ mixture, 1,048,576 beads per GPU, nm_kjmol, 80/20 types, box 37.2 nm, "
+            "rc 0.9 (shifted), skin 0.1, max_neighbors 128, sort every rebuild, Berendsen 120 K "
+            "tau 0.1, dt 0.002, seeded uniform start relaxed by 500 capped steepest-descent "
+            "steps")
+L2_NOTE = "inputs larger than L2 (list ~4*mean_nbr*N bytes + state ~100 B per bead)"
+
+
+def metric(world: int) -> str:
+    return (f"atom-steps/s on {world} B200 (1M-bead binary LJ mixture per GPU, FP32 pair "
+            "math, fixed-point totals)")
 
 
 def _dist():
@@ -50,6 +68,20 @@ def _dist():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
+
+
+def _launch_ranks(gpus: int) -> None:
+    """Re-executes this command under torch.distributed.run with `gpus` local
+    ranks when no launcher set WORLD_SIZE (does not return)."""
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           str(pathlib.Path(__file__).resolve()), *sys.argv[1:]]
+    os.execv(sys.executable, cmd)
 
 
 def _peaks():
@@ -120,6 +152,20 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
                 "samples": len(self.rows)}
+
+
+def _load_until(eng, since: float, window_s: float = CLOCK_WINDOW_S) -> int:
+    """Keeps the GPU stepping (untimed) until `window_s` seconds have passed
+    since `since`, so a 200 ms clock sampler sees the kernels under load even
+    when the timed steps take a few milliseconds.  Returns the extra steps."""
+    import torch
+
+    extra = 0
+    while time.perf_counter() - since < window_s:
+        eng.run(16)
+        torch.cuda.synchronize()
+        extra += 16
+    return extra
 
 
 def _prepare_engine(local_rank: int, n_beads: int = N_BEADS):
@@ -216,55 +262,69 @@ def _cpu_baseline_melt(spec, budget_s: float):
                       f"step), {wall:.1f} s of host work, FP64 oracle with OpenMP"}
 
 
-def _lattice_mixture(n_side: int):
-    """The workload's mixture (same density, composition, parameters) on a
-    jittered n_side^3 simple-cubic lattice: no overlaps, so the CPU arm needs
-    no relaxation (its cost is set by pair counts, not by overlaps)."""
+def _relaxed_on_host(seed: int = 3):
+    """The workload's input prepared on the host cores: the same seeded
+    uniform start relaxed by the same 500 capped steepest-descent steps
+    (x += 0.004 nm F / max(|F|, 200), LJ on r^2 >= 0.49 sigma^2), in the CPU
+    oracle's FP64 restatement instead of the GPU engine.  Returns the spec (with
+    the relaxed positions) and the oracle state ready to step."""
     from beads_b200 import workloads
 
-    n = n_side ** 3
-    box = (n / (N_BEADS / 37.2 ** 3)) ** (1 / 3)
-    spec = workloads.lj_mixture(n=n, box=box, seed=3)
-    a = box / n_side
-    g = np.indices((n_side,) * 3).reshape(3, -1).T.astype(np.float64)
-    rng = np.random.default_rng(3)
-    pos = (((g + 0.5) * a + rng.uniform(-0.02, 0.02, g.shape)) % box).astype(np.float32)
-    spec.positions = pos
-    return spec
+    spec = workloads.lj_mixture(n=N_BEADS, box=37.2, seed=seed)
+    sim, _ = _cpu_sim(spec, spec.positions, spec.n)
+    sim.minimize(500, 0.004, 200.0)
+    pos, _, img, _ = sim.state()
+    spec.positions = workloads._inside(pos, np.zeros(3), np.full(3, 37.2))
+    spec.images = img
+    return spec, sim
 
 
 def run_reference(args) -> None:
+    """The reference's algorithm for this path on the host cores: the CPU
+    oracle port (FP64, OpenMP on every host thread; the reference itself has
+    no CPU implementation) on the whole 1,048,576-bead workload, one MD step
+    per bench step with the reference's rebuild policy.  Beside it, the
+    reference's own CUDA build on the same relaxed input through its
+    execute_simulation, timed by its log (`reference_cuda`; outside `value`)."""
     world, rank, _ = _dist()
     if rank != 0:
         return
     from oracle import oracle as O
 
-    # Each bench step is one MD step (with the reference's rebuild policy) of
-    # a lattice-started copy of the workload, sized so warm-up + steps take
-    # about args.ref_budget seconds of host work.
-    probe_spec = _lattice_mixture(40)
-    probe, n_probe = _cpu_sim(probe_spec, probe_spec.positions, probe_spec.n)
-    probe.step(1)
-    rate, _ = _cpu_rate(probe, n_probe, 2)
-    probe.close()
-    per_step = args.ref_budget / (args.steps + args.warmup)
-    n_target = min(N_BEADS, max(8192, rate * per_step))
-    spec = _lattice_mixture(max(20, int(round(n_target ** (1 / 3)))))
-    sim, n = _cpu_sim(spec, spec.positions, spec.n)
+    t_prep = time.perf_counter()
+    spec, sim = _relaxed_on_host()
+    prep_s = time.perf_counter() - t_prep
     for _ in range(args.warmup):
         sim.step(1)
+    builds0 = sim.state()[3]
     t0 = time.perf_counter()
     for _ in range(args.steps):
         sim.step(1)
     total = time.perf_counter() - t0
+    builds = sim.state()[3] - builds0
     sim.close()
+    n = spec.n
     value = n * args.steps / total
     cores = O.num_threads()
-    sample = (f"{n}-bead copy of the mixture (same density and parameters, jittered-lattice "
-              f"start), one MD step per bench step")
+    sample = (f"the whole {n}-bead workload, relaxed on the host ({prep_s:.0f} s, untimed), "
+              f"{args.warmup} warm-up + {args.steps} timed MD steps, {builds} neighbour "
+              "rebuilds in the timed steps; FP64 oracle port with OpenMP")
+    reference_cuda = None
+    if not args.no_reference_cuda:
+        try:
+            from oracle import ref_bench
+
+            # The reference's steps_per_second covers its whole run, the
+            # initial build included, so it runs long enough for steady state.
+            reference_cuda = ref_bench.reference_engine_rate(spec, args.reference_cuda_steps)
+            reference_cuda.update(
+                unit=UNIT, build="the reference's own sources compiled for sm_100a, float32 "
+                "(oracle/build_ref.py), same relaxed spec, its execute_simulation and log timer")
+        except Exception as e:  # noqa: BLE001 - reported, not fatal
+            reference_cuda = {"unavailable": f"{type(e).__name__}: {e}"[:300]}
     line = {
         "impl": "reference",
-        "metric": METRIC,
+        "metric": metric(world),
         "value": value,
         "unit": UNIT,
         "n_gpus": world,
@@ -276,13 +336,45 @@ def run_reference(args) -> None:
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "binary LJ mixture, 1,048,576 beads, nm_kjmol, rc 0.9, skin 0.1, "
-                               "Berendsen 120 K", "sampled_beads": n},
+        "config": {"workload": WORKLOAD, "l2": L2_NOTE},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "run": {"neighbor_builds_timed": int(builds), "host_relaxation_s": prep_s},
+        "reference_cuda": reference_cuda,
     }
     print(json.dumps(line))
+
+
+def _energy_drift(spec, eng, steps: int = 2000, every: int = 100) -> dict:
+    """Energy drift of the workload's dynamics: an NVE copy (Berendsen off,
+    which would otherwise add or remove energy) of the engine's current state
+    runs `steps` steps with a thermo row every `every` steps; the drift is the
+    least-squares slope of the total energy per bead against time."""
+    import dataclasses
+
+    from beads_b200 import workloads
+    from beads_b200.engine import Engine
+
+    st = eng.state()
+    box = np.asarray(spec.box_bound, np.float64)
+    nve = dataclasses.replace(
+        spec, thermostat=None, images=st["images"],
+        positions=workloads._inside(st["positions"].astype(np.float64), box[0], box[1]),
+        velocities=st["velocities"])
+    with Engine(nve) as e:
+        rows = [e.eval()[0]]
+        for _ in range(steps // every):
+            rows.append(e.run(every, every)[0])
+    etot = np.array([r["pe"] + r["ke"] for r in rows], np.float64) / spec.n
+    t_ns = np.arange(len(rows)) * every * spec.dt / 1000.0  # dt in ps
+    slope = float(np.polyfit(t_ns, etot, 1)[0])
+    return {"value": slope, "unit": "kJ/mol per bead per ns", "steps": steps,
+            "dt_ps": spec.dt, "e_total_per_bead_start": float(etot[0]),
+            "e_total_per_bead_end": float(etot[-1]),
+            "relative_change": float((etot[-1] - etot[0]) / abs(etot[0])),
+            "ensemble": "NVE copy (Berendsen off) of the engine state after the timed steps, "
+                        "float32 pair math, fixed-point totals"}
 
 
 def run_ours(args) -> None:
@@ -323,6 +415,7 @@ def run_ours(args) -> None:
     sampler = ClockSampler(local)
     barrier()
     sampler.start()
+    t_sample = time.perf_counter()
     if profile_region:  # lets a profiler started with capture off see only these steps
         torch.cuda.profiler.start()
     start = torch.cuda.Event(enable_timing=True)
@@ -333,9 +426,13 @@ def run_ours(args) -> None:
     stop.synchronize()
     if profile_region:
         torch.cuda.profiler.stop()
+    c1 = eng.counters()
+    # The clock record covers at least CLOCK_WINDOW_S of the same stepping
+    # (untimed steps after the timed ones); the value is the timed steps'.
+    clock_extra_steps = 0 if profile_region else _load_until(eng, t_sample)
     barrier()
     clocks = sampler.stop()
-    c1 = eng.counters()
+    clocks["untimed_steps_after_timed"] = clock_extra_steps
     timed_builds = c1["builds"] - c0["builds"]
     timed_chains = c1["chain_launches"] - c0["chain_launches"]
     elapsed_ms = start.elapsed_time(stop)
@@ -380,8 +477,11 @@ def run_ours(args) -> None:
         e2e_wall = float(t.item())
     if e2e_calls:
         e2e_value = world * spec.n * E2E_STEPS * e2e_calls / e2e_wall
-    h2d = 2 * spec.n * 3 * 4
-    d2h = 2 * spec.n * 3 * 4
+    # Bytes copied per call (positions + velocities in, the same out), per MD step.
+    h2d = 2 * spec.n * 3 * 4 / E2E_STEPS
+    d2h = 2 * spec.n * 3 * 4 / E2E_STEPS
+
+    drift = None if args.no_drift else _energy_drift(spec, eng)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -395,7 +495,7 @@ def run_ours(args) -> None:
     per_step = 4 if eng.tuning()["fuse_post"] else 5
     gpu_launches = per_step * args.steps + 7 * int(timed_chains)
     line = {
-        "metric": METRIC,
+        "metric": metric(world),
         "value": value,
         "unit": UNIT,
         "n_gpus": world,
@@ -407,11 +507,9 @@ def run_ours(args) -> None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {
-            "workload": "binary LJ mixture, 1,048,576 beads per GPU, nm_kjmol, rc 0.9 (shifted), "
-                        "skin 0.1, max_neighbors 128, Berendsen 120 K tau 0.1, dt 0.002",
+        "config": {"workload": WORKLOAD, "l2": L2_NOTE},
+        "run": {
             "parallelism": f"replicas x{world}",
-            "l2": "inputs larger than L2 (list ~4*mean_nbr*N bytes + state)",
             "mean_neighbors": round(mean_nbr, 2),
             "max_neighbors_seen": stats["max"],
             "neighbor_builds_timed": int(timed_builds),
@@ -431,10 +529,15 @@ def run_ours(args) -> None:
             "kernel_ms": force_ms,
         },
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "md_steps_per_call": E2E_STEPS},
+                "d2h_bytes_per_step": d2h, "md_steps_per_call": E2E_STEPS,
+                "calls": e2e_calls,
+                "call": "beads_upload_all (pinned host positions + velocities) -> "
+                        "beads_run(100) -> beads_download_all, per call"},
         "gpu_launches": gpu_launches,
         "clocks": clocks,
     }
+    if drift is not None:
+        line["energy_drift"] = drift
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if rank == 0:
@@ -444,34 +547,56 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
-REPLICA_METRIC = ("atom-steps/s on 1 B200 (512-replica batch of uneven LJ systems in one launch "
-                  "per kernel, FP32 pair math, fixed-point totals)")
+def replica_metric(world: int) -> str:
+    return (f"atom-steps/s on {world} B200 (512-replica batch of uneven LJ systems in one launch "
+            "per kernel per GPU, FP32 pair math, fixed-point totals)")
+
+
+def _init_nccl(world: int):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return dist
 
 
 def run_replicas(args) -> None:
     """The 512-replica batch: uneven single-type LJ replicas (sizes seeded
     log-uniform in [256, 32768], density U[0.7, 0.9], Berendsen target T
     U[0.8, 1.5] tau 1, rc 2.5, dt 0.005) stepped together, beside the same
-    replicas run one at a time through the same engine."""
+    replicas run one at a time through the same engine.  With several ranks
+    the one batch is split over them by atom count (every rank builds the same
+    description and keeps its share); the time is the slowest rank's."""
     import torch
 
     from beads_b200 import workloads
+    from beads_b200.distributed import max_over_ranks, shard_replicas, sum_over_ranks
     from beads_b200.engine import Engine
 
     world, rank, local = _dist()
     torch.cuda.set_device(local)
-    specs = workloads.replica_batch(args.replicas, seed=7 + rank)
+    dist = _init_nccl(world)
+    dev = torch.device("cuda", local)
+    all_specs = workloads.replica_batch(args.replicas, seed=7)
+    total_atoms = sum(s.n for s in all_specs)
+    _, specs = shard_replicas(all_specs, world, rank)
     atoms = sum(s.n for s in specs)
     eng = Engine(specs)
-    stream = torch.cuda.ExternalStream(eng.info()["stream"], device=torch.device("cuda", local))
+    stream = torch.cuda.ExternalStream(eng.info()["stream"], device=dev)
     eng.run(max(3, args.warmup))
     eng.run(GRAPH_WARMUP)
     builds_before = sum(eng.counters(r)["builds"] for r in range(len(specs)))
     chains_before = eng.counters()["chain_launches"]
     profile_region = os.environ.get("BEADS_PROFILE_TIMED") == "1"
     sampler = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
     torch.cuda.synchronize()
     sampler.start()
+    t_sample = time.perf_counter()
     if profile_region:  # lets a profiler started with capture off see only these steps
         torch.cuda.profiler.start()
     start = torch.cuda.Event(enable_timing=True)
@@ -482,17 +607,20 @@ def run_replicas(args) -> None:
     stop.synchronize()
     if profile_region:
         torch.cuda.profiler.stop()
-    clocks = sampler.stop()
-    batch_ms = start.elapsed_time(stop)
     builds = sum(eng.counters(r)["builds"] for r in range(len(specs))) - builds_before
     chains = eng.counters()["chain_launches"] - chains_before
+    extra = 0 if profile_region else _load_until(eng, t_sample)
+    clocks = sampler.stop()
+    clocks["untimed_steps_after_timed"] = extra
+    batch_ms = max_over_ranks(start.elapsed_time(stop), dev)
+    builds = int(sum_over_ranks(builds, dev))
     schedule = eng.tuning()
-    value = atoms * args.steps / (batch_ms / 1e3)
+    value = total_atoms * args.steps / (batch_ms / 1e3)
     eng.close()
 
     # The same replicas one at a time (one engine each, same kernels), every
     # replica for `seq_steps` steps after warm-up; the sequential rate is the
-    # total atom-steps over the summed device time.
+    # total atom-steps over the summed device time (slowest rank's sum).
     seq_steps = max(10, min(args.steps, 200))
     seq_ms = 0.0
     for spec in specs:
@@ -507,9 +635,12 @@ def run_replicas(args) -> None:
             b.record(s1)
             b.synchronize()
             seq_ms += a.elapsed_time(b)
-    seq_value = atoms * seq_steps / (seq_ms / 1e3)
+    seq_ms = max_over_ranks(seq_ms, dev)
+    seq_value = total_atoms * seq_steps / (seq_ms / 1e3)
+    if dist is not None:
+        dist.destroy_process_group()
     line = {
-        "metric": REPLICA_METRIC,
+        "metric": replica_metric(world),
         "value": value,
         "unit": UNIT,
         "n_gpus": world,
@@ -517,14 +648,17 @@ def run_replicas(args) -> None:
         "warmup": args.warmup,
         "ms_per_step": batch_ms / args.steps,
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong",
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
         "config": {
-            "workload": f"{len(specs)} LJ replicas, {atoms} beads in total, sizes log-uniform "
-                        "[256, 32768], rho U[0.7, 0.9], Berendsen T U[0.8, 1.5], rc 2.5, skin 0.3",
-            "parallelism": "replicas in one batch",
+            "workload": f"{len(all_specs)} LJ replicas, {total_atoms} beads in total, sizes "
+                        "log-uniform [256, 32768], rho U[0.7, 0.9], Berendsen T U[0.8, 1.5], "
+                        "rc 2.5, skin 0.3",
+            "parallelism": (f"one batch split over {world} GPUs by atom count"
+                            if world > 1 else "replicas in one batch"),
+            "beads_per_rank_this_rank": atoms,
             "sequential_value": seq_value,
             "sequential_steps_per_replica": seq_steps,
             "batch_over_sequential": value / seq_value,
@@ -541,7 +675,7 @@ def run_replicas(args) -> None:
 
 
 CHAINS_METRIC = ("atom-steps/s on 1 B200 (400,000-bead bead-spring melt: WCA pairs, harmonic "
-                 "bonds, angles and dihedrals, 1-2/1-3 exclusions)")
+                 "bonds, angles and dihedrals, 1-2/1-3 exclusions; one system, one GPU)")
 
 
 def run_chains(args) -> None:
@@ -616,8 +750,9 @@ def run_chains(args) -> None:
     print(json.dumps(line))
 
 
-ADJOINT_METRIC = ("differentiated atom-steps/s on 1 B200 (64 x 8192-bead LJ mixture, forward "
-                  "with checkpoints + adjoint backward, FP32 pair math)")
+def adjoint_metric(world: int) -> str:
+    return (f"differentiated atom-steps/s on {world} B200 (64 x 8192-bead LJ mixture, forward "
+            "with checkpoints + adjoint backward, FP32 pair math)")
 
 
 def run_adjoint(args) -> None:
@@ -633,17 +768,26 @@ def run_adjoint(args) -> None:
     from beads_b200.adjoint import trajectory_observables
     from beads_b200.engine import Engine
 
+    from beads_b200.distributed import max_over_ranks, reduce_gradients, shard_replicas
+
     world, rank, local = _dist()
     torch.cuda.set_device(local)
+    dist = _init_nccl(world)
+    dev = torch.device("cuda", local)
     steps, every = args.adj_steps, 50
     window = min(200, steps)
-    specs = workloads.fit_mixture(n_replicas=64, n=8192, seed=21 + rank)
-    atoms = sum(s.n for s in specs)
+    # One 64-replica fit, split over the ranks by atom count; the targets are
+    # drawn for the whole batch, each rank keeps its replicas' entries.
+    all_specs = workloads.fit_mixture(n_replicas=64, n=8192, seed=21)
+    rng = np.random.default_rng(5)
+    pe_all = rng.uniform(-6.0, -5.0, len(all_specs)) * 8192
+    p_all = rng.uniform(0.5, 1.5, len(all_specs))
+    mine, specs = shard_replicas(all_specs, world, rank)
+    total_atoms = sum(s.n for s in all_specs)
     vols = torch.tensor([float(np.prod(np.asarray(s.box_bound[1], np.float64) - s.box_bound[0]))
                          for s in specs])
-    rng = np.random.default_rng(5 + rank)
-    pe_t = torch.tensor(rng.uniform(-6.0, -5.0, len(specs)) * 8192)
-    p_t = torch.tensor(rng.uniform(0.5, 1.5, len(specs)))
+    pe_t = torch.tensor(pe_all[mine])
+    p_t = torch.tensor(p_all[mine])
     x0 = torch.tensor(np.concatenate([s.positions for s in specs]), dtype=torch.float64)
     v0 = torch.tensor(np.concatenate([s.velocities for s in specs]), dtype=torch.float64)
     eps = torch.tensor(workloads.MIXTURE_EPS, dtype=torch.float64, requires_grad=True)
@@ -676,9 +820,15 @@ def run_adjoint(args) -> None:
         press = ((2.0 * obs[:, :, 2] + obs[:, :, 1]) / (3.0 * vols)).mean(0)
         loss = ((pe - pe_t) ** 2 + (press - p_t) ** 2).sum()
         loss.backward()
+        # eps and sigma are shared by every replica of every rank: sum the
+        # ranks' gradients (and losses) with one all-reduce.
+        loss_total = loss.detach().clone().reshape(1)
+        reduce_gradients([eps.grad, sig.grad, loss_total], dev)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
-    fwd_s, bwd_s = t1 - t0, t2 - t1
+    fwd_s = max_over_ranks(t1 - t0, dev)
+    bwd_s = max_over_ranks(t2 - t1, dev)
+    plain_s = max_over_ranks(plain_s, dev)
     # The same gradient with every step's state kept by the forward pass
     # (checkpoint_every = 0, no replay): the memory-for-compute trade that
     # HBM affords at this size ((steps + 1) x 32 B per particle).
@@ -698,18 +848,25 @@ def run_adjoint(args) -> None:
         pe2 = obs2[:, :, 0].mean(0)
         press2 = ((2.0 * obs2[:, :, 2] + obs2[:, :, 1]) / (3.0 * vols)).mean(0)
         ((pe2 - pe_t) ** 2 + (press2 - p_t) ** 2).sum().backward()
+        reduce_gradients([eps2.grad, sig2.grad], dev)
         torch.cuda.synchronize()
         t5 = time.perf_counter()
+    stored_fwd = max_over_ranks(t4 - t3, dev)
+    stored_bwd = max_over_ranks(t5 - t4, dev)
+    x_grad_sq = torch.tensor([float(x.grad.norm()) ** 2], dtype=torch.float64)
+    reduce_gradients([x_grad_sq], dev)
+    if dist is not None:
+        dist.destroy_process_group()
     line = {
-        "metric": ADJOINT_METRIC,
-        "value": atoms * steps / (fwd_s + bwd_s),
+        "metric": adjoint_metric(world),
+        "value": total_atoms * steps / (fwd_s + bwd_s),
         "unit": UNIT,
         "n_gpus": world,
         "steps": steps,
         "warmup": args.warmup,
         "ms_per_step": 1e3 * (fwd_s + bwd_s) / steps,
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong",
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
@@ -717,18 +874,22 @@ def run_adjoint(args) -> None:
             "workload": "64 x 8192-bead binary LJ mixture (reduced, rho 0.8, T 1, Berendsen tau 1, "
                         f"dt 0.005), {steps} steps, loss over the last {window} steps, checkpoint "
                         f"every {every}",
+            "parallelism": (f"one batch split over {world} GPUs by atom count, gradients "
+                            "all-reduced" if world > 1 else "replicas in one batch"),
             "plain_forward_s": plain_s,
             "adjoint_forward_s": fwd_s,
             "backward_s": bwd_s,
             "backward_over_plain_forward": bwd_s / plain_s,
             "forward_plus_backward_over_plain_forward": (fwd_s + bwd_s) / plain_s,
-            "stored_forward_s": t4 - t3,
-            "stored_backward_s": t5 - t4,
-            "stored_backward_over_plain_forward": (t5 - t4) / plain_s,
-            "loss": float(loss.detach()),
+            "stored_forward_s": stored_fwd,
+            "stored_backward_s": stored_bwd,
+            "stored_backward_over_plain_forward": stored_bwd / plain_s,
+            "loss": float(loss_total.item()),
             "grad_eps": eps.grad.tolist(),
             "grad_sigma": sig.grad.tolist(),
-            "grad_x0_norm": float(x.grad.norm()),
+            "grad_eps_stored": eps2.grad.tolist(),
+            "grad_sigma_stored": sig2.grad.tolist(),
+            "grad_x0_norm": float(x_grad_sq.item()) ** 0.5,
         },
     }
     if rank == 0:
@@ -738,15 +899,18 @@ def run_adjoint(args) -> None:
 def main() -> None:
     parser = argparse.ArgumentParser(description=__doc__)
     parser.add_argument("--gpus", type=int, default=1)
-    parser.add_argument("--steps", type=int, default=2000)
-    parser.add_argument("--warmup", type=int, default=20)
+    parser.add_argument("--steps", type=int, default=200)
+    parser.add_argument("--warmup", type=int, default=10)
     parser.add_argument("--impl", default="ours", choices=["ours", "reference"])
     parser.add_argument("--cpu-budget", type=float, default=15.0,
                         help="seconds of host work for the cpu_baseline sample")
-    parser.add_argument("--ref-budget", type=float, default=90.0,
-                        help="seconds of host work for the whole reference arm")
+    parser.add_argument("--no-reference-cuda", action="store_true",
+                        help="reference arm: skip timing the reference's own CUDA build")
+    parser.add_argument("--reference-cuda-steps", type=int, default=2000,
+                        help="reference arm: MD steps of the reference CUDA build's run")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    parser.add_argument("--no-drift", action="store_true", help="skip the energy-drift run")
     parser.add_argument("--adj-steps", type=int, default=1000)
     parser.add_argument("--workload", default="mixture",
                         choices=["mixture", "replicas", "adjoint", "chains"],
@@ -760,6 +924,11 @@ def main() -> None:
     args = parser.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        _launch_ranks(args.gpus)
+    world = _dist()[0]
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but the launcher started {world} ranks")
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "replicas":

@@ -218,6 +218,9 @@ struct FF {
   const double* dihedral_k;
   const int32_t* dihedral_d;
   const int32_t* dihedral_n;
+  // Steepest-descent form only: LJ evaluated on r^2 clamped to at least
+  // clamp_sig2 * sigma^2 (0 = the plain pair force).
+  double clamp_sig2 = 0.0;
 };
 
 struct Out {
@@ -258,7 +261,8 @@ void pair_forces(uint32_t n, const float* pos, const int32_t* types, const Box& 
       const int tj = types[j] - 1;
       const double eps = ff.eps[ti * ff.ntypes + tj];
       const double sig = ff.sig[ti * ff.ntypes + tj];
-      const double r2 = dot(d, d);
+      double r2 = dot(d, d);
+      if (ff.clamp_sig2 > 0.0) r2 = std::max(r2, ff.clamp_sig2 * sig * sig);
       const double sr2 = sig * sig / r2;
       const double sr6 = sr2 * sr2 * sr2;
       const double sr12 = sr6 * sr6;
@@ -653,6 +657,55 @@ void* orc_sim_create(uint32_t n, const double* pos, const double* vel, const dou
 }
 
 void orc_sim_destroy(void* sim) { delete static_cast<OracleSim*>(sim); }
+
+// Capped steepest descent of the state's positions (velocities untouched),
+// the engine's relaxation of random starts restated in double: per iteration
+// forces at the current positions with LJ on r^2 clamped to >= 0.49 sigma^2,
+// every particle moved by dmax * F / max(|F|, fref), wrapped, and the list
+// rebuilt when a displacement since the last build exceeds skin / 2.
+// Afterwards the list and the plain forces are rebuilt and the step and build
+// counters restart, as for a fresh run.
+void orc_sim_minimize(void* sim, uint32_t iterations, double dmax, double fref) {
+  auto* s = static_cast<OracleSim*>(sim);
+  s->ff.clamp_sig2 = 0.49;
+  s->rebuild();
+  for (uint32_t it = 0; it < iterations; ++it) {
+    s->forces();
+    const Box& box = s->box;
+#pragma omp parallel for
+    for (int64_t i = 0; i < static_cast<int64_t>(s->n); ++i) {
+      const double fx = s->f[3 * i], fy = s->f[3 * i + 1], fz = s->f[3 * i + 2];
+      const double fn = std::sqrt(fx * fx + fy * fy + fz * fz);
+      const double k = dmax / std::max(fn, fref);
+      if (!std::isfinite(k) || !std::isfinite(fn)) continue;
+      for (int a = 0; a < 3; ++a) {
+        double& x = s->pos[3 * i + a];
+        x += k * s->f[3 * i + a];
+        const double c = std::floor((x - box.lo[a]) / box.len[a]);
+        x -= c * box.len[a];
+        s->img[3 * i + a] += static_cast<int32_t>(c);
+      }
+    }
+    int exceeded = 0;
+#pragma omp parallel for reduction(| : exceeded)
+    for (int64_t i = 0; i < static_cast<int64_t>(s->n); ++i) {
+      double d2 = 0;
+      for (int a = 0; a < 3; ++a) {
+        const double d = s->pos[3 * i + a] - s->ref[3 * i + a] +
+                         static_cast<double>(s->img[3 * i + a] - s->ref_img[3 * i + a]) *
+                             box.len[a];
+        d2 += d * d;
+      }
+      exceeded |= d2 > s->thr ? 1 : 0;
+    }
+    if (exceeded) s->rebuild();
+  }
+  s->ff.clamp_sig2 = 0.0;
+  s->rebuild();
+  s->forces();
+  s->builds = 0;
+  s->step = 0;
+}
 
 // Advances `steps`; writes the observables of the last force evaluation:
 // [step, pair, bond, angle, dihedral, ke, virial] (ke after Berendsen).

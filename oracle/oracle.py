@@ -73,6 +73,8 @@ def _declare(L) -> None:
     L.orc_sim_destroy.restype = None
     L.orc_sim_step.argtypes = [c.c_void_p, c.c_uint64, _f64p]
     L.orc_sim_step.restype = None
+    L.orc_sim_minimize.argtypes = [c.c_void_p, c.c_uint32, c.c_double, c.c_double]
+    L.orc_sim_minimize.restype = None
     L.orc_sim_state.argtypes = [c.c_void_p, _f64p, _f64p, _i32p, c.POINTER(c.c_uint64)]
     L.orc_sim_state.restype = None
     L.orc_num_threads.argtypes = []
@@ -254,6 +256,11 @@ class Sim:
         obs = np.zeros(7, np.float64)
         lib().orc_sim_step(self._h, int(steps), obs)
         return obs
+
+    def minimize(self, iterations: int, dmax: float, fref: float) -> None:
+        """Capped steepest descent of the positions (the engine's relaxation
+        of random starts, in double); counters restart afterwards."""
+        lib().orc_sim_minimize(self._h, int(iterations), float(dmax), float(fref))
 
     def state(self):
         pos = np.zeros(3 * self.n, np.float64)

@@ -47,6 +47,19 @@ def _relaxed_mixture(n: int):
     return spec
 
 
+def reference_engine_rate(r, steps: int) -> dict:
+    """The reference engine's own float32 build on replica `r` through its
+    execute_simulation (a thermo row at the end only), timed by its own log
+    (steps_per_second: wall time of the whole run, initial build included).
+    Returns the steps, its steps/s and atom-steps/s."""
+    spec = spec_for(r, steps, "run", forces=False, thermo_every=steps)
+    with tempfile.TemporaryDirectory() as tmp:
+        tmp = pathlib.Path(tmp)
+        ref.run("f32", spec, tmp / "ref")
+        sps = _sps(tmp / "ref" / "run.log")
+    return {"steps": steps, "steps_per_second": sps, "atom_steps_per_s": sps * r.n}
+
+
 def _replica_batch(steps: int, count: int) -> dict:
     """The uneven 512-replica batch: the reference engine one replica at a
     time (its own timer per run, summed) against one batched beads_b200 engine
