@@ -1,6 +1,6 @@
 """Times one stage of the step on a named workload, for profilers.
 
-    python -m beads_b200.stage_profile --workload fit-mixture --beads 524288 \
+    python -m tests.stage_profile --workload fit-mixture --beads 524288 \
         --stage rebuild --reps 1
 
 Builds the workload, runs ``--warm`` MD steps, then calls
@@ -26,13 +26,18 @@ def _workload(name: str, beads: int):
         return workloads.lj_lattice(n_side=side)
     if name == "replicas":
         return workloads.replica_batch(512)
+    if name == "melt":
+        # the bead-spring melt benchmark's input: chains of 200, grown in
+        # lockstep and relaxed (beads // 200 chains)
+        return workloads.relaxed(workloads.polymer_melt(n_chains=max(1, beads // 200), seed=5,
+                                                        growth="lockstep"))
     raise ValueError(f"unknown workload {name!r}")
 
 
 def main(argv: list[str] | None = None) -> dict:
     parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     parser.add_argument("--workload", default="fit-mixture",
-                        choices=["fit-mixture", "lattice", "replicas"])
+                        choices=["fit-mixture", "lattice", "replicas", "melt"])
     parser.add_argument("--beads", type=int, default=524288)
     parser.add_argument("--stage", default="rebuild",
                         choices=["forces", "forces_kick", "rebuild", "step"])

@@ -4,7 +4,7 @@ from __future__ import annotations
 
 import pytest
 
-from beads_b200 import stage_profile
+from tests import stage_profile
 
 pytestmark = pytest.mark.gpu
 
