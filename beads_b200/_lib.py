@@ -160,6 +160,8 @@ EXPORTED = (
     "beads_counters",
     "beads_set_tuning",
     "beads_get_tuning",
+    "beads_set_list_layout",
+    "beads_get_list_layout",
     "beads_set_lj",
     "beads_adjoint_forward",
     "beads_adjoint_backward",
@@ -211,6 +213,8 @@ def load():
     L.beads_counters.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)]
     L.beads_set_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
     L.beads_get_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+    L.beads_set_list_layout.argtypes = [vp, ctypes.c_int32]
+    L.beads_get_list_layout.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
     L.beads_set_lj.argtypes = [vp, ctypes.c_uint32, vp, vp]
     L.beads_adjoint_forward.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, vp]
     L.beads_adjoint_backward.argtypes = [vp, vp, vp, vp, vp, vp]

@@ -705,6 +705,9 @@ void Engine::adjoint_forward(uint64_t steps, uint64_t record_from, uint32_t ever
   int max_types = 0;
   for (const auto& h : rep_) max_types = std::max(max_types, h.n_types);
   if (max_types > kAdjTypes) throw InvalidArgument("the adjoint supports up to 4 particle types.");
+  // The adjoint pair kernel reads slot rows of slot entries: leave the staged
+  // list layout (same forward bits, the list is rebuilt in slot layout).
+  set_list_staged(false);
 
   if (!adj_) adj_ = std::make_unique<AdjointStore>();
   AdjointStore& A = *adj_;

@@ -400,6 +400,20 @@ int beads_get_tuning(beads_ctx* ctx, int32_t* schedule) {
   });
 }
 
+int beads_set_list_layout(beads_ctx* ctx, int32_t staged) {
+  return guarded([&] {
+    require(ctx && ctx->engine, "NULL argument.");
+    ctx->engine->set_list_staged(staged != 0);
+  });
+}
+
+int beads_get_list_layout(beads_ctx* ctx, int32_t* staged) {
+  return guarded([&] {
+    require(ctx && ctx->engine && staged, "NULL argument.");
+    *staged = ctx->engine->list_staged() ? 1 : 0;
+  });
+}
+
 int beads_set_lj(beads_ctx* ctx, uint32_t replica, const double* epsilon, const double* sigma) {
   return guarded([&] {
     require(ctx && ctx->engine && epsilon && sigma, "NULL argument.");

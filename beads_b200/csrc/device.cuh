@@ -81,6 +81,7 @@ struct ReplicaParams {
   uint32_t lj_offset;        // first entry of this replica's LJ table
   int32_t n_types;
   uint32_t bond_type_base, angle_type_base, dihedral_type_base;
+  uint32_t staged;           // pair forces from a shared-memory stage (kernels.cu)
 };
 
 // Mutable per-replica device state.
@@ -198,6 +199,11 @@ struct DeviceView {
   long long* ke_part;            // [replica][kKeBuckets][whole, frac] kinetic-energy buckets
   const LjCoeff* lj;
   uint32_t n_replicas;
+  // Staged context: list rows (and counts) by cell-order index of the last
+  // build, entries of staged groups are stage indices; stage_cap is the
+  // stage capacity in entries of a group (shared memory of k_lj_staged).
+  int list_by_q;
+  uint32_t stage_cap;
   uint32_t n_slots;
   uint32_t n_blocks;
   uint32_t total_cells;

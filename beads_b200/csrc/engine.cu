@@ -170,12 +170,16 @@ void Engine::autotune() {
       chosen = l;
     }
   };
-  try {
-    // The pair-force shape first (second half-kick as its own kernel), then
-    // the best shape with the kick fused.
+  // The pair-force shape first (second half-kick as its own kernel), then
+  // the best shape with the kick fused.  The staged kernel has no L1 policy
+  // choice (its neighbour positions are in shared memory).
+  auto tune_layout = [&]() {
+    best = 0.f;
+    const bool staged_now = v_.list_by_q != 0;
     for (int tpa : {1, 2, 4}) {
       for (int unroll : {8, 4}) {
         for (int no_l1 : {0, 1}) {
+          if (staged_now && no_l1 == 0) continue;
           StepLaunch l = launch_;
           l.lj_tpa = tpa;
           l.lj_unroll = unroll;
@@ -188,6 +192,32 @@ void Engine::autotune() {
     StepLaunch fused = chosen;
     fused.fuse_post = 1;
     trial(fused);
+  };
+  try {
+    tune_layout();
+    // Both list layouts when the context can stage: the other layout is
+    // built from the same positions (relayout_list) and tuned the same way.
+    if (stage_cap_ > 0) {
+      const float best_first = best;
+      const StepLaunch chosen_first = chosen;
+      const bool first_staged = v_.list_by_q != 0;
+      v_.list_by_q = first_staged ? 0 : 1;
+      launch_.v = v_;
+      relayout_list();
+      tune_layout();
+      if (log) {
+        std::fprintf(stderr, "beads autotune: staged layout %.4f ms, slot layout %.4f ms\n",
+                     (first_staged ? best_first : best) / kReps,
+                     (first_staged ? best : best_first) / kReps);
+      }
+      if (best_first <= best) {
+        best = best_first;
+        chosen = chosen_first;
+        v_.list_by_q = first_staged ? 1 : 0;
+        launch_.v = v_;
+        relayout_list();
+      }
+    }
   } catch (...) {
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -200,10 +230,8 @@ void Engine::autotune() {
   cuda_check(cudaMemcpyAsync(v_.rs, saved.data(), saved.size() * sizeof(ReplicaState),
                              cudaMemcpyHostToDevice, stream_), "state restore");
   sync();
-  if (chosen.lj_tpa != launch_.lj_tpa || chosen.fuse_post != launch_.fuse_post ||
-      chosen.lj_unroll != launch_.lj_unroll || chosen.lj_no_l1 != launch_.lj_no_l1) {
-    clear_graphs();
-  }
+  // Captured graphs hold the kernels of one schedule and one layout.
+  clear_graphs();
   launch_.lj_tpa = chosen.lj_tpa;
   launch_.lj_unroll = chosen.lj_unroll;
   launch_.lj_no_l1 = chosen.lj_no_l1;
@@ -335,6 +363,31 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
     bonds += s.n_bonds;
     angles += s.n_angles;
     dihedrals += s.n_dihedrals;
+  }
+  // Cell-tile staging of the pair forces (kernels.cu, stage_layout): a
+  // replica with >= 4 cells on every axis stages its groups of 128 particles.
+  // A group's stage is 9 stencil rows of the home cells plus one cell on each
+  // side per home row: about 9 (128 + 5 m) entries for m particles per cell
+  // when the group spans two rows; the capacity adds a quarter for density
+  // fluctuations (a group beyond it keeps slot entries).  Replicas that would
+  // need more than kStageMaxEntries (crowded cells) are not staged.
+  // BEADS_STAGED=0 turns staging off for every context of the process.
+  {
+    constexpr uint32_t kStageMaxEntries = 8192;  // 128 KiB of shared memory
+    bool enabled = true;
+    if (const char* e = std::getenv("BEADS_STAGED")) enabled = std::string(e) != "0";
+    uint32_t cap = 0;
+    for (uint32_t r = 0; r < n; ++r) {
+      const ReplicaHost& h = rep_[r];
+      const bool regular = h.plan.nc[0] >= 4 && h.plan.nc[1] >= 4 && h.plan.nc[2] >= 4;
+      const double occ = static_cast<double>(h.n_atoms) / std::max<uint32_t>(1, h.plan.n_cells);
+      const double need = 1.25 * 9.0 * (static_cast<double>(kBlock) + 5.0 * occ);
+      const uint32_t want = static_cast<uint32_t>((std::ceil(need) + 255.0) / 256.0) * 256u;
+      rp[r].staged = (enabled && regular && want <= kStageMaxEntries) ? 1u : 0u;
+      if (rp[r].staged) cap = std::max(cap, want);
+    }
+    stage_cap_ = cap;
+    staged_ = cap > 0;
   }
   n_tags_ = tags;
   total_bond_types_ = static_cast<uint32_t>(bond_types);
@@ -511,6 +564,8 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   v.nbr_stride = stride;
   v.excl_cap = static_cast<uint32_t>(excl_cap);
   v.has_bonded = any_bonded ? 1 : 0;
+  v.list_by_q = staged_ ? 1 : 0;
+  v.stage_cap = stage_cap_;
   v.pos = dalloc<float4>(S + 1);
   v.vel = dalloc<float4>(S);
   v.force = dalloc<float4>(S);
@@ -628,6 +683,7 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   launch_.max_atoms_per_replica = max_atoms;
   launch_.excl_cap = excl_cap;
   launch_.need_kinetic = any_thermostat ? 1 : 0;
+  if (staged_) prepare_staged_kernels(static_cast<size_t>(stage_cap_ + 1) * sizeof(float4));
   // Initial slot-space exclusion rows (slot order = input order).
   launch_project_exclusions(launch_, true);
   cuda_check(cudaStreamSynchronize(stream_), "setup");
@@ -1108,7 +1164,66 @@ void Engine::debug_cells(uint32_t r, uint32_t* cell_by_tag) {
   }
 }
 
+void Engine::set_list_staged(bool staged) {
+  const bool want = staged && stage_cap_ > 0;
+  if ((v_.list_by_q != 0) == want) return;
+  clear_graphs();
+  v_.list_by_q = want ? 1 : 0;
+  launch_.v = v_;
+  if (initialized_) relayout_list();
+}
+
+// Rebuilds the current list in the current layout from the positions of the
+// last build (ref_pos), without counting a build or reordering: the same
+// cells, the same candidates in the same order, so the same list.  The
+// displacement reference (images and crossing counts since that build) and
+// the positions are restored afterwards, so the dynamics continue bit for
+// bit as they would have without the change.
+void Engine::relayout_list() {
+  const size_t S = v_.n_slots;
+  float4* save_pos = nullptr;
+  int4* save_img = nullptr;
+  uint32_t* save_cross = nullptr;
+  cuda_check(cudaMalloc(&save_pos, S * sizeof(float4)), "cudaMalloc");
+  cudaError_t e1 = cudaMalloc(&save_img, S * sizeof(int4));
+  cudaError_t e2 = cudaMalloc(&save_cross, S * sizeof(uint32_t));
+  try {
+    cuda_check(e1, "cudaMalloc");
+    cuda_check(e2, "cudaMalloc");
+    auto d2d = [&](void* dst, const void* src, size_t bytes) {
+      cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream_), "copy");
+    };
+    d2d(save_pos, v_.pos, S * sizeof(float4));
+    d2d(save_img, v_.ref_img, S * sizeof(int4));
+    d2d(save_cross, v_.cross, S * sizeof(uint32_t));
+    d2d(v_.pos, v_.ref_pos, S * sizeof(float4));
+    std::vector<ReplicaState> saved(rep_.size());
+    sync();
+    cuda_check(cudaMemcpy(saved.data(), v_.rs, saved.size() * sizeof(ReplicaState),
+                          cudaMemcpyDeviceToHost), "state save");
+    launch_rebuild(launch_, true, false);
+    d2d(v_.pos, save_pos, S * sizeof(float4));
+    d2d(v_.ref_img, save_img, S * sizeof(int4));
+    d2d(v_.cross, save_cross, S * sizeof(uint32_t));
+    cuda_check(cudaMemcpyAsync(v_.rs, saved.data(), saved.size() * sizeof(ReplicaState),
+                               cudaMemcpyHostToDevice, stream_), "state restore");
+    sync();
+  } catch (...) {
+    cudaFree(save_pos);
+    if (save_img) cudaFree(save_img);
+    if (save_cross) cudaFree(save_cross);
+    throw;
+  }
+  cudaFree(save_pos);
+  cudaFree(save_img);
+  cudaFree(save_cross);
+}
+
 void Engine::debug_neighbors(uint32_t r, uint32_t cap, uint32_t* counts, uint32_t* partners) {
+  if (v_.list_by_q) {
+    debug_neighbors_staged(r, cap, counts, partners);
+    return;
+  }
   const ReplicaHost& h = rep_.at(r);
   sync();
   const uint32_t S = v_.n_slots;
@@ -1128,6 +1243,45 @@ void Engine::debug_neighbors(uint32_t r, uint32_t cap, uint32_t* counts, uint32_
     for (uint32_t q = 0; q < c && q < cap; ++q) {
       const uint64_t at = nbr_index(slot, q, v_.nbr_stride) - g0 * per_group;
       const uint32_t j = list[at];
+      partners[static_cast<uint64_t>(t) * cap + q] = tag[j] - h.tag_base + 1;
+    }
+  }
+}
+
+// Staged contexts keep list rows by cell order and stage indices as entries:
+// a device pass decodes them into a slot-indexed copy of neighbour slots.
+void Engine::debug_neighbors_staged(uint32_t r, uint32_t cap, uint32_t* counts,
+                                    uint32_t* partners) {
+  const ReplicaHost& h = rep_.at(r);
+  sync();
+  const uint32_t S = v_.n_slots;
+  uint32_t* d_count = nullptr;
+  uint32_t* d_list = nullptr;
+  cuda_check(cudaMalloc(&d_count, S * 4ull), "cudaMalloc");
+  cuda_check(cudaMalloc(&d_list, static_cast<size_t>(S) * cap * 4ull), "cudaMalloc");
+  std::vector<uint32_t> cnt(S), tag(S), list(static_cast<size_t>(h.n_atoms) * cap);
+  try {
+    cuda_check(cudaMemsetAsync(d_count, 0, S * 4ull, stream_), "memset");
+    launch_list_to_slots(launch_, cap, d_count, d_list);
+    sync();
+    cuda_check(cudaMemcpy(cnt.data(), d_count, S * 4ull, cudaMemcpyDeviceToHost), "d2h");
+    cuda_check(cudaMemcpy(list.data(), d_list + static_cast<size_t>(h.atom_begin) * cap,
+                          list.size() * 4ull, cudaMemcpyDeviceToHost), "d2h");
+    cuda_check(cudaMemcpy(tag.data(), v_.tag, S * 4ull, cudaMemcpyDeviceToHost), "d2h");
+  } catch (...) {
+    cudaFree(d_count);
+    cudaFree(d_list);
+    throw;
+  }
+  cudaFree(d_count);
+  cudaFree(d_list);
+  for (uint32_t k = 0; k < h.n_atoms; ++k) {
+    const uint32_t slot = h.atom_begin + k;
+    const uint32_t t = tag[slot] - h.tag_base;
+    const uint32_t c = cnt[slot];
+    counts[t] = c;
+    for (uint32_t q = 0; q < c && q < cap; ++q) {
+      const uint32_t j = list[static_cast<size_t>(k) * cap + q];
       partners[static_cast<uint64_t>(t) * cap + q] = tag[j] - h.tag_base + 1;
     }
   }

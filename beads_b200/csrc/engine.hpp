@@ -101,6 +101,14 @@ class Engine {
   void download_all(float* pos, float* vel);
   void debug_cells(uint32_t r, uint32_t* cell_by_tag);
   void debug_neighbors(uint32_t r, uint32_t cap, uint32_t* counts, uint32_t* partners);
+  // Pair forces from shared-memory cell tiles (list rows by cell order, stage
+  // indices as entries) or from global gathers (rows by slot, slot entries).
+  // Contexts start staged when some replica qualifies; switching rebuilds the
+  // list before the next force evaluation.  Results are the same bits.
+  void set_list_staged(bool staged);
+  bool list_staged() const { return v_.list_by_q != 0; }
+  void debug_neighbors_staged(uint32_t r, uint32_t cap, uint32_t* counts, uint32_t* partners);
+  void relayout_list();
   uint64_t step() const { return step_; }
   bool initialized() const { return initialized_; }
   // Applies a pending Berendsen scale to the velocities (state reads).
@@ -188,6 +196,8 @@ class Engine {
   bool use_graphs_ = true;
   bool use_conditional_ = true;
   uint32_t total_bond_types_ = 0, total_angle_types_ = 0, total_dihedral_types_ = 0;
+  bool staged_ = false;                // some replica stages its pair forces
+  uint32_t stage_cap_ = 0;             // stage entries per group (k_lj_staged)
   bool tuning_fixed_ = false;          // set_tuning() with an explicit choice
   bool tuned_ = false;                 // autotune() has run
   cudaStream_t side_stream_ = nullptr;

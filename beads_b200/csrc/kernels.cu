@@ -462,12 +462,127 @@ k_project_exclusions(DeviceView v, int force_all) {
 constexpr int kBuildWarps = kBlock / 32;
 constexpr uint32_t kMaxSegments = 27;
 
+// ---------------------------------------------------------------------------
+// Cell-tile staging of the pair-force kernel.
+//
+// In a staged context the list of a particle is stored in ROW q, its index in
+// the cell order of the last build (cell_atoms[q] is its slot), and a
+// "group" is 128 consecutive rows: the particles of k_lj_staged's block.  The
+// home cells of a group are one contiguous run of cell indices; the group's
+// STAGE is the union of their stencils, laid out as windows: for every home
+// row (a run of cells of one x-row, at most kStageRows of them) and every one
+// of its 9 stencil rows, the cells [xa - 1, xb + 2) of that row, cut in two
+// where they wrap in x (or the whole row when that is shorter).  A window is
+// a contiguous run of cell-order indices, so the stage holds
+// pos[cell_atoms[q]] for q in every window, one after another; the force
+// kernel copies it into shared memory once per step.  A list entry of a
+// staged group is the neighbour's stage index (q + delta of its window); a
+// group whose stage would exceed the context's capacity, or whose home cells
+// span more rows, keeps slot entries and gathers positions from global
+// memory instead.  The build and the force kernel derive the layout from the
+// same cell_start by the same function, so they agree on it.
+constexpr uint32_t kStageRows = 3;                      // home rows per group at most
+constexpr uint32_t kStageWindows = 2 * 9 * kStageRows;  // 54
+struct StageLayout {
+  uint32_t n_win;                  // windows (0: the group keeps slot entries)
+  uint32_t size;                   // stage entries
+  uint32_t row_first;              // replica-local row (y + ny z) of the first home cell
+  uint32_t q_first, q_end;         // rows of the group's particles
+  uint32_t qbeg[kStageWindows];    // cell-order index of a window's first entry
+  uint32_t base[kStageWindows];    // its stage index
+  uint32_t x0[kStageWindows];      // x-range of its cells
+  uint32_t x1[kStageWindows];
+};
+
+// Fills `lay` for group g (one full warp; lay is the warp's shared scratch).
+// Only replicas with the staged flag and grids of >= 4 cells on every axis
+// are staged: their stencil rows are distinct and their segments never wrap
+// inside a window.
+__device__ __forceinline__ void stage_layout(const DeviceView& v, const ReplicaParams& p,
+                                             uint32_t g, uint32_t lane, uint32_t cap,
+                                             StageLayout& lay) {
+  const uint32_t q_lo = max(g * (uint32_t)kBlock, p.atom_begin);
+  const uint32_t q_hi = min((g + 1u) * (uint32_t)kBlock, p.atom_begin + p.n_atoms);
+  const uint32_t nx = p.nc[0], ny = p.nc[1], nz = p.nc[2];
+  bool ok = p.staged != 0u && q_lo < q_hi && nx >= 4u && ny >= 4u && nz >= 4u;
+  uint32_t cf = 0, cl = 0;
+  if (ok) {
+    cf = v.cell_of_slot[v.cell_atoms[q_lo]] - p.cell_begin;
+    cl = v.cell_of_slot[v.cell_atoms[q_hi - 1u]] - p.cell_begin;
+  }
+  const uint32_t rf = cf / nx, rl = cl / nx;
+  const uint32_t nsub = ok ? rl - rf + 1u : 0u;
+  ok = ok && nsub <= kStageRows;
+  // lane l < 9 nsub: home row rf + l / 9, stencil row l % 9 (z-major, as the
+  // build walks it); two windows per lane.
+  uint32_t qa0 = 0, qa1 = 0, qb0 = 0, qb1 = 0, xa0 = 0, xa1 = 0, xb0 = 0, xb1 = 0;
+  if (ok && lane < 9u * nsub) {
+    const uint32_t sub = lane / 9u, k = lane % 9u;
+    const uint32_t row = rf + sub;
+    const uint32_t y = row % ny, z = row / ny;
+    const uint32_t xa = sub == 0u ? cf % nx : 0u;
+    const uint32_t xb = sub + 1u == nsub ? cl % nx : nx - 1u;
+    const uint32_t yy = stencil_cell(y, ny, k % 3u), zz = stencil_cell(z, nz, k / 3u);
+    const uint32_t rowbase = nx * (yy + ny * zz);
+    if (xb - xa + 3u >= nx) {
+      xa0 = 0u, xa1 = nx;
+    } else if (xa == 0u) {
+      xa0 = nx - 1u, xa1 = nx, xb0 = 0u, xb1 = xb + 2u;
+    } else if (xb == nx - 1u) {
+      xa0 = xa - 1u, xa1 = nx, xb0 = 0u, xb1 = 1u;
+    } else {
+      xa0 = xa - 1u, xa1 = xb + 2u;
+    }
+    const uint32_t* start = v.cell_start + p.start_base;
+    qa0 = start[rowbase + xa0];
+    qa1 = start[rowbase + xa1];
+    if (xb1 > xb0) {
+      qb0 = start[rowbase + xb0];
+      qb1 = start[rowbase + xb1];
+    }
+  }
+  const uint32_t len = (qa1 - qa0) + (qb1 - qb0);
+  uint32_t inc = len;
+#pragma unroll
+  for (uint32_t o = 1; o < 32u; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kFull, inc, o);
+    if (lane >= o) inc += t;
+  }
+  const uint32_t total = __shfl_sync(kFull, inc, 31);
+  ok = ok && total <= cap;
+  __syncwarp();
+  if (lane < 9u * kStageRows) {
+    const uint32_t b = inc - len;
+    lay.qbeg[2 * lane] = qa0;
+    lay.base[2 * lane] = b;
+    lay.x0[2 * lane] = xa0;
+    lay.x1[2 * lane] = xa1;
+    lay.qbeg[2 * lane + 1] = qb0;
+    lay.base[2 * lane + 1] = b + (qa1 - qa0);
+    lay.x0[2 * lane + 1] = xb0;
+    lay.x1[2 * lane + 1] = xb1;
+  }
+  if (lane == 0) {
+    lay.n_win = ok ? 18u * nsub : 0u;
+    lay.size = ok ? total : 0u;
+    lay.row_first = rf;
+    lay.q_first = q_lo;
+    lay.q_end = q_hi;
+  }
+  __syncwarp();
+}
+
 struct BuildShared {
   uint32_t seg_end[kMaxSegments];  // stream offset one past the segment
   uint32_t seg_q[kMaxSegments];    // cell_atoms index of the segment's stream offset 0
   float seg_s[3][kMaxSegments];    // periodic shift of the segment (regular grids)
   float4 home_a[32];               // {x, x, y, y} of the home particles
   float4 home_b[32];               // {z, z, slot bits, 0}
+  // Staged contexts: the home particles in flight belong to one group; a
+  // candidate's entry is its cell-order index + delta[segment] when that
+  // group is staged, else its slot.
+  uint32_t delta[kMaxSegments];
+  StageLayout lay;
 };
 
 enum BuildForm : int { kBuildInterior = 0, kBuildShifted = 1, kBuildMinImage = 2 };
@@ -476,6 +591,7 @@ enum BuildForm : int { kBuildInterior = 0, kBuildShifted = 1, kBuildMinImage = 2
 // stream positions base + 64 q + lane (.x) and base + 64 q + 32 + lane (.y).
 struct CandPair {
   uint32_t jx, jy;       // slots (0xffffffff past the stream)
+  uint32_t ex, ey;       // list entries: stage indices in a staged group, else the slots
   float2 nx, ny, nz;     // minus their coordinates
   float2 sx, sy, sz;     // periodic shifts of their segments
 };
@@ -549,15 +665,16 @@ __device__ __forceinline__ void build_chunk(const DeviceView& v, const ReplicaPa
       }
     }
     uint32_t k = __shfl_sync(kFull, my_cnt, h);
-    uint32_t* row = v.nbr + nbr_index(i, 0, v.nbr_stride);
+    // The list row: the slot, or in a staged context the cell-order index.
+    uint32_t* row = v.nbr + nbr_index(__float_as_uint(hb.w), 0, v.nbr_stride);
 #pragma unroll
     for (int q = 0; q < kBuildPairs; ++q) {
       const uint32_t kx = k + __popc(bx[q] & lt);
       k += __popc(bx[q]);
       const uint32_t ky = k + __popc(by[q] & lt);
       k += __popc(by[q]);
-      if (ax[q] && kx < cap) row[(size_t)kx * kGroup] = c[q].jx;
-      if (ay[q] && ky < cap) row[(size_t)ky * kGroup] = c[q].jy;
+      if (ax[q] && kx < cap) row[(size_t)kx * kGroup] = c[q].ex;
+      if (ay[q] && ky < cap) row[(size_t)ky * kGroup] = c[q].ey;
     }
     if (lane == h) my_cnt = k;
   }
@@ -579,9 +696,11 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
   // Segment table: lane s describes segment s.
   uint32_t q0 = 0u, q1 = 0u;
   float shx = 0.0f, shy = 0.0f, shz = 0.0f;
+  uint32_t seg_lo = 0u, seg_k = 0u;  // x of the segment's first cell, its stencil row
   if (regular) {
     if (lane < 18u) {
       const uint32_t a = lane / 6u, bb = (lane / 2u) % 3u, sg = lane & 1u;
+      seg_k = 3u * a + bb;
       const uint32_t zc = stencil_cell(cz, nz, a), yc = stencil_cell(cy, ny, bb);
       shz = (cz == 0u && a == 0u) ? p.len[2] : (cz == nz - 1u && a == 2u) ? -p.len[2] : 0.0f;
       shy = (cy == 0u && bb == 0u) ? p.len[1] : (cy == ny - 1u && bb == 2u) ? -p.len[1] : 0.0f;
@@ -600,6 +719,7 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
         q0 = start[row + lo];
         q1 = start[row + hi];
       }
+      seg_lo = lo;
     }
   } else {
     const uint32_t sxn = min(nx, 3u), syn = min(ny, 3u), szn = min(nz, 3u);
@@ -633,9 +753,25 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
                        : kBuildInterior;
   const uint32_t nseg = regular ? 18u : kMaxSegments;
   bool any_overflow = false;
+  const bool by_q = v.list_by_q != 0;
+  const bool staged_replica = by_q && p.staged != 0u && regular;
 
-  for (uint32_t i0 = cs; i0 < ce; i0 += 32u) {
-    const uint32_t nh = min(32u, ce - i0);
+  // In a staged context the home particles in flight never span two groups
+  // (128 cell-order rows), so one stage layout serves all of them.
+  for (uint32_t i0 = cs, i1 = 0; i0 < ce; i0 = i1) {
+    i1 = min(i0 + 32u, ce);
+    if (staged_replica) i1 = min(i1, (i0 / (uint32_t)kBlock + 1u) * (uint32_t)kBlock);
+    const uint32_t nh = i1 - i0;
+    bool staged_group = false;
+    if (staged_replica) {
+      stage_layout(v, p, i0 / (uint32_t)kBlock, lane, v.stage_cap, sh.lay);
+      staged_group = sh.lay.n_win != 0u;
+      if (staged_group && lane < 18u) {
+        const uint32_t w0 = 2u * (((cy + ny * cz) - sh.lay.row_first) * 9u + seg_k);
+        const uint32_t w = (sh.lay.x0[w0] <= seg_lo && seg_lo < sh.lay.x1[w0]) ? w0 : w0 + 1u;
+        sh.delta[lane] = sh.lay.base[w] - sh.lay.qbeg[w];
+      }
+    }
     uint32_t i = 0u;
     float4 xi = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncwarp();
@@ -643,7 +779,8 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
       i = v.cell_atoms[i0 + lane];
       xi = v.pos2[i0 + lane];
       sh.home_a[lane] = make_float4(xi.x, xi.x, xi.y, xi.y);
-      sh.home_b[lane] = make_float4(xi.z, xi.z, __uint_as_float(i), 0.0f);
+      sh.home_b[lane] = make_float4(xi.z, xi.z, __uint_as_float(i),
+                                    __uint_as_float(by_q ? i0 + lane : i));
     }
     __syncwarp();
     uint32_t my_cnt = 0u;
@@ -657,20 +794,22 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
         // Past the stream: an infinite coordinate fails every distance test.
         uint32_t j = 0xffffffffu;
         float4 x = make_float4(INFINITY, 0.f, 0.f, 0.f);
-        if (u < total) {
-          j = v.cell_atoms[sh.seg_q[seg[t]] + u];
-          x = v.pos2[sh.seg_q[seg[t]] + u];
-        }
         const uint32_t st = min(seg[t], kMaxSegments - 1u);
+        const uint32_t qc = sh.seg_q[st] + u;
+        if (u < total) {
+          j = v.cell_atoms[qc];
+          x = v.pos2[qc];
+        }
+        const uint32_t e = staged_group ? qc + sh.delta[st] : j;
         const float sx = form == kBuildShifted ? sh.seg_s[0][st] : 0.f;
         const float sy = form == kBuildShifted ? sh.seg_s[1][st] : 0.f;
         const float sz = form == kBuildShifted ? sh.seg_s[2][st] : 0.f;
         CandPair& cp = c[t >> 1];
         if ((t & 1) == 0) {
-          cp.jx = j, cp.nx.x = -x.x, cp.ny.x = -x.y, cp.nz.x = -x.z;
+          cp.jx = j, cp.ex = e, cp.nx.x = -x.x, cp.ny.x = -x.y, cp.nz.x = -x.z;
           cp.sx.x = sx, cp.sy.x = sy, cp.sz.x = sz;
         } else {
-          cp.jy = j, cp.nx.y = -x.x, cp.ny.y = -x.y, cp.nz.y = -x.z;
+          cp.jy = j, cp.ey = e, cp.nx.y = -x.x, cp.ny.y = -x.y, cp.nz.y = -x.z;
           cp.sx.y = sx, cp.sy.y = sy, cp.sz.y = sz;
         }
       }
@@ -683,7 +822,7 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
       }
     }
     if (lane < nh) {
-      v.nbr_count[i] = min(my_cnt, p.max_neighbors);
+      v.nbr_count[by_q ? i0 + lane : i] = min(my_cnt, p.max_neighbors);
       v.ref_pos[i] = xi;
       v.ref_img[i] = v.img[i];
       v.cross[i] = 0u;
@@ -994,19 +1133,26 @@ struct CoeffRow {
   }
 };
 
-// The pair loop of k_lj for one particle (see k_lj).  kFar = false drops the
-// straddling-pair test: valid for warps whose particles all lie at least rc
-// inside every face, where no pair within rc can straddle the boundary.
-template <bool kObs, bool kClamp, int kTpa, int kUnroll, bool kNoL1, bool kFar, int kNt>
+// The pair loop of k_lj / k_lj_staged for one particle.  kFar = false drops
+// the straddling-pair test: valid for warps whose particles all lie at least
+// rc inside every face, where no pair within rc can straddle the boundary.
+// The neighbour positions come from `src`: the global positions (list
+// entries are slots, padding entries the far particle at n_slots) or, with
+// kStage, a group's stage in shared memory (entries are stage indices, the
+// far particle at the end of the stage); `row` is the particle's list row and
+// `pad` the index of the far particle.
+template <bool kObs, bool kClamp, int kTpa, int kUnroll, bool kNoL1, bool kFar, int kNt,
+          bool kStage = false>
 __device__ __forceinline__ void lj_pairs(const DeviceView& v, const ReplicaParams& p,
-                                         const CoeffRow<kNt>& coeff, float4 xi, uint32_t i,
+                                         const CoeffRow<kNt>& coeff, float4 xi, uint32_t row,
+                                         const float4* src, uint32_t pad,
                                          uint32_t sub, uint32_t n, uint32_t n_warp, float rc2,
                                          float half_min_sq, LjAcc<kTpa>& ax, LjAcc<kTpa>& ay,
                                          LjAcc<kTpa>& az, LjAcc<kTpa>& ae, LjAcc<kTpa>& aw) {
   const float2 xi2x = make_float2(xi.x, xi.x);
   const float2 xi2y = make_float2(xi.y, xi.y);
   const float2 xi2z = make_float2(xi.z, xi.z);
-  const uint32_t* list = v.nbr + nbr_index(i, 0, v.nbr_stride) + sub * kGroup;
+  const uint32_t* list = v.nbr + nbr_index(row, 0, v.nbr_stride) + sub * kGroup;
   // Software-pipelined over batches of kUnroll (4 or 8) own entries: all
   // list loads of a batch are issued, then all position gathers, then the
   // arithmetic, so a warp keeps kUnroll independent misses in flight
@@ -1022,7 +1168,7 @@ __device__ __forceinline__ void lj_pairs(const DeviceView& v, const ReplicaParam
 #pragma unroll
   for (uint32_t u = 0; u < kUnroll; ++u) {
     const uint32_t k = u * kTpa + sub;
-    jn[u] = k < n ? list_load<kNoL1>(list + (size_t)(u * kTpa) * kGroup) : v.n_slots;
+    jn[u] = k < n ? list_load<kNoL1>(list + (size_t)(u * kTpa) * kGroup) : pad;
   }
   for (uint32_t k0 = 0; k0 < n_warp; k0 += kStep) {
     uint32_t j[kUnroll];
@@ -1030,12 +1176,12 @@ __device__ __forceinline__ void lj_pairs(const DeviceView& v, const ReplicaParam
     for (uint32_t u = 0; u < kUnroll; ++u) j[u] = jn[u];
     float4 xj[kUnroll];
 #pragma unroll
-    for (uint32_t u = 0; u < kUnroll; ++u) xj[u] = __ldg(&v.pos[j[u]]);
+    for (uint32_t u = 0; u < kUnroll; ++u) xj[u] = kStage ? src[j[u]] : __ldg(&src[j[u]]);
 #pragma unroll
     for (uint32_t u = 0; u < kUnroll; ++u) {
       const uint32_t k = k0 + kStep + u * kTpa + sub;
       jn[u] = k < n ? list_load<kNoL1>(list + (size_t)(k0 + kStep + u * kTpa) * kGroup)
-                    : v.n_slots;
+                    : pad;
     }
     // Own entries 2h and 2h+1 of the batch run through the packed FP32x2
     // pipe of sm_100 (__fadd2_rn / __fmul2_rn / __ffma2_rn round each lane
@@ -1147,13 +1293,13 @@ __global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
          xi.y - p.lo[1] >= rcm && p.lo[1] + p.len[1] - xi.y > rcm &&
          xi.z - p.lo[2] >= rcm && p.lo[2] + p.len[2] - xi.z > rcm);
     if (__all_sync(kFull, inside)) {
-      lj_pairs<kObs, kClamp, kTpa, kUnroll, kNoL1, false, kNt>(v, p, coeff, xi, i, sub, n,
-                                                               n_warp, rc2, half_min_sq, ax, ay,
-                                                               az, ae, aw);
+      lj_pairs<kObs, kClamp, kTpa, kUnroll, kNoL1, false, kNt>(
+          v, p, coeff, xi, i, v.pos, v.n_slots, sub, n, n_warp, rc2, half_min_sq, ax, ay, az,
+          ae, aw);
     } else {
-      lj_pairs<kObs, kClamp, kTpa, kUnroll, kNoL1, true, kNt>(v, p, coeff, xi, i, sub, n,
-                                                              n_warp, rc2, half_min_sq, ax, ay,
-                                                              az, ae, aw);
+      lj_pairs<kObs, kClamp, kTpa, kUnroll, kNoL1, true, kNt>(
+          v, p, coeff, xi, i, v.pos, v.n_slots, sub, n, n_warp, rc2, half_min_sq, ax, ay, az,
+          ae, aw);
     }
   }
   const float fx = ax.total(), fy = ay.total(), fz = az.total();
@@ -1168,6 +1314,136 @@ __global__ void __launch_bounds__(kBlock) k_lj(DeviceView v) {
     block_add_lane<kBlock>(owner, 0.5 * (double)w, st, kAccVirial);
   }
   if (kPost) post_partial<kKinetic>(v, st, r, owner, ke);
+}
+
+// LJ pair forces of a staged context: block g handles the 128 particles of
+// cell-order rows [128 g, 128 g + 128) (kTpa threads each).  Its first warp
+// derives the group's stage layout (stage_layout, the same function the list
+// build used), the block copies the stage -- pos[cell_atoms[q]] for every q
+// of every window, one window per warp at a time -- into shared memory, and
+// every neighbour position of the pair loop is then a shared-memory load
+// instead of an L1/L2 gather.  A group whose layout fell back to slot
+// entries reads global positions, as k_lj does.  The arithmetic, the list
+// order and the canonical summation order are k_lj's, so the forces, energies
+// and virial are bit-identical to k_lj's for the same list.
+template <bool kObs, int kMode, int kTpa, int kUnroll, bool kNoL1, int kNt>
+__global__ void __launch_bounds__(kBlock* kTpa) k_lj_staged(DeviceView v) {
+  constexpr int kThreads = kBlock * kTpa;
+  constexpr bool kClamp = kMode == kForceClamp;
+  constexpr bool kPost = kMode >= kForcePost;
+  constexpr bool kKinetic = kMode == kForcePostKinetic || (kPost && kObs);
+  extern __shared__ float4 stage[];  // v.stage_cap + 1 entries
+  __shared__ StageLayout lay;
+  __shared__ LjCoeff table[kMaxTypes * kMaxTypes];
+  const uint32_t g = blockIdx.x;
+  const uint32_t r = v.block_replica[g];
+  const ReplicaParams& p = v.rp[r];
+  const int nt = p.n_types;
+  for (int t = threadIdx.x; t < nt * nt; t += kThreads) table[t] = v.lj[p.lj_offset + t];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  if (warp == 0) stage_layout(v, p, g, lane, v.stage_cap, lay);
+  __syncthreads();
+  const bool staged = lay.n_win != 0u;
+  if (staged) {
+    const uint32_t n_win = lay.n_win;
+    for (uint32_t w = warp; w < n_win; w += kThreads / 32) {
+      const uint32_t q0 = lay.qbeg[w], b = lay.base[w];
+      const uint32_t len = (w + 1u < n_win ? lay.base[w + 1u] : lay.size) - b;
+      for (uint32_t t = lane; t < len; t += 32u) stage[b + t] = v.pos[v.cell_atoms[q0 + t]];
+    }
+    if (threadIdx.x == 0) stage[lay.size] = v.pos[v.n_slots];  // the far particle
+    __syncthreads();
+  }
+
+  const uint32_t sub = threadIdx.x % kTpa;
+  const uint32_t q = g * kBlock + threadIdx.x / kTpa;
+  const bool real = q >= lay.q_first && q < lay.q_end;
+  // Padding rows are padding slots (inert, never written).
+  const uint32_t i = real ? v.cell_atoms[q] : q;
+  LjAcc<kTpa> ax, ay, az, ae, aw;
+  float4 vm_kick = make_float4(0.f, 0.f, 0.f, 1.f);
+  ax.zero();
+  ay.zero();
+  az.zero();
+  ae.zero();
+  aw.zero();
+  {
+    const float4 xi = v.pos[i];
+    if (kPost) vm_kick = (real && sub == 0u) ? v.vel[i] : make_float4(0.f, 0.f, 0.f, 1.f);
+    CoeffRow<kNt> coeff;
+    coeff.init(table + __float_as_int(xi.w) * nt);
+    const uint32_t n = real ? v.nbr_count[q] : 0u;
+    const uint32_t n_warp = __reduce_max_sync(kFull, n);
+    const float rc2 = p.force_cut_sq;
+    const float hmin = fminf(p.half[0], fminf(p.half[1], p.half[2]));
+    const float half_min_sq = hmin * hmin;
+    const float rcm = 1.001f * sqrtf(rc2) + 1e-6f * fmaxf(p.len[0], fmaxf(p.len[1], p.len[2]));
+    const bool inside = !real ||
+        (xi.x - p.lo[0] >= rcm && p.lo[0] + p.len[0] - xi.x > rcm &&
+         xi.y - p.lo[1] >= rcm && p.lo[1] + p.len[1] - xi.y > rcm &&
+         xi.z - p.lo[2] >= rcm && p.lo[2] + p.len[2] - xi.z > rcm);
+    const bool all_inside = __all_sync(kFull, inside);
+    if (staged) {
+      if (all_inside) {
+        lj_pairs<kObs, kClamp, kTpa, kUnroll, kNoL1, false, kNt, true>(
+            v, p, coeff, xi, q, stage, lay.size, sub, n, n_warp, rc2, half_min_sq, ax, ay, az,
+            ae, aw);
+      } else {
+        lj_pairs<kObs, kClamp, kTpa, kUnroll, kNoL1, true, kNt, true>(
+            v, p, coeff, xi, q, stage, lay.size, sub, n, n_warp, rc2, half_min_sq, ax, ay, az,
+            ae, aw);
+      }
+    } else {
+      if (all_inside) {
+        lj_pairs<kObs, kClamp, kTpa, kUnroll, kNoL1, false, kNt>(
+            v, p, coeff, xi, q, v.pos, v.n_slots, sub, n, n_warp, rc2, half_min_sq, ax, ay, az,
+            ae, aw);
+      } else {
+        lj_pairs<kObs, kClamp, kTpa, kUnroll, kNoL1, true, kNt>(
+            v, p, coeff, xi, q, v.pos, v.n_slots, sub, n, n_warp, rc2, half_min_sq, ax, ay, az,
+            ae, aw);
+      }
+    }
+  }
+  const float fx = ax.total(), fy = ay.total(), fz = az.total();
+  const bool owner = real && sub == 0u;
+  if (owner) v.force[i] = make_float4(fx, fy, fz, 0.f);
+  ReplicaState* st = &v.rs[r];
+  double ke = 0.0;
+  if (kPost) ke = post_slot_vm<true, kKinetic>(v, p, st, i, owner, vm_kick, fx, fy, fz);
+  if (kObs) {
+    const float e = ae.total(), w = aw.total();
+    block_add_lane<kThreads>(owner, 0.5 * (double)e, st, kAccPair);
+    block_add_lane<kThreads>(owner, 0.5 * (double)w, st, kAccVirial);
+  }
+  if (kPost) post_partial<kKinetic>(v, st, r, owner, ke);
+}
+
+// Slot-indexed copy of a staged context's list (debug views): out_count[slot]
+// and out[slot * cap + k] = neighbour slot, decoding stage indices through the
+// group's layout.  One block of 128 threads per group.
+__global__ void __launch_bounds__(kBlock) k_list_to_slots(DeviceView v, uint32_t cap,
+                                                          uint32_t* out_count, uint32_t* out) {
+  __shared__ StageLayout lay;
+  const uint32_t g = blockIdx.x;
+  const ReplicaParams& p = v.rp[v.block_replica[g]];
+  if (threadIdx.x < 32) stage_layout(v, p, g, threadIdx.x, v.stage_cap, lay);
+  __syncthreads();
+  const uint32_t q = g * kBlock + threadIdx.x;
+  if (q < lay.q_first || q >= lay.q_end) return;
+  const uint32_t i = v.cell_atoms[q];
+  const uint32_t n = v.nbr_count[q];
+  out_count[i] = n;
+  const uint32_t* list = v.nbr + nbr_index(q, 0, v.nbr_stride);
+  for (uint32_t k = 0; k < n && k < cap; ++k) {
+    uint32_t e = list[(size_t)k * kGroup];
+    if (lay.n_win != 0u) {
+      uint32_t w = 0;  // last window whose base <= e
+      while (w + 1u < lay.n_win && lay.base[w + 1u] <= e) ++w;
+      e = v.cell_atoms[lay.qbeg[w] + (e - lay.base[w])];
+    }
+    out[(size_t)i * cap + k] = e;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1502,9 +1778,10 @@ void launch_project_exclusions(const StepLaunch& l, bool force_all) {
   check_launch("project_exclusions");
 }
 
-void launch_rebuild(const StepLaunch& l, bool force_all) {
+void launch_rebuild(const StepLaunch& l, bool force_all, bool count_build) {
   if (force_all) {
-    k_force_rebuild_flags<<<(l.v.n_replicas + 127) / 128, 128, 0, l.stream>>>(l.v, 1);
+    k_force_rebuild_flags<<<(l.v.n_replicas + 127) / 128, 128, 0, l.stream>>>(
+        l.v, count_build ? 1 : 0);
     check_launch("force_rebuild_flags");
   }
   k_bin<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
@@ -1572,11 +1849,118 @@ void launch_lj_nt(const StepLaunch& l, int mode) {
   }
 }
 
+namespace {
+
+// Staged contexts: every pair-force launch goes to k_lj_staged (the list
+// rows are cell-order rows there), with (stage_cap + 1) float4 of dynamic
+// shared memory.
+size_t staged_smem(const StepLaunch& l) { return (size_t)(l.v.stage_cap + 1u) * sizeof(float4); }
+
+template <bool kObs, int kMode, int kTpa, int kUnroll, int kNt>
+void staged_one(const StepLaunch& l) {
+  k_lj_staged<kObs, kMode, kTpa, kUnroll, true, kNt>
+      <<<l.v.n_blocks, kBlock * kTpa, staged_smem(l), l.stream>>>(l.v);
+}
+
+template <bool kObs, int kMode, int kTpa, int kUnroll, int kNt>
+void staged_attr(size_t smem) {
+  const cudaError_t e =
+      cudaFuncSetAttribute(k_lj_staged<kObs, kMode, kTpa, kUnroll, true, kNt>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) {
+    throw std::runtime_error(std::string("staged pair kernel shared memory: ") +
+                             cudaGetErrorString(e));
+  }
+}
+
+template <int kTpa, int kUnroll, int kNt>
+void staged_attr_modes(size_t smem) {
+  staged_attr<false, kForcePlain, kTpa, kUnroll, kNt>(smem);
+  staged_attr<false, kForcePost, kTpa, kUnroll, kNt>(smem);
+  staged_attr<false, kForcePostKinetic, kTpa, kUnroll, kNt>(smem);
+}
+
+template <int kTpa, int kUnroll, int kNt>
+void staged_plain(const StepLaunch& l, int mode) {
+  switch (mode) {
+    case kForcePlain: staged_one<false, kForcePlain, kTpa, kUnroll, kNt>(l); break;
+    case kForcePost: staged_one<false, kForcePost, kTpa, kUnroll, kNt>(l); break;
+    default: staged_one<false, kForcePostKinetic, kTpa, kUnroll, kNt>(l); break;
+  }
+}
+
+template <int kTpa, int kUnroll>
+void staged_plain_nt(const StepLaunch& l, int mode) {
+  switch (l.lj_types) {
+    case 1: staged_plain<kTpa, kUnroll, 1>(l, mode); break;
+    case 2: staged_plain<kTpa, kUnroll, 2>(l, mode); break;
+    default: staged_plain<kTpa, kUnroll, 0>(l, mode); break;
+  }
+}
+
+void launch_forces_staged(const StepLaunch& l, bool observables, bool clamp, int mode) {
+  if (clamp) {
+    staged_one<false, kForceClamp, 2, 4, 0>(l);
+  } else if (observables) {
+    const bool plain = mode == kForcePlain;
+    switch (l.lj_tpa) {
+      case 2:
+        plain ? staged_one<true, kForcePlain, 2, 4, 0>(l) : staged_one<true, kForcePost, 2, 4, 0>(l);
+        break;
+      case 4:
+        plain ? staged_one<true, kForcePlain, 4, 4, 0>(l) : staged_one<true, kForcePost, 4, 4, 0>(l);
+        break;
+      default:
+        plain ? staged_one<true, kForcePlain, 1, 4, 0>(l) : staged_one<true, kForcePost, 1, 4, 0>(l);
+        break;
+    }
+  } else {
+    const int key = l.lj_tpa * 10 + l.lj_unroll;
+    switch (key) {
+      case 14: staged_plain_nt<1, 4>(l, mode); break;
+      case 18: staged_plain_nt<1, 8>(l, mode); break;
+      case 24: staged_plain_nt<2, 4>(l, mode); break;
+      case 28: staged_plain_nt<2, 8>(l, mode); break;
+      case 44: staged_plain_nt<4, 4>(l, mode); break;
+      case 48: staged_plain_nt<4, 8>(l, mode); break;
+      default: throw std::runtime_error("unsupported staged pair-force schedule");
+    }
+  }
+  check_launch("lj_staged");
+}
+
+}  // namespace
+
+// Raises the dynamic shared-memory limit of every staged pair-force variant to
+// `smem` bytes (once per context, outside any stream capture).
+void prepare_staged_kernels(size_t smem) {
+  staged_attr<false, kForceClamp, 2, 4, 0>(smem);
+  staged_attr<true, kForcePlain, 1, 4, 0>(smem);
+  staged_attr<true, kForcePost, 1, 4, 0>(smem);
+  staged_attr<true, kForcePlain, 2, 4, 0>(smem);
+  staged_attr<true, kForcePost, 2, 4, 0>(smem);
+  staged_attr<true, kForcePlain, 4, 4, 0>(smem);
+  staged_attr<true, kForcePost, 4, 4, 0>(smem);
+#define BB_ATTR(t, u)                    \
+  staged_attr_modes<t, u, 0>(smem);      \
+  staged_attr_modes<t, u, 1>(smem);      \
+  staged_attr_modes<t, u, 2>(smem);
+  BB_ATTR(1, 4) BB_ATTR(1, 8) BB_ATTR(2, 4) BB_ATTR(2, 8) BB_ATTR(4, 4) BB_ATTR(4, 8)
+#undef BB_ATTR
+}
+
+void launch_list_to_slots(const StepLaunch& l, uint32_t cap, uint32_t* out_count, uint32_t* out) {
+  k_list_to_slots<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, cap, out_count, out);
+  check_launch("list_to_slots");
+}
+
 void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post) {
   const bool fuse = post && l.fuse_post != 0;
   const int fin = !fuse ? kForcePlain : (l.need_kinetic ? kForcePostKinetic : kForcePost);
   const bool bonded = l.v.has_bonded != 0;
-  if (clamp) {
+  if (l.v.list_by_q) {
+    launch_forces_staged(l, observables, clamp, bonded ? kForcePlain : fin);
+  } else if (clamp) {
     k_lj<false, kForceClamp, 1, 8, false, 0><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
   } else if (observables) {
     const int mode = bonded ? kForcePlain : fin;

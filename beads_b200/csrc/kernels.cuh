@@ -31,12 +31,19 @@ struct StepLaunch {
 // handle is `cond`; the kernel switches that node on when a replica rebuilds.
 void launch_pre(const StepLaunch& l, int mode, cudaGraphConditionalHandle cond = 0,
                 bool use_cond = false);
-void launch_rebuild(const StepLaunch& l, bool force_all);
+// force_all: every replica rebuilds now; count_build = false rebuilds without
+// counting a build or reordering (a list-layout change of the same list).
+void launch_rebuild(const StepLaunch& l, bool force_all, bool count_build = true);
 // post: finish the step with the second half-kick, the kinetic-energy total
 // and the per-replica step epilogue -- inside the last force kernel when
 // fuse_post is set, else as a separate k_post launch.
 void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post = false);
 void launch_post(const StepLaunch& l, bool kick, bool observables);
+// Staged contexts (list rows by cell order): raise the dynamic shared-memory
+// limit of the staged pair-force kernels, and decode the list into slot rows
+// of neighbour slots (debug views).
+void prepare_staged_kernels(size_t smem);
+void launch_list_to_slots(const StepLaunch& l, uint32_t cap, uint32_t* out_count, uint32_t* out);
 void launch_project_exclusions(const StepLaunch& l, bool force_all);
 void launch_apply_lambda(const StepLaunch& l);
 // Scatter a tag-ordered host copy (already on the device) into slots.

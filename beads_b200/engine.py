@@ -282,11 +282,23 @@ class Engine:
         _lib.check(self._lib.beads_set_tuning(self._h, sched))
 
     def tuning(self) -> dict:
+        """The kernel schedule; "staged" is the list layout (not part of
+        set_tuning: see set_list_staged)."""
         out = (ctypes.c_int32 * 5)()
         _lib.check(self._lib.beads_get_tuning(self._h, out))
         return {"threads_per_particle": out[0], "fuse_post": bool(out[1]),
                 "batch_depth": out[2], "list_bypass_l1": bool(out[3]),
-                "autotuned": bool(out[4])}
+                "autotuned": bool(out[4]), "staged": self.list_staged()}
+
+    def set_list_staged(self, staged: bool) -> None:
+        """Pair forces from shared-memory cell tiles (True) or global gathers
+        (False); the same bits either way (beads_set_list_layout)."""
+        _lib.check(self._lib.beads_set_list_layout(self._h, 1 if staged else 0))
+
+    def list_staged(self) -> bool:
+        out = ctypes.c_int32()
+        _lib.check(self._lib.beads_get_list_layout(self._h, ctypes.byref(out)))
+        return bool(out.value)
 
     # -- differentiation ------------------------------------------------------
     def set_lj(self, replica: int, epsilon, sigma) -> None:

@@ -836,7 +836,7 @@ def run_adjoint(args) -> None:
     sig2 = sig.detach().clone().requires_grad_(True)
     x2 = x0.clone().requires_grad_(True)
     with Engine(specs) as eng2:
-        eng2.set_tuning(**{k: v for k, v in schedule.items() if k != "autotuned"})
+        eng2.set_tuning(**{k: v for k, v in schedule.items() if k not in ("autotuned", "staged")})
         eng2.run(max(3, args.warmup))
         eng2.run(GRAPH_WARMUP)
         torch.cuda.synchronize()

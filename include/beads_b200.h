@@ -282,6 +282,19 @@ BEADS_API int beads_list_stats(beads_ctx* ctx, uint64_t* total_entries,
 BEADS_API int beads_set_tuning(beads_ctx* ctx, const int32_t* schedule);
 BEADS_API int beads_get_tuning(beads_ctx* ctx, int32_t* schedule);
 
+/* Neighbour-list layout of a context.  Staged (1, the default when some
+ * replica has >= 4 cells on every axis): list rows in the cell order of the
+ * last build, and for every group of 128 rows whose stage fits, entries that
+ * index a shared-memory copy of the group's stencil cells, from which the
+ * pair-force kernel reads every neighbour position.  Slot layout (0): rows
+ * and entries by slot, positions gathered from global memory.  The choice
+ * never changes a result; switching rebuilds the list before the next force
+ * evaluation.  beads_get_list_layout reports 0 when no replica can stage.
+ * No reference counterpart (the reference keeps one slot-major list,
+ * neighbor_list.cuh:12-71). */
+BEADS_API int beads_set_list_layout(beads_ctx* ctx, int32_t staged);
+BEADS_API int beads_get_list_layout(beads_ctx* ctx, int32_t* staged);
+
 /* ---- differentiation (no reference counterpart) ------------------------- */
 /* Replaces one replica's LJ tables (symmetric [n_types * n_types], same
  * meaning as beads_forcefield_desc.lj_epsilon / lj_sigma); the cutoff and

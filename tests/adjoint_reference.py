@@ -117,3 +117,69 @@ def trajectory(x0, v0, masses, types, box, eps, sig, rc, shift, dt, steps, recor
         if step >= record_from:
             rows.append(torch.stack([pe, w, lam * lam * kin]))
     return torch.stack(rows)
+
+
+def lj_pair_terms(x, types, box, eps, sig, rc, shift, pi, pj):
+    """lj_terms over a fixed set of unordered pairs (pi < pj): every pair
+    that can come within rc during the trajectory must be in the set.  As in
+    lj_terms (and the full-list engine), the force on a particle uses its own
+    row of the type tables, and the energy and virial take half of each
+    ordered pair, so the table gradients split over [a, b] and [b, a] alike."""
+    d = x[pi] - x[pj]
+    d = d - box * torch.round(d / box)
+    r2 = (d * d).sum(-1)
+    mask = r2 < rc * rc
+    r2s = torch.where(mask, r2, torch.ones_like(r2))
+    inv = 1.0 / r2s
+    ti, tj = types[pi], types[pj]
+
+    def oriented(e, s):
+        sr6 = (s * s * inv) ** 3
+        sr12 = sr6 * sr6
+        phi = torch.where(mask, 24.0 * e * inv * (2.0 * sr12 - sr6), torch.zeros_like(r2))
+        u = 4.0 * e * (sr12 - sr6)
+        if shift:
+            sc6 = (s * s / (rc * rc)) ** 3
+            u = u - 4.0 * e * (sc6 * sc6 - sc6)
+        return phi, torch.where(mask, u, torch.zeros_like(u))
+
+    phi_i, u_i = oriented(eps[ti, tj], sig[ti, tj])
+    phi_j, u_j = oriented(eps[tj, ti], sig[tj, ti])
+    force = (torch.zeros_like(x).index_add(0, pi, phi_i[:, None] * d)
+             .index_add(0, pj, -phi_j[:, None] * d))
+    pe = 0.5 * (u_i + u_j).sum()
+    w = 0.5 * ((phi_i + phi_j) * r2s).sum()
+    return force, pe, w
+
+
+def trajectory_pairs(x0, v0, masses, types, box, eps, sig, rc, shift, dt, steps, record_from,
+                     pi, pj, thermostat=None):
+    """trajectory() with the pair terms over a fixed pair set (large systems).
+    Returns the observables and the largest displacement of any particle from
+    x0 over the run, which must stay below half the pair set's buffer."""
+    m = masses[:, None]
+    h = 0.5 * dt
+    n = x0.shape[0]
+    dof = 3.0 * n - 3.0
+    x, v = x0, v0
+    lam = torch.ones((), dtype=x0.dtype, device=x0.device)
+    f, pe, w = lj_pair_terms(x, types, box, eps, sig, rc, shift, pi, pj)
+    kin = 0.5 * (m * v * v).sum()
+    rows = []
+    moved = torch.zeros((), dtype=x0.dtype, device=x0.device)
+    if record_from == 0:
+        rows.append(torch.stack([pe, w, kin]))
+    for step in range(1, steps + 1):
+        u = lam * v + h * f / m
+        x = x + dt * u
+        moved = torch.maximum(moved, ((x - x0) ** 2).sum(-1).max().detach().sqrt())
+        f, pe, w = lj_pair_terms(x, types, box, eps, sig, rc, shift, pi, pj)
+        v = u + h * f / m
+        kin = 0.5 * (m * v * v).sum()
+        if thermostat is not None:
+            kt, tau = thermostat
+            arg = 1.0 + (dt / tau) * (kt * dof / (2.0 * kin) - 1.0)
+            lam = torch.sqrt(torch.clamp(arg, min=0.0))
+        if step >= record_from:
+            rows.append(torch.stack([pe, w, lam * lam * kin]))
+    return torch.stack(rows), float(moved)

@@ -26,6 +26,12 @@ def _workload(name: str, beads: int):
         return workloads.lj_lattice(n_side=side)
     if name == "replicas":
         return workloads.replica_batch(512)
+    if name == "mixture":
+        # the benchmark mixture (same density and composition) at `beads`
+        # beads, relaxed as the benchmark relaxes it
+        box = 37.2 * (beads / 1_048_576) ** (1.0 / 3.0)
+        return workloads.relaxed(workloads.lj_mixture(n=beads, box=box, seed=3),
+                                 iterations=500, dmax=0.004, fref=200.0, capacity=256)
     if name == "melt":
         # the bead-spring melt benchmark's input: chains of 200, grown in
         # lockstep and relaxed (beads // 200 chains)
@@ -37,7 +43,7 @@ def _workload(name: str, beads: int):
 def main(argv: list[str] | None = None) -> dict:
     parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     parser.add_argument("--workload", default="fit-mixture",
-                        choices=["fit-mixture", "lattice", "replicas", "melt"])
+                        choices=["fit-mixture", "lattice", "replicas", "melt", "mixture"])
     parser.add_argument("--beads", type=int, default=524288)
     parser.add_argument("--stage", default="rebuild",
                         choices=["forces", "forces_kick", "rebuild", "step"])
@@ -45,6 +51,9 @@ def main(argv: list[str] | None = None) -> dict:
     parser.add_argument("--warm", type=int, default=20)
     parser.add_argument("--schedule", default="2,0,4,1",
                         help="threads per particle, fused kick, depth, list bypass L1")
+    parser.add_argument("--layout", default="staged", choices=["staged", "slot"],
+                        help="neighbour-list layout (pair forces from shared-memory cell "
+                             "tiles, or gathered from global memory)")
     args = parser.parse_args(argv)
 
     import torch
@@ -54,12 +63,14 @@ def main(argv: list[str] | None = None) -> dict:
     tpa, fuse, depth, bypass = (int(x) for x in args.schedule.split(","))
     with Engine(_workload(args.workload, args.beads)) as eng:
         eng.set_tuning(tpa, bool(fuse), depth, bool(bypass))
+        eng.set_list_staged(args.layout == "staged")
         eng.run(args.warm)
         torch.cuda.synchronize()
         torch.cuda.profiler.start()
         ms = eng.profile(args.stage, args.reps)
         torch.cuda.profiler.stop()
-    out = {"workload": args.workload, "stage": args.stage, "reps": args.reps, "ms": ms}
+    out = {"workload": args.workload, "stage": args.stage, "reps": args.reps, "ms": ms,
+           "layout": args.layout}
     print(json.dumps(out))
     return out
 

@@ -247,3 +247,69 @@ def test_stored_trajectory_gives_the_replayed_gradients_bitwise():
         grads.append((eps.grad.clone(), sig.grad.clone(), x.grad.clone(), v.grad.clone()))
     for a, b in zip(*grads):
         assert torch.equal(a, b)
+
+
+def test_adjoint_at_fit_scale_matches_fp64_autograd():
+    """Two replicas of the 64 x 8192-bead fit workload over 30 steps (the
+    loss window's form: weighted PE / virial / KE of the last 20 steps),
+    checkpoints every 10 steps, against autograd through the FP64 restatement
+    run on the GPU over a fixed pair set with a 1.0 buffer beyond rc."""
+    from oracle import oracle as O
+    from tests.adjoint_reference import trajectory_pairs
+
+    specs = workloads.fit_mixture(n_replicas=2)
+    steps, rec, every = 30, 11, 10
+    dev = torch.device("cuda", 0)
+    eps0 = torch.tensor(workloads.MIXTURE_EPS, dtype=torch.float64)
+    sig0 = torch.tensor(specs[0].sigma, dtype=torch.float64)
+    x0 = torch.tensor(np.concatenate([s.positions for s in specs]), dtype=torch.float64)
+    v0 = torch.tensor(np.concatenate([s.velocities for s in specs]), dtype=torch.float64)
+    rng = np.random.default_rng(1)
+    weights = torch.tensor(rng.standard_normal((steps - rec + 1, len(specs), 3)))
+    weights[:, :, 0] /= 8192.0  # PE and virial are extensive: comparable terms
+    weights[:, :, 1] /= 8192.0
+
+    eps = eps0.clone().requires_grad_(True)
+    sig = sig0.clone().requires_grad_(True)
+    x = x0.clone().requires_grad_(True)
+    v = v0.clone().requires_grad_(True)
+    with Engine(specs) as eng:
+        obs = trajectory_observables(eng, eps, sig, x, v, steps=steps, record_from=rec,
+                                     checkpoint_every=every)
+        (obs * weights).sum().backward()
+
+    buffer = 1.0
+    g_eps, g_sig, g_x, g_v, ref_obs = 0.0, 0.0, [], [], []
+    at = 0
+    for r, s in enumerate(specs):
+        n = s.n
+        counts, partners = O.neighbors(s.positions, s.box_bound, s.cutoff, buffer, cap=512)
+        rows = np.repeat(np.arange(n), counts)
+        cols = np.concatenate([partners[i, :counts[i]] for i in range(n)])
+        keep = rows < cols
+        pi = torch.tensor(rows[keep], device=dev)
+        pj = torch.tensor(cols[keep].astype(np.int64), device=dev)
+        e = eps0.to(dev).clone().requires_grad_(True)
+        sg = sig0.to(dev).clone().requires_grad_(True)
+        xr = x0[at:at + n].to(dev).clone().requires_grad_(True)
+        vr = v0[at:at + n].to(dev).clone().requires_grad_(True)
+        box = torch.tensor(np.asarray(s.box_bound[1], np.float64) - s.box_bound[0], device=dev)
+        o, moved = trajectory_pairs(xr, vr, torch.tensor(s.masses, dtype=torch.float64,
+                                                         device=dev),
+                                    torch.tensor(s.types - 1, dtype=torch.long, device=dev),
+                                    box, e, sg, s.cutoff, s.shift, s.dt, steps, rec, pi, pj,
+                                    thermostat=s.thermostat)
+        assert moved < 0.5 * buffer, moved
+        (o * weights[:, r, :].to(dev)).sum().backward()
+        ref_obs.append(o.detach().cpu())
+        g_eps = g_eps + e.grad.cpu()
+        g_sig = g_sig + sg.grad.cpu()
+        g_x.append(xr.grad.cpu())
+        g_v.append(vr.grad.cpu())
+        at += n
+    ref_obs = torch.stack(ref_obs, dim=1)
+    assert _rel(obs.detach(), ref_obs) < 1e-5
+    assert _rel(eps.grad, g_eps) < 1e-4, (eps.grad, g_eps)
+    assert _rel(sig.grad, g_sig) < 1e-4, (sig.grad, g_sig)
+    assert _rel(x.grad, torch.cat(g_x)) < 1e-4
+    assert _rel(v.grad, torch.cat(g_v)) < 1e-4

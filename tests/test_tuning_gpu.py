@@ -27,17 +27,21 @@ def _case(name):
 def test_every_schedule_gives_identical_bits(name):
     spec = _case(name)
     outs = []
-    for tpa, fuse, depth, pf in SCHEDULES:
+    runs = [(sched, staged) for sched in SCHEDULES for staged in (True, False)]
+    for (tpa, fuse, depth, pf), staged in runs:
         with Engine(spec) as eng:
             eng.set_tuning(tpa, fuse, depth, pf)
+            eng.set_list_staged(staged)
             rows = [eng.run(20, 20), eng.run(20, 20)]
             states = [eng.state(r) for r in range(len(eng.sizes))]
-            assert eng.tuning() == {"threads_per_particle": tpa, "fuse_post": fuse,
-                                    "batch_depth": depth, "list_bypass_l1": pf,
-                                    "autotuned": False}
+            t = eng.tuning()
+            got = t.pop("staged")
+            assert got == staged or (name == "batch" and not got)
+            assert t == {"threads_per_particle": tpa, "fuse_post": fuse,
+                         "batch_depth": depth, "list_bypass_l1": pf, "autotuned": False}
         outs.append((rows, states))
     rows0, states0 = outs[0]
-    for (rows, states), sched in zip(outs[1:], SCHEDULES[1:]):
+    for (rows, states), sched in zip(outs[1:], runs[1:]):
         assert rows == rows0, sched
         for a, b in zip(states, states0):
             for key in ("positions", "velocities", "forces", "images"):
