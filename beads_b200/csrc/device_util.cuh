@@ -131,9 +131,11 @@ __device__ __forceinline__ void wait_prior_grid() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
-// |d|^2 with the contraction order fixed: fma(dz,dz, fma(dy,dy, dx*dx)).
+// |d|^2 with the contraction order fixed: fma(dz,dz, fma(dx,dx, dy*dy)), the
+// order nvcc gives the reference's dx * dx + dy * dy + dz * dz (its neighbour
+// lists include exactly the pairs this form puts at or below the cutoff).
 __device__ __forceinline__ float norm2(float dx, float dy, float dz) {
-  return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+  return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
 }
 
 __device__ __forceinline__ uint32_t axis_cell(float x, float lo, float inv,

@@ -27,7 +27,8 @@
 //   * discrete decisions that the reference takes in float (cell index,
 //     neighbour inclusion r^2 <= (rc+skin)^2) are evaluated in float with the
 //     same operation order the CUDA engine documents: d = xi - xj, one shift by
-//     L, r^2 = fma(dz,dz, fma(dy,dy, dx*dx));
+//     L, r^2 = fma(dz,dz, fma(dx,dx, dy*dy)) (the contraction nvcc gives the
+//     reference's dx * dx + dy * dy + dz * dz, pinned by its own neighbour lists);
 //   * the pair-cutoff decision r^2 < rc^2 is taken in float on the exactly
 //     rounded minimum-image difference (the engine's rule), so float and
 //     double evaluations include the same pairs;
@@ -85,7 +86,7 @@ inline double exact_delta(float xi, float xj, double len, double half) {
 }
 
 inline float norm2_f(float dx, float dy, float dz) {
-  return std::fmaf(dz, dz, std::fmaf(dy, dy, dx * dx));
+  return std::fmaf(dz, dz, std::fmaf(dx, dx, dy * dy));
 }
 
 uint32_t axis_cell(float x, float lo, float inv, uint32_t n) {

@@ -103,9 +103,9 @@ def _brute_neighbors(pos, box, cutoff, skin, excluded=frozenset()):
     for i in range(pos.shape[0]):
         d = (pos[i] - pos).astype(np.float32)
         d = np.where(d > half, d - length, np.where(d < -half, d + length, d)).astype(np.float32)
-        # r^2 = fma(dz,dz, fma(dy,dy, dx*dx)): emulate the two fused steps exactly in float64.
-        dx2 = (d[:, 0] * d[:, 0]).astype(np.float32)
-        s1 = (d[:, 1].astype(np.float64) ** 2 + dx2.astype(np.float64)).astype(np.float32)
+        # r^2 = fma(dz,dz, fma(dx,dx, dy*dy)): emulate the two fused steps exactly in float64.
+        dy2 = (d[:, 1] * d[:, 1]).astype(np.float32)
+        s1 = (d[:, 0].astype(np.float64) ** 2 + dy2.astype(np.float64)).astype(np.float32)
         r2 = (d[:, 2].astype(np.float64) ** 2 + s1.astype(np.float64)).astype(np.float32)
         js = [j for j in np.nonzero(r2 <= sc2)[0] if j != i and (min(i, j), max(i, j)) not in excluded]
         out.append(tuple(sorted(js)))
