@@ -14,7 +14,13 @@
 namespace bb {
 
 constexpr int kBlock = 128;          // threads per block of per-slot kernels
-constexpr int kGroup = 32;           // neighbour-list interleave width
+// Neighbour-list interleave width: entry k of the rows of one group of kGroup
+// consecutive rows is stored contiguously (see nbr_index).
+#ifndef BEADS_NBR_GROUP
+#define BEADS_NBR_GROUP 32
+#endif
+constexpr int kGroup = BEADS_NBR_GROUP;
+static_assert(kGroup == 8 || kGroup == 16 || kGroup == 32, "interleave of 8, 16 or 32 rows");
 constexpr int kMaxTypes = 16;        // LJ type table held in shared memory
 constexpr uint32_t kKeBuckets = 128; // fixed-point kinetic-energy buckets per replica
 // Coordinates of the far particle at pos[n_slots] (pads neighbour batches);
@@ -139,7 +145,8 @@ __host__ __device__ inline uint32_t term_pack(uint32_t kind, uint32_t role,
 
 __host__ __device__ inline uint64_t nbr_index(uint32_t slot, uint32_t k,
                                               uint32_t stride) {
-  return ((uint64_t)(slot >> 5) * stride + k) * kGroup + (slot & 31u);
+  return ((uint64_t)(slot / (uint32_t)kGroup) * stride + k) * kGroup +
+         (slot % (uint32_t)kGroup);
 }
 
 struct DeviceView {

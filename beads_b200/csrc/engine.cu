@@ -197,7 +197,7 @@ void Engine::autotune() {
     tune_layout();
     // Both list layouts when the context can stage: the other layout is
     // built from the same positions (relayout_list) and tuned the same way.
-    if (stage_cap_ > 0) {
+    if (stage_cap_ > 0 && !layout_fixed_) {
       const float best_first = best;
       const StepLaunch chosen_first = chosen;
       const bool first_staged = v_.list_by_q != 0;
@@ -966,6 +966,10 @@ double Engine::profile(int stage, uint32_t reps) {
         step_ += 1;
       } else if (stage == 2) {
         launch_rebuild(launch_, true);
+      } else if (stage == 4) {
+        launch_forces(launch_, false, false, false, kForcePair);
+      } else if (stage == 5) {
+        launch_forces(launch_, false, false, false, kForceBonded);
       } else {
         throw InvalidArgument("unknown profile stage");
       }
@@ -980,6 +984,9 @@ double Engine::profile(int stage, uint32_t reps) {
   }
   cudaEventDestroy(start);
   cudaEventDestroy(stop);
+  // The pair-only and bonded-only stages leave partial (or repeatedly added)
+  // forces: one full evaluation restores them.
+  if (stage == 4 || stage == 5) launch_forces(launch_, false, false);
   if (stage == 3) {
     cuda_check(cudaMemcpyAsync(v_.vel, v_.vel2, v_.n_slots * sizeof(float4),
                                cudaMemcpyDeviceToDevice, stream_), "velocity restore");
@@ -1166,6 +1173,7 @@ void Engine::debug_cells(uint32_t r, uint32_t* cell_by_tag) {
 
 void Engine::set_list_staged(bool staged) {
   const bool want = staged && stage_cap_ > 0;
+  layout_fixed_ = true;
   if ((v_.list_by_q != 0) == want) return;
   clear_graphs();
   v_.list_by_q = want ? 1 : 0;

@@ -637,7 +637,7 @@ __device__ __forceinline__ void build_chunk(const DeviceView& v, const ReplicaPa
           dz = __fadd2_rn(dz, c[q].sz);
         }
       }
-      const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+      const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
       ax[q] = !(r2.x > cut) && c[q].jx != i;
       ay[q] = !(r2.y > cut) && c[q].jy != i;
       bx[q] = __ballot_sync(kFull, ax[q]);
@@ -1193,7 +1193,7 @@ __device__ __forceinline__ void lj_pairs(const DeviceView& v, const ReplicaParam
       float2 dx = __fadd2_rn(xi2x, make_float2(-xj[u0].x, -xj[u1].x));
       float2 dy = __fadd2_rn(xi2y, make_float2(-xj[u0].y, -xj[u1].y));
       float2 dz = __fadd2_rn(xi2z, make_float2(-xj[u0].z, -xj[u1].z));
-      float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+      float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
       // Plain differences are already the once-rounded exact values unless
       // the pair straddles the periodic boundary, which needs r^2 above
       // (L_min/2)^2; only then (warp-uniform branch) recompute that pair
@@ -1472,6 +1472,39 @@ __device__ __forceinline__ V3 arm(const DeviceView& v, const ReplicaParams& p,
             acc_delta(a.z, b.z, p.len[2], p.half[2]));
 }
 
+// |d| and |d| - r0 of a float vector d, the stretch accurate to a few units
+// of 2^-48 relative to |d| instead of 2^-24: the squares are split into
+// rounded products and their exact errors (fma), the two additions into sums
+// and their exact errors (TwoSum), and one Newton step corrects the float
+// square root against the compensated sum.  A stiff bond (k = 500 at r0 =
+// 0.97) turns the 2^-24 error of a plain r - r0 into a force error of
+// ~3e-5, near the 1e-5 relative-RMS force bar of a relaxed melt, whose total
+// forces are small next to the bonded ones they cancel.
+__device__ __forceinline__ float two_sum_err(float a, float b, float s) {
+  const float bb = __fsub_rn(s, a);
+  return __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+__device__ __forceinline__ float bond_length(V3 d, float r0, float& stretch) {
+  const float px = __fmul_rn(d.x, d.x), py = __fmul_rn(d.y, d.y), pz = __fmul_rn(d.z, d.z);
+  const float ex = __fmaf_rn(d.x, d.x, -px), ey = __fmaf_rn(d.y, d.y, -py),
+              ez = __fmaf_rn(d.z, d.z, -pz);
+  const float s1 = __fadd_rn(px, py);
+  const float t1 = two_sum_err(px, py, s1);
+  const float q = __fadd_rn(s1, pz);
+  const float t2 = two_sum_err(s1, pz, q);
+  const float lo = __fadd_rn(__fadd_rn(__fadd_rn(ex, ey), __fadd_rn(ez, t1)), t2);
+  const float r = sqrtf(q);
+  if (r == 0.0f) {
+    stretch = -r0;
+    return 0.0f;
+  }
+  // sqrt(q + lo) = r + (q - r^2 + lo) / (2 r) to second order; q - r^2 is
+  // exact in one fma.
+  const float corr = __fdiv_rn(__fadd_rn(__fmaf_rn(-r, r, q), lo), __fmul_rn(2.0f, r));
+  stretch = __fadd_rn(__fsub_rn(r, r0), corr);
+  return __fadd_rn(r, corr);
+}
+
 // Force on member `role` of a harmonic bond; energy and virial of the whole
 // term.  U = 0.5 k (r - r0)^2.
 __device__ V3 bond_term(const DeviceView& v, const ReplicaParams& p,
@@ -1480,23 +1513,28 @@ __device__ V3 bond_term(const DeviceView& v, const ReplicaParams& p,
   const uint4 t = v.bonds[idx];
   const BondCoeff c = v.bond_coeff[t.z];
   const V3 d = arm(v, p, t.x, t.y);
-  const float r2 = dot3(d, d);
-  const float r = sqrtf(r2);
-  const float s = r - c.r0;
+  float s;
+  const float r = bond_length(d, c.r0, s);
   energy = 0.5f * c.k * s * s;
   if (r == 0.0f) {
     virial = 0.f;
     return v3(0.f, 0.f, 0.f);
   }
   const float sc = -c.k * s / r;
-  virial = sc * r2;
+  virial = -c.k * s * r;
   const float sign = role == 0u ? 1.0f : -1.0f;
   return scal(sc * sign, d);
 }
 
-// U = 0.5 k (theta - theta0)^2 with the reference's conventions: cosine
-// clamped to [-1, 1], sin(theta) floored at 1e-3, theta = 0 (energy only) on
-// a zero-length arm.
+// U = 0.5 k (theta - theta0)^2 with the reference's conventions: sin(theta)
+// floored at 1e-3 where sin^2 <= 1e-6, theta = 0 (energy only) on a
+// zero-length arm.  Written for float accuracy near straight angles, where
+// the reference's form (cos clamped to [-1, 1], theta = acos(cos), sin =
+// sqrt(1 - cos^2)) loses digits to cancellation: sin(theta) comes from the
+// cross product n = a1 x a2 (|n| = r1 r2 sin), theta = atan2(|n|, a1.a2),
+// and the force on i, a (cos a1 / r1^2 - a2 / (r1 r2)) with a = -k dtheta /
+// sin, is evaluated as a (a1 x n) / (r1^2 r1 r2) = -k dtheta (a1 x n) /
+// (r1^2 |n|) (likewise for k); the same quantities in exact arithmetic.
 __device__ V3 angle_term(const DeviceView& v, const ReplicaParams& p,
                          uint32_t idx, uint32_t role, float& energy,
                          float& virial) {
@@ -1511,21 +1549,29 @@ __device__ V3 angle_term(const DeviceView& v, const ReplicaParams& p,
     virial = 0.f;
     return v3(0.f, 0.f, 0.f);
   }
-  const float r1 = sqrtf(q1);
-  const float r2 = sqrtf(q2);
-  float cs = dot3(a1, a2) / (r1 * r2);
-  cs = fminf(1.0f, fmaxf(-1.0f, cs));
-  const float theta = cs == 1.0f ? 0.0f : (cs == -1.0f ? 3.14159265358979323846f : acosf(cs));
+  const V3 n = cross3(a1, a2);
+  const float qn = dot3(n, n);
+  const float nm = sqrtf(qn);
+  const float dt = dot3(a1, a2);
+  const float theta = atan2f(nm, dt);
   const float dth = theta - c.theta0;
   energy = 0.5f * c.k * dth * dth;
-  const float s2 = 1.0f - cs * cs;
-  const float sn = s2 <= 1.0e-6f ? 1.0e-3f : sqrtf(s2);
-  const float a = -c.k * dth / sn;
-  const float c11 = a * cs / q1;
-  const float c12 = -a / (r1 * r2);
-  const float c22 = a * cs / q2;
-  const V3 fi = axpy(c12, a2, scal(c11, a1));
-  const V3 fk = axpy(c12, a1, scal(c22, a2));
+  V3 fi, fk;
+  if (qn <= 1.0e-6f * q1 * q2) {
+    // The reference's floor: sin = 1e-3.
+    const float r1 = sqrtf(q1), r2 = sqrtf(q2);
+    const float cs = fminf(1.0f, fmaxf(-1.0f, dt / (r1 * r2)));
+    const float a = -c.k * dth * 1.0e3f;
+    const float c11 = a * cs / q1;
+    const float c12 = -a / (r1 * r2);
+    const float c22 = a * cs / q2;
+    fi = axpy(c12, a2, scal(c11, a1));
+    fk = axpy(c12, a1, scal(c22, a2));
+  } else {
+    const float g = -c.k * dth / nm;
+    fi = scal(g / q1, cross3(a1, n));
+    fk = scal(g / q2, cross3(n, a2));
+  }
   virial = dot3(a1, fi) + dot3(a2, fk);
   if (role == 0u) return fi;
   if (role == 2u) return fk;
@@ -1533,7 +1579,10 @@ __device__ V3 angle_term(const DeviceView& v, const ReplicaParams& p,
 }
 
 // U = k (1 + d cos(n phi)), signed phi; singular geometry contributes energy
-// only (k(1+d) if n == 0, else k).
+// only (k(1+d) if n == 0, else k).  phi = atan2(|b1| b0.(b1 x b2),
+// (b0 x b1).(b1 x b2)): the reference's acos of the normalised cosine with
+// the sign of b0.(b1 x b2), in a form that keeps float accuracy near
+// phi = 0 and pi (cis and trans), where acos loses digits.
 __device__ V3 dihedral_term(const DeviceView& v, const ReplicaParams& p,
                             uint32_t idx, uint32_t role, float& energy,
                             float& virial) {
@@ -1552,14 +1601,13 @@ __device__ V3 dihedral_term(const DeviceView& v, const ReplicaParams& p,
     virial = 0.f;
     return v3(0.f, 0.f, 0.f);
   }
-  float cs = dot3(m, n) * (1.0f / sqrtf(qm * qn));
-  cs = fminf(1.0f, fmaxf(-1.0f, cs));
-  float phi = cs == 1.0f ? 0.0f : (cs == -1.0f ? 3.14159265358979323846f : acosf(cs));
-  if (dot3(b0, n) < 0.0f) phi = -phi;
-  const float arg = (float)c.n * phi;
-  energy = c.k * (1.0f + (float)c.d * cosf(arg));
-  const float de = -c.k * (float)c.d * (float)c.n * sinf(arg);
   const float l1 = sqrtf(q1);
+  const float phi = atan2f(l1 * dot3(b0, n), dot3(m, n));
+  const float arg = (float)c.n * phi;
+  float sn, cn;
+  sincosf(arg, &sn, &cn);
+  energy = c.k * (1.0f + (float)c.d * cn);
+  const float de = -c.k * (float)c.d * (float)c.n * sn;
   const V3 fi = scal(-de * l1 / qm, m);
   const V3 fl = scal(de * l1 / qn, n);
   const float inv_q1 = 1.0f / q1;
@@ -1954,11 +2002,13 @@ void launch_list_to_slots(const StepLaunch& l, uint32_t cap, uint32_t* out_count
   check_launch("list_to_slots");
 }
 
-void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post) {
+void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post, int parts) {
   const bool fuse = post && l.fuse_post != 0;
   const int fin = !fuse ? kForcePlain : (l.need_kinetic ? kForcePostKinetic : kForcePost);
-  const bool bonded = l.v.has_bonded != 0;
-  if (l.v.list_by_q) {
+  const bool bonded = l.v.has_bonded != 0 && (parts & kForceBonded) != 0;
+  if ((parts & kForcePair) == 0) {
+    // bonded terms alone (profiling)
+  } else if (l.v.list_by_q) {
     launch_forces_staged(l, observables, clamp, bonded ? kForcePlain : fin);
   } else if (clamp) {
     k_lj<false, kForceClamp, 1, 8, false, 0><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
@@ -1983,7 +2033,7 @@ void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post)
       default: throw std::runtime_error("unsupported pair-force schedule");
     }
   }
-  check_launch("lj");
+  if (parts & kForcePair) check_launch("lj");
   if (bonded) {
 #define BB_BONDED(obs, mode) k_bonded<obs, mode><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v)
     if (observables) {

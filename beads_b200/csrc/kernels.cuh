@@ -37,7 +37,11 @@ void launch_rebuild(const StepLaunch& l, bool force_all, bool count_build = true
 // post: finish the step with the second half-kick, the kinetic-energy total
 // and the per-replica step epilogue -- inside the last force kernel when
 // fuse_post is set, else as a separate k_post launch.
-void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post = false);
+// parts: which force kernels run (kForcePair | kForceBonded; the profiler
+// times them one at a time).
+constexpr int kForcePair = 1, kForceBonded = 2;
+void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post = false,
+                   int parts = kForcePair | kForceBonded);
 void launch_post(const StepLaunch& l, bool kick, bool observables);
 // Staged contexts (list rows by cell order): raise the dynamic shared-memory
 // limit of the staged pair-force kernels, and decode the list into slot rows

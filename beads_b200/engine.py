@@ -261,10 +261,12 @@ class Engine:
         return {"n_replicas": nr.value, "n_particles": nt.value, "stream": st.value or 0}
 
     def profile(self, stage: str, reps: int) -> float:
-        """Mean milliseconds per launch of 'forces', 'step', 'rebuild' or
+        """Mean milliseconds per launch of 'forces', 'step', 'rebuild',
         'forces_kick' (the force kernel as a step runs it, with the second
-        half-kick; velocities and step state are restored afterwards)."""
-        code = {"forces": 0, "step": 1, "rebuild": 2, "forces_kick": 3}[stage]
+        half-kick; velocities and step state are restored afterwards), 'pair'
+        (the pair-force kernel alone) or 'bonded' (the bonded kernel alone)."""
+        code = {"forces": 0, "step": 1, "rebuild": 2, "forces_kick": 3, "pair": 4,
+                "bonded": 5}[stage]
         out = ctypes.c_double()
         _lib.check(self._lib.beads_profile(self._h, code, int(reps), ctypes.byref(out)))
         if code == 1:
@@ -292,7 +294,8 @@ class Engine:
 
     def set_list_staged(self, staged: bool) -> None:
         """Pair forces from shared-memory cell tiles (True) or global gathers
-        (False); the same bits either way (beads_set_list_layout)."""
+        (False); the same bits either way (beads_set_list_layout).  Once set,
+        the autotuner keeps this layout instead of timing both."""
         _lib.check(self._lib.beads_set_list_layout(self._h, 1 if staged else 0))
 
     def list_staged(self) -> bool:

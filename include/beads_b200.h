@@ -257,8 +257,9 @@ BEADS_API int beads_ctx_info(beads_ctx* ctx, uint32_t* n_replicas,
  * list (no observables); 1: one full MD step; 2: one forced neighbour
  * rebuild; 3: the force kernels as a step launches them (with the second
  * half-kick and the kinetic-energy total), velocities and per-replica step
- * state restored afterwards.  Stages 1 and 2 advance or rebuild the state
- * they time. */
+ * state restored afterwards; 4: the pair-force kernel alone; 5: the bonded
+ * kernel alone (forces re-evaluated in full after stages 4 and 5).  Stages 1
+ * and 2 advance or rebuild the state they time. */
 BEADS_API int beads_profile(beads_ctx* ctx, int32_t stage, uint32_t reps,
                             double* avg_ms);
 /* Neighbour-list statistics of the last build over all replicas: total list
@@ -289,7 +290,9 @@ BEADS_API int beads_get_tuning(beads_ctx* ctx, int32_t* schedule);
  * pair-force kernel reads every neighbour position.  Slot layout (0): rows
  * and entries by slot, positions gathered from global memory.  The choice
  * never changes a result; switching rebuilds the list before the next force
- * evaluation.  beads_get_list_layout reports 0 when no replica can stage.
+ * evaluation.  Without a call the autotuner times both layouts at the first
+ * run and keeps the faster; after a call it keeps the layout set here.
+ * beads_get_list_layout reports 0 when no replica can stage.
  * No reference counterpart (the reference keeps one slot-major list,
  * neighbor_list.cuh:12-71). */
 BEADS_API int beads_set_list_layout(beads_ctx* ctx, int32_t staged);

@@ -7,7 +7,8 @@ Builds the workload, runs ``--warm`` MD steps, then calls
 ``Engine.profile(stage, reps)`` between cudaProfilerStart and
 cudaProfilerStop, so a profiler started with ``--profile-from-start off``
 sees exactly those launches.  Prints the mean milliseconds per launch.
-Stages: forces, forces_kick, rebuild, step (see ``Engine.profile``).
+Stages: forces, forces_kick, rebuild, step, pair, bonded (see
+``Engine.profile``).
 """
 
 from __future__ import annotations
@@ -46,7 +47,8 @@ def main(argv: list[str] | None = None) -> dict:
                         choices=["fit-mixture", "lattice", "replicas", "melt", "mixture"])
     parser.add_argument("--beads", type=int, default=524288)
     parser.add_argument("--stage", default="rebuild",
-                        choices=["forces", "forces_kick", "rebuild", "step"])
+                        choices=["forces", "forces_kick", "rebuild", "step", "pair",
+                                 "bonded"])
     parser.add_argument("--reps", type=int, default=1)
     parser.add_argument("--warm", type=int, default=20)
     parser.add_argument("--schedule", default="2,0,4,1",
