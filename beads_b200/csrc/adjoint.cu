@@ -71,6 +71,9 @@ struct AdjView {
   long long* theta;
   const float4* ck_ref_pos;
   const int* list_src;   // per replica: -1 checkpoint build positions, else step index
+  const uint32_t* snap_nbr;  // list snapshots (null: the current list, rebuilt per step)
+  const uint32_t* snap_cnt;
+  uint64_t snap_entries;     // list entries per snapshot
   const int* shift_on;   // per replica: LJ energy shift active
   long long* dot;        // [2 lanes][R][whole, frac]: sum u_bar . v, double-buffered
   long long* theta_bond;      // [global bond type][k, r0][whole, frac]
@@ -105,6 +108,27 @@ __global__ void k_adj_list_positions(DeviceView v, AdjView a, uint32_t segment,
   const int src = a.list_src[r];
   v.pos[i] = src < 0 ? a.ck_ref_pos[(size_t)segment * a.slots + i]
                      : a.seg_pos[(size_t)src * a.slots + i];
+}
+
+// Copies the list rows (and counts) of slot block b into snapshot k: every
+// block when `all`, else the blocks of replicas that rebuilt their list in
+// the step just run.  A block's 128 rows are one contiguous run of the
+// interleaved list (4 whole groups of 32 rows).
+__global__ void k_adj_snapshot(DeviceView v, uint32_t* snap_nbr, uint32_t* snap_cnt,
+                               uint32_t k, int all) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  if (!all && !v.rs[r].need_rebuild) return;
+  const size_t entries = (size_t)kBlock * v.nbr_stride;
+  const size_t base = (size_t)b * entries;
+  const size_t per_snap = (size_t)v.n_slots * v.nbr_stride;
+  const uint4* src = reinterpret_cast<const uint4*>(v.nbr + base);
+  uint4* dst = reinterpret_cast<uint4*>(snap_nbr + (size_t)k * per_snap + base);
+  for (size_t t = threadIdx.x; t < entries / 4; t += blockDim.x) dst[t] = __ldcs(src + t);
+  if (threadIdx.x < kBlock) {
+    const size_t i = (size_t)b * kBlock + threadIdx.x;
+    snap_cnt[(size_t)k * v.n_slots + i] = v.nbr_count[i];
+  }
 }
 
 // Crossing counts of restored slots: img - ref_img of the checkpoint.
@@ -248,11 +272,20 @@ k_adj_lj(DeviceView v, AdjView a, const float4* __restrict__ pos, uint32_t m, ui
   const int ti = __float_as_int(xi.w);
   const AdjCoeff* row = table + ti * kNt;
   const float4 fi = a.fbar[i];
-  const uint32_t n = real ? v.nbr_count[i] : 0u;  // every thread of the particle
+  // The list forward step m used: its snapshot, or the current (rebuilt) list.
+  const uint32_t* nbr = v.nbr;
+  const uint32_t* cnt = v.nbr_count;
+  if (a.snap_nbr != nullptr) {
+    const int src = a.list_src[r];
+    const size_t s = src < 0 ? 0u : (size_t)src;
+    nbr = a.snap_nbr + s * a.snap_entries;
+    cnt = a.snap_cnt + s * v.n_slots;
+  }
+  const uint32_t n = real ? cnt[i] : 0u;  // every thread of the particle
   const uint32_t n_warp = __reduce_max_sync(kFull, n);
   const float hmin = fminf(p.half[0], fminf(p.half[1], p.half[2]));
   const float half_min_sq = hmin * hmin;
-  const uint32_t* list = v.nbr + nbr_index(i, 0, v.nbr_stride);
+  const uint32_t* list = nbr + nbr_index(i, 0, v.nbr_stride);
   constexpr uint32_t kU = 4;
   uint32_t jn[kU];
 #pragma unroll
@@ -606,7 +639,8 @@ void Engine::adjoint_segment_storage(uint32_t K) {
   if (A.seg_capacity >= K + 1) return;
   clear_replay_graphs();  // they record into the buffers replaced here
   A.seg_capacity = K + 1;
-  A.seg_pos = A.alloc<float4>(static_cast<size_t>(K + 1) * S);
+  // one spare entry: a list entry naming the far particle (slot S) stays in bounds
+  A.seg_pos = A.alloc<float4>(static_cast<size_t>(K + 1) * S + 1);
   A.seg_vel = A.alloc<float4>(static_cast<size_t>(K + 1) * S);
   A.seg_lam = A.alloc<double>(static_cast<size_t>(K + 1) * R);
   A.seg_kin = A.alloc<double>(static_cast<size_t>(K + 1) * R);
@@ -628,6 +662,7 @@ cudaGraphExec_t Engine::replay_graph_for(uint32_t steps) {
   cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
   try {
     adjoint_record(0);
+    adjoint_snapshot(0, true);
     for (uint32_t k = 1; k <= steps; ++k) {
       if (use_conditional_) {
         record_step_conditional(false);
@@ -635,6 +670,7 @@ cudaGraphExec_t Engine::replay_graph_for(uint32_t steps) {
         record_step(false);
       }
       adjoint_record(k);
+      adjoint_snapshot(k, false);
     }
     cuda_check(cudaStreamEndCapture(stream_, &graph), "end capture");
     cuda_check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
@@ -659,6 +695,15 @@ void Engine::adjoint_record(uint32_t k) {
   k_adj_record<<<(A.replicas + 127) / 128, 128, 0, stream_>>>(v_, A.seg_lam, A.seg_kin,
                                                                A.seg_flags, k);
   launch_check("adjoint record");
+}
+
+// Snapshot k of the list (see k_adj_snapshot); nothing when the backward
+// pass rebuilds its lists instead.
+void Engine::adjoint_snapshot(uint32_t k, bool all) {
+  AdjointStore& A = *adj_;
+  if (!A.snap_on) return;
+  k_adj_snapshot<<<v_.n_blocks, 256, 0, stream_>>>(v_, A.snap_nbr, A.snap_cnt, k, all ? 1 : 0);
+  launch_check("adjoint list snapshot");
 }
 
 // Puts the particle state of checkpoint c back, with the neighbour list the
@@ -811,10 +856,35 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
   const uint32_t K = A.every;
 
   adjoint_segment_storage(K);
+  // List snapshots for the reverse sweep when the device holds K + 1 of them
+  // with room to spare (a replayed segment records them; storing every step
+  // in the forward pass has no replay and rebuilds instead).
+  {
+    const uint64_t want = static_cast<uint64_t>(K) + 1u;
+    const uint64_t bytes = want * S * (static_cast<uint64_t>(v_.nbr_stride) + 1u) * 4u;
+    bool on = false;
+    if (!A.store_all) {
+      if (A.snap_capacity >= want) {
+        on = true;
+      } else {
+        size_t free_b = 0, total_b = 0;
+        cuda_check(cudaMemGetInfo(&free_b, &total_b), "memory info");
+        if (bytes <= free_b / 2) {
+          clear_replay_graphs();  // they copy into the buffers replaced here
+          A.snap_nbr = A.alloc<uint32_t>(want * S * v_.nbr_stride);
+          A.snap_cnt = A.alloc<uint32_t>(want * S);
+          A.snap_capacity = static_cast<uint32_t>(want);
+          on = true;
+        }
+      }
+    }
+    if (on != A.snap_on) clear_replay_graphs();  // they hold (or lack) the snapshot copies
+    A.snap_on = on;
+  }
   if (!A.xbar) {
     A.xbar = A.alloc<float4>(S);
     A.vbar = A.alloc<float4>(S);
-    A.fbar = A.alloc<float4>(S);
+    A.fbar = A.alloc<float4>(S + 1);  // + the far particle's (zero) entry
     A.ubar = A.alloc<float4>(S);
     A.theta = A.alloc<long long>(static_cast<size_t>(R) * kAdjTypes * kAdjTypes * 4);
     A.tag_xfer = A.alloc<float>(3 * n_tags_);
@@ -866,6 +936,9 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
   av.theta = A.theta;
   av.ck_ref_pos = A.ck_ref_pos;
   av.list_src = nullptr;
+  av.snap_nbr = A.snap_on ? A.snap_nbr : nullptr;
+  av.snap_cnt = A.snap_on ? A.snap_cnt : nullptr;
+  av.snap_entries = static_cast<uint64_t>(S) * v_.nbr_stride;
   av.shift_on = d_shift;
   av.dot = A.dot;
   av.theta_bond = A.theta_bond;
@@ -890,9 +963,11 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
                    "replay launch");
       } else {
         adjoint_record(0);
+        adjoint_snapshot(0, true);
         for (uint64_t k = 1; k <= b - a; ++k) {
           launch_chunk(1, false);
           adjoint_record(static_cast<uint32_t>(k));
+          adjoint_snapshot(static_cast<uint32_t>(k), false);
         }
       }
     }
@@ -934,9 +1009,9 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
                           cudaMemcpyHostToDevice), "adjoint list sources");
     for (uint64_t m = b + 1; m-- > m_lo;) {
       const uint32_t k = static_cast<uint32_t>(m - a);
-      if (any_k[k]) {
-        AdjView lv = av;
-        lv.list_src = A.seg_src + static_cast<size_t>(k) * R;
+      AdjView lv = av;
+      lv.list_src = A.seg_src + static_cast<size_t>(k) * R;
+      if (any_k[k] && !A.snap_on) {
         k_adj_list_positions<<<v_.n_blocks, kBlock, 0, stream_>>>(
             v_, lv, static_cast<uint32_t>(s), A.seg_changed + static_cast<size_t>(k) * R);
         launch_check("adjoint list positions");
@@ -957,10 +1032,10 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
       const dim3 grid(v_.n_blocks);
       const uint32_t mm = static_cast<uint32_t>(m);
       if (A.max_types <= 2) {
-        k_adj_lj<2, 1><<<grid, kBlock, 0, stream_>>>(v_, av, pos_m, mm, k, first, lane_out,
+        k_adj_lj<2, 1><<<grid, kBlock, 0, stream_>>>(v_, lv, pos_m, mm, k, first, lane_out,
                                                      !bonded);
       } else {
-        k_adj_lj<4, 1><<<grid, kBlock, 0, stream_>>>(v_, av, pos_m, mm, k, first, lane_out,
+        k_adj_lj<4, 1><<<grid, kBlock, 0, stream_>>>(v_, lv, pos_m, mm, k, first, lane_out,
                                                      !bonded);
       }
       launch_check("adjoint pair");

@@ -5,7 +5,9 @@
 // time from its checkpoint, recording positions, velocities, Berendsen scales
 // and kinetic energies of every step of the segment, then walks the segment
 // backwards.  Memory: (segments + 1) checkpoints of 80 bytes per slot plus
-// K + 1 recorded steps of 32 bytes per slot.
+// K + 1 recorded steps of 32 bytes per slot; when the device has room, K + 1
+// list snapshots of 4 (max_neighbors + 1) bytes per slot, so the reverse
+// sweep reads each step's list instead of rebuilding it.
 #pragma once
 
 #include <cstdint>
@@ -46,6 +48,14 @@ struct AdjointStore {
   int* seg_src = nullptr;        // [k * R + r] step whose positions built step a+k's list
   uint32_t* seg_changed = nullptr;  // [k * R + r] that list differs from step a+k+1's
   uint32_t seg_capacity = 0;     // K + 1 allocated
+
+  // list snapshots of one replayed segment: snapshot 0 holds every replica's
+  // list at the segment start, snapshot k the rows of the replicas that
+  // rebuilt at step a+k (the other rows of snapshot k are not used)
+  uint32_t* snap_nbr = nullptr;  // [k][slots * stride], the list layout of DeviceView::nbr
+  uint32_t* snap_cnt = nullptr;  // [k][slots]
+  uint32_t snap_capacity = 0;    // snapshots allocated (0: lists are rebuilt)
+  bool snap_on = false;          // the current backward pass uses the snapshots
 
   // adjoint vectors (per slot) and reductions
   float4* xbar = nullptr;

@@ -164,6 +164,7 @@ class Engine {
   void set_sort_enabled(bool on);
   void adjoint_restore(uint32_t segment);
   void adjoint_record(uint32_t k);
+  void adjoint_snapshot(uint32_t k, bool all);
   void adjoint_segment_storage(uint32_t K);
   void adjoint_select_list(uint32_t a, uint32_t m, std::vector<int>& current,
                            const std::vector<uint32_t>& flags);

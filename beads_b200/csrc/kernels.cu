@@ -129,7 +129,13 @@ __global__ void k_decide(DeviceView v, cudaGraphConditionalHandle cond, int use_
   const unsigned exceeded = st->exceeded;
   st->exceeded = 0u;
   unsigned need = 0u;
-  if (kMode == kPreDescent || p.skin == 0.0f) {
+  if (st->status & (kStatusNonFinite | kStatusFixedOverflow)) {
+    // The state has failed (non-finite velocities, or a value beyond the
+    // fixed-point range): no more list builds for this replica, whose
+    // coordinates may no longer be finite; the host raises at the end of the
+    // chunk.
+    need = 0u;
+  } else if (kMode == kPreDescent || p.skin == 0.0f) {
     need = (kMode == kPreDescent) ? exceeded : 1u;
   } else if (check_step) {
     const bool first = st->checks_since_build == 0u;
@@ -348,16 +354,20 @@ __device__ __forceinline__ void sort_cell(const DeviceView& v, const ReplicaPara
         v.pos2[s0 + rank] = v.pos[key];
       }
     } else {
-      if (lane == 0) {
-        for (uint32_t a = s0 + 1; a < s1; ++a) {
-          const uint32_t key = v.cell_atoms[a];
-          uint32_t q = a;
-          while (q > s0 && v.cell_atoms[q - 1] > key) {
-            v.cell_atoms[q] = v.cell_atoms[q - 1];
-            --q;
-          }
-          v.cell_atoms[q] = key;
-        }
+      // A crowded cell: its members in ascending slot order are the slots of
+      // the replica whose cell is c, in the order a scan of the replica meets
+      // them; the warp scans cell_of_slot 32 slots at a time and compacts the
+      // matches by ballot (work linear in the replica's size, whatever the
+      // occupancy).
+      const uint32_t cg = p.cell_begin + c;
+      const uint32_t lt = (1u << lane) - 1u;
+      uint32_t at = s0;
+      for (uint32_t b0 = p.atom_begin; b0 < p.atom_begin + p.n_atoms && at < s1; b0 += 32u) {
+        const uint32_t s = b0 + lane;
+        const bool in = s < p.atom_begin + p.n_atoms && v.cell_of_slot[s] == cg;
+        const uint32_t m = __ballot_sync(kFull, in);
+        if (in && at + __popc(m & lt) < s1) v.cell_atoms[at + __popc(m & lt)] = s;
+        at += __popc(m);
       }
       __syncwarp();
       for (uint32_t q = s0 + lane; q < s1; q += 32u) v.pos2[q] = v.pos[v.cell_atoms[q]];
@@ -791,16 +801,22 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
       for (int t = 0; t < 2 * kBuildPairs; ++t) {
         const uint32_t u = base + 32u * t + lane;
         while (seg[t] < nseg && u >= sh.seg_end[seg[t]]) ++seg[t];
-        // Past the stream: an infinite coordinate fails every distance test.
-        uint32_t j = 0xffffffffu;
+        // Past the stream: an infinite coordinate fails every distance test
+        // against a finite home particle.  Its slot and entry are the far
+        // particle's (pos[n_slots], or the stage's last entry), so even a
+        // home particle with non-finite coordinates, which accepts every
+        // candidate (r^2 NaN is not above the cutoff, the reference's rule),
+        // lists only valid indices.
+        uint32_t j = v.n_slots;
         float4 x = make_float4(INFINITY, 0.f, 0.f, 0.f);
         const uint32_t st = min(seg[t], kMaxSegments - 1u);
         const uint32_t qc = sh.seg_q[st] + u;
+        uint32_t e = staged_group ? sh.lay.size : v.n_slots;
         if (u < total) {
           j = v.cell_atoms[qc];
           x = v.pos2[qc];
+          e = staged_group ? qc + sh.delta[st] : j;
         }
-        const uint32_t e = staged_group ? qc + sh.delta[st] : j;
         const float sx = form == kBuildShifted ? sh.seg_s[0][st] : 0.f;
         const float sy = form == kBuildShifted ? sh.seg_s[1][st] : 0.f;
         const float sz = form == kBuildShifted ? sh.seg_s[2][st] : 0.f;

@@ -50,6 +50,7 @@ UNIT = "atom-steps/s"
 N_BEADS = 1_048_576
 E2E_STEPS = 100  # MD steps per end-to-end call
 GRAPH_WARMUP = 31  # untimed steps that instantiate every captured step graph
+REF_MIN_STEPS = 60  # fewest timed MD steps of the host-core reference arm
 CLOCK_WINDOW_S = 0.6  # shortest stretch of load the clock sampler sees
 WORKLOAD = ("binary LJ mixture, 1,048,576 beads per GPU, nm_kjmol, 80/20 types, box 37.2 nm, "
             "rc 0.9 (shifted), skin 0.1, max_neighbors 128, sort every rebuild, Berendsen 120 K "
@@ -154,15 +155,21 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def _load_until(eng, since: float, window_s: float = CLOCK_WINDOW_S) -> int:
-    """Keeps the GPU stepping (untimed) until `window_s` seconds have passed
+def _load_until(eng, since: float, window_s: float = CLOCK_WINDOW_S, stepping: bool = True) -> int:
+    """Keeps the GPU busy (untimed) until `window_s` seconds have passed
     since `since`, so a 200 ms clock sampler sees the kernels under load even
-    when the timed steps take a few milliseconds.  Returns the extra steps."""
+    when the timed steps take a few milliseconds: MD steps, or (stepping =
+    False) force evaluations of the current state, which leave the
+    trajectory where the timed steps ended.  Returns the extra steps or
+    evaluations."""
     import torch
 
     extra = 0
     while time.perf_counter() - since < window_s:
-        eng.run(16)
+        if stepping:
+            eng.run(16)
+        else:
+            eng.profile("forces", 16)
         torch.cuda.synchronize()
         extra += 16
     return extra
@@ -297,17 +304,20 @@ def run_reference(args) -> None:
     for _ in range(args.warmup):
         sim.step(1)
     builds0 = sim.state()[3]
+    # At least REF_MIN_STEPS timed steps, so the sample holds list rebuilds
+    # (this workload rebuilds every ~25 steps) like the GPU arm's timing.
+    n_steps = max(args.steps, REF_MIN_STEPS)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(n_steps):
         sim.step(1)
     total = time.perf_counter() - t0
     builds = sim.state()[3] - builds0
     sim.close()
     n = spec.n
-    value = n * args.steps / total
+    value = n * n_steps / total
     cores = O.num_threads()
     sample = (f"the whole {n}-bead workload, relaxed on the host ({prep_s:.0f} s, untimed), "
-              f"{args.warmup} warm-up + {args.steps} timed MD steps, {builds} neighbour "
+              f"{args.warmup} warm-up + {n_steps} timed MD steps, {builds} neighbour "
               "rebuilds in the timed steps; FP64 oracle port with OpenMP")
     reference_cuda = None
     if not args.no_reference_cuda:
@@ -328,9 +338,9 @@ def run_reference(args) -> None:
         "value": value,
         "unit": UNIT,
         "n_gpus": world,
-        "steps": args.steps,
+        "steps": n_steps,
         "warmup": args.warmup,
-        "ms_per_step": 1e3 * total / args.steps,
+        "ms_per_step": 1e3 * total / n_steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
@@ -346,17 +356,19 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
-def _energy_drift(spec, eng, steps: int = 2000, every: int = 100) -> dict:
+def _energy_drift(spec, eng, steps: int = 2000, every: int = 100, time_unit: str = "ns",
+                  state: dict | None = None) -> dict:
     """Energy drift of the workload's dynamics: an NVE copy (Berendsen off,
     which would otherwise add or remove energy) of the engine's current state
     runs `steps` steps with a thermo row every `every` steps; the drift is the
-    least-squares slope of the total energy per bead against time."""
+    least-squares slope of the total energy per bead against time (time_unit
+    "ns" for nm_kjmol inputs, whose dt is in ps; "tau" for reduced units)."""
     import dataclasses
 
     from beads_b200 import workloads
     from beads_b200.engine import Engine
 
-    st = eng.state()
+    st = eng.state() if state is None else state
     box = np.asarray(spec.box_bound, np.float64)
     nve = dataclasses.replace(
         spec, thermostat=None, images=st["images"],
@@ -367,13 +379,16 @@ def _energy_drift(spec, eng, steps: int = 2000, every: int = 100) -> dict:
         for _ in range(steps // every):
             rows.append(e.run(every, every)[0])
     etot = np.array([r["pe"] + r["ke"] for r in rows], np.float64) / spec.n
-    t_ns = np.arange(len(rows)) * every * spec.dt / 1000.0  # dt in ps
-    slope = float(np.polyfit(t_ns, etot, 1)[0])
-    return {"value": slope, "unit": "kJ/mol per bead per ns", "steps": steps,
-            "dt_ps": spec.dt, "e_total_per_bead_start": float(etot[0]),
+    scale = 1.0 / 1000.0 if time_unit == "ns" else 1.0  # dt in ps, or in tau
+    t = np.arange(len(rows)) * every * spec.dt * scale
+    slope = float(np.polyfit(t, etot, 1)[0])
+    unit = "kJ/mol per bead per ns" if time_unit == "ns" else "epsilon per bead per tau"
+    return {"value": slope, "unit": unit, "steps": steps,
+            "dt": spec.dt, "e_total_per_bead_start": float(etot[0]),
             "e_total_per_bead_end": float(etot[-1]),
             "relative_change": float((etot[-1] - etot[0]) / abs(etot[0])),
-            "ensemble": "NVE copy (Berendsen off) of the engine state after the timed steps, "
+            "ensemble": "NVE copy (Berendsen off) of the engine state after the timed steps "
+                        "(the relaxed start for the melt), "
                         "float32 pair math, fixed-point totals"}
 
 
@@ -697,6 +712,15 @@ def run_chains(args) -> None:
     spec = workloads.relaxed(workloads.polymer_melt(seed=5, growth="lockstep"))
     eng = Engine(spec)
     stream = torch.cuda.ExternalStream(eng.info()["stream"], device=torch.device("cuda", local))
+    # The relaxed start, kept on the host: the end-to-end calls and the drift
+    # run start from it.  This melt's dynamics are stable for a few hundred
+    # steps only (a bond angle reaching 180 degrees makes the harmonic
+    # dihedral force diverge; the reference's float32 build stops at step
+    # ~150 on the same input), so every leg stays inside that window.
+    pin_pos = torch.empty((spec.n, 3), dtype=torch.float32, pin_memory=True)
+    pin_vel = torch.empty((spec.n, 3), dtype=torch.float32, pin_memory=True)
+    eng.download_all(pin_pos.numpy(), pin_vel.numpy())
+    start_state = eng.state()
     eng.run(max(3, args.warmup))
     eng.run(GRAPH_WARMUP)
     builds_before = eng.counters(0)["builds"]
@@ -704,17 +728,58 @@ def run_chains(args) -> None:
     sampler = ClockSampler(local)
     torch.cuda.synchronize()
     sampler.start()
+    t_sample = time.perf_counter()
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     start.record(stream)
     eng.run(args.steps)
     stop.record(stream)
     stop.synchronize()
+    clock_extra = _load_until(eng, t_sample, stepping=False)
     clocks = sampler.stop()
+    clocks["untimed_force_evaluations_after_timed"] = clock_extra
     ms = start.elapsed_time(stop)
     builds = eng.counters(0)["builds"] - builds_before
     chains = eng.counters()["chain_launches"] - chains_before
     schedule = eng.tuning()
+    stats = eng.list_stats()
+    mean_nbr = stats["entries"] / spec.n
+
+    # The two force kernels timed alone on the current list; the roofline is
+    # the slower one's, against its algorithmic bytes per bead.
+    pair_ms = eng.profile("pair", 50)
+    bonded_ms = eng.profile("bonded", 50)
+    pair_bytes = 4.0 * mean_nbr + 36.0
+    bonded_bytes = _bonded_bytes_per_bead(spec)
+    if bonded_ms >= pair_ms:
+        kname, kms, kbytes = "k_bonded (harmonic bonds, angles, dihedrals)", bonded_ms, bonded_bytes
+    else:
+        kname, kms, kbytes = "k_lj (pair forces)", pair_ms, pair_bytes
+    achieved = spec.n * kbytes / (kms / 1e3) / 1e9
+    peak, peak_kind = _peaks()
+
+    # End to end through the C ABI with host buffers, as for the mixture,
+    # each call from the relaxed start.
+    e2e_calls = 0 if args.no_e2e else max(2, args.steps // (4 * E2E_STEPS))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_calls):
+        eng.upload_all(pin_pos.numpy(), pin_vel.numpy())
+        eng.run(E2E_STEPS)
+        eng.download_all(pin_pos.numpy(), pin_vel.numpy())
+    torch.cuda.synchronize()
+    e2e_wall = time.perf_counter() - t0
+    e2e_value = spec.n * E2E_STEPS * e2e_calls / e2e_wall if e2e_calls else None
+    drift = None
+    if not args.no_drift:
+        try:
+            drift = _energy_drift(spec, None, steps=200, every=20, time_unit="tau",
+                                  state=start_state)
+        except OverflowError as e:
+            # Without the thermostat the relaxed melt's released bending
+            # energy heats it until a dihedral diverges.
+            drift = {"unavailable": f"the NVE copy of the relaxed melt diverged within 200 "
+                                    f"steps: {e}"[:300]}
     eng.close()
     line = {
         "metric": CHAINS_METRIC,
@@ -744,10 +809,49 @@ def run_chains(args) -> None:
         # projection and list build per rebuild chain.
         "gpu_launches": (5 if schedule["fuse_post"] else 6) * args.steps + 8 * int(chains),
         "clocks": clocks,
+        "roofline": {
+            "bound": "hbm",
+            "kernel": kname,
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": None,
+            "peak_kind": peak_kind,
+            "bytes_per_atom": kbytes,
+            "kernel_ms": kms,
+            "pair_ms": pair_ms,
+            "bonded_ms": bonded_ms,
+            "pair_bytes_per_atom": pair_bytes,
+            "bonded_bytes_per_atom": bonded_bytes,
+            "mean_neighbors": round(mean_nbr, 3),
+        },
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": 2 * spec.n * 3 * 4 / E2E_STEPS,
+                "d2h_bytes_per_step": 2 * spec.n * 3 * 4 / E2E_STEPS,
+                "md_steps_per_call": E2E_STEPS, "calls": e2e_calls,
+                "call": "beads_upload_all (pinned host positions + velocities) -> "
+                        "beads_run(100) -> beads_download_all, per call"},
     }
+    if drift is not None:
+        line["energy_drift"] = drift
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = _cpu_baseline_melt(spec, args.cpu_budget)
     print(json.dumps(line))
+
+
+def _bonded_bytes_per_bead(spec) -> float:
+    """Algorithmic bytes per bead of the bonded kernel, each array element
+    counted once: the bead's tag, its two term offsets and force (read and
+    written), one 4-byte membership word per term it belongs to, the 16-byte
+    term records (and 4-byte dihedral types) once each, the tag-to-slot map
+    and the positions the terms read."""
+    n = spec.n
+    nb = 0 if spec.bonds is None else len(spec.bonds)
+    na = 0 if spec.angles is None else len(spec.angles)
+    nd = 0 if spec.dihedrals is None else len(spec.dihedrals)
+    memberships = 2 * nb + 3 * na + 4 * nd
+    return (4 + 8 + 32 + 4 + 16) + (4.0 * memberships + 16.0 * (nb + na + nd) + 4.0 * nd) / n
 
 
 def adjoint_metric(world: int) -> str:
@@ -797,6 +901,15 @@ def run_adjoint(args) -> None:
         stream = torch.cuda.ExternalStream(eng.info()["stream"],
                                            device=torch.device("cuda", local))
         eng.run(max(3, args.warmup))
+        autotuned_staged = eng.list_staged()
+        # One untimed differentiated run of two segments first: it switches
+        # the context to the list layout the adjoint reads (slot rows) and
+        # instantiates the segment replay graph, so neither the plain nor the
+        # differentiated timing below includes graph capture.
+        warm = trajectory_observables(eng, eps.detach(), sig.detach().clone().requires_grad_(True),
+                                      x0.clone(), v0.clone(), steps=min(2 * every, steps),
+                                      record_from=1, checkpoint_every=every)
+        warm.sum().backward()
         eng.run(GRAPH_WARMUP)
         # plain forward of the same length from the same start
         eng.upload_all(x0.numpy().astype(np.float32), v0.numpy().astype(np.float32))
@@ -837,6 +950,7 @@ def run_adjoint(args) -> None:
     x2 = x0.clone().requires_grad_(True)
     with Engine(specs) as eng2:
         eng2.set_tuning(**{k: v for k, v in schedule.items() if k not in ("autotuned", "staged")})
+        eng2.set_list_staged(False)
         eng2.run(max(3, args.warmup))
         eng2.run(GRAPH_WARMUP)
         torch.cuda.synchronize()
@@ -877,6 +991,9 @@ def run_adjoint(args) -> None:
             "parallelism": (f"one batch split over {world} GPUs by atom count, gradients "
                             "all-reduced" if world > 1 else "replicas in one batch"),
             "plain_forward_s": plain_s,
+            "plain_forward_layout": "slot rows (the adjoint's; the autotuner had picked "
+                                    + ("the staged" if autotuned_staged else "the slot")
+                                    + " layout)",
             "adjoint_forward_s": fwd_s,
             "backward_s": bwd_s,
             "backward_over_plain_forward": bwd_s / plain_s,

@@ -7,6 +7,9 @@
     native/src/simulation/neighbor/neighbor_system.cpp:143.)  The overflow
     itself is an ordinary status bit: the build clamps its writes at the
     capacity, so nothing runs out of bounds.
+  * A replica whose state has failed (a kinetic energy beyond the
+    fixed-point range) builds no more lists: the rest of the chunk steps on
+    the last list, and the error arrives at the chunk's end.
   * An interrupt (a pending signal, as Ctrl-C leaves it) stops
     execute_simulation at the next poll, well before the run would end (the
     reference polls every max(1, 100000 / N) steps,
@@ -86,3 +89,34 @@ def test_interrupt_stops_execute_simulation(tmp_path, monkeypatch):
     # 2,000,000 steps of 4096 beads take about a minute; the poll stops it
     # within a few chunks of the signal.
     assert elapsed < 15.0, elapsed
+
+
+def test_failed_state_stops_list_builds():
+    import numpy as np
+
+    import dataclasses
+
+    # Berendsen on: the kinetic-energy total (fixed point) is formed every
+    # step, so the failure is a status bit inside the chunk.
+    spec = dataclasses.replace(workloads.lj_lattice(check_every=1), thermostat=(1.0, 1.0))
+    with Engine(spec) as eng:
+        eng.eval()
+        pos = eng.state()["positions"].copy()
+        # Two particles 0.05 sigma apart: energy (1.6e16) and virial (2e16)
+        # are inside the fixed-point range at the evaluation, but the first
+        # kick gives them ~1e16 sigma/tau, whose kinetic energy is not; the
+        # next drifts throw them across the box, a rebuild on every step if
+        # builds went on.
+        pos[1] = pos[0] + np.array([0.05, 0.0, 0.0], np.float32)
+        eng.set_state(0, positions=pos)
+        eng.eval()
+        builds0 = eng.counters()["builds"]
+        with pytest.raises(OverflowError):
+            eng.run(4 * CHUNK)
+        c = eng.counters()
+    # Step 1 may rebuild (its decision comes before the failing kick); none of
+    # the later steps of the chunk does, and the error arrives within two
+    # chunks.
+    assert c["steps"] >= 2, c
+    assert c["builds"] <= builds0 + 1, (builds0, c)
+    assert c["steps"] <= 2 * CHUNK, c
