@@ -260,9 +260,17 @@ def _cpu_baseline_melt(spec, budget_s: float):
                 dt=spec.dt, skin=spec.cutoff_buffer, check_every=spec.rebuild_check_every,
                 bonds=spec.bonds, angles=spec.angles, dihedrals=spec.dihedrals,
                 thermostat=True, kt_target=spec.thermostat[0], tau=spec.thermostat[1])
-    rate, wall = _cpu_rate(sim, spec.n, 1)
-    steps = max(1, int(budget_s / max(wall, 1e-3)))
-    rate, wall = _cpu_rate(sim, spec.n, steps)
+    sim.step(1)
+    # One step at a time until the budget is spent (at most 100 steps): the
+    # melt rebuilds its list every few steps, so the first step's time does
+    # not predict the rest, and the melt diverges after a few hundred steps.
+    steps, wall = 0, 0.0
+    t0 = time.perf_counter()
+    while wall < budget_s and steps < 100:
+        sim.step(1)
+        steps += 1
+        wall = time.perf_counter() - t0
+    rate = spec.n * steps / wall
     sim.close()
     return {"value": rate, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
             "sample": f"{steps} MD steps of the full {spec.n}-bead melt (after one untimed "
@@ -729,13 +737,18 @@ def run_chains(args) -> None:
     torch.cuda.synchronize()
     sampler.start()
     t_sample = time.perf_counter()
+    profile_region = os.environ.get("BEADS_PROFILE_TIMED") == "1"
+    if profile_region:  # lets a profiler started with capture off see only these steps
+        torch.cuda.profiler.start()
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     start.record(stream)
     eng.run(args.steps)
     stop.record(stream)
     stop.synchronize()
-    clock_extra = _load_until(eng, t_sample, stepping=False)
+    if profile_region:
+        torch.cuda.profiler.stop()
+    clock_extra = 0 if profile_region else _load_until(eng, t_sample, stepping=False)
     clocks = sampler.stop()
     clocks["untimed_force_evaluations_after_timed"] = clock_extra
     ms = start.elapsed_time(stop)
