@@ -4,8 +4,8 @@
 // derivative parts of a term's force, energy and virial are then exact
 // directional derivatives (Jacobian-vector products, parameter derivatives).
 //
-// The term conventions are the step kernels' (kernels.cu, bond_term /
-// angle_term / dihedral_term, after native/src/forcefield/bond/
+// The term conventions are the step kernels' (kernels.cu, bond_forces /
+// angle_forces / dihedral_forces, after native/src/forcefield/bond/
 // bond_harmonic.cu:24-99, angle/angle_harmonic.cu:54-178 and
 // dihedral/dihedral_harmonic.cu:65-227): arms are minimum-image differences
 // of member positions, cos clamped to [-1, 1], sin floored at 1e-3, singular

@@ -23,6 +23,7 @@ constexpr int kGroup = BEADS_NBR_GROUP;
 static_assert(kGroup == 8 || kGroup == 16 || kGroup == 32, "interleave of 8, 16 or 32 rows");
 constexpr int kMaxTypes = 16;        // LJ type table held in shared memory
 constexpr uint32_t kKeBuckets = 128; // fixed-point kinetic-energy buckets per replica
+constexpr uint32_t kScanChunk = 4096;  // cells per block of the cell-count scan
 // Coordinates of the far particle at pos[n_slots] (pads neighbour batches);
 // its squared distance to any particle is ~3e36, above kFarR2.
 constexpr float kFarCoord = 1.0e18f;
@@ -88,6 +89,7 @@ struct ReplicaParams {
   int32_t n_types;
   uint32_t bond_type_base, angle_type_base, dihedral_type_base;
   uint32_t staged;           // pair forces from a shared-memory stage (kernels.cu)
+  uint32_t sparse;           // lists built one thread per particle (k_build_sparse)
 };
 
 // Mutable per-replica device state.
@@ -162,6 +164,14 @@ struct DeviceView {
   uint32_t* cross;  // net boundary crossings since the last build (see pack_cross)
   uint32_t* work_start;  // [n_replicas + 1] first work item (cell) of each rebuilding
                          // replica, then the total
+  // Cell-count scan in chunks of kScanChunk cells: chunk b belongs to
+  // replica scan_chunk_replica[b]; replica r's chunks start at
+  // scan_chunk_first[r]; scan_chunk_sum[b] holds the chunk's count total, then
+  // its exclusive prefix inside the replica.
+  const uint32_t* scan_chunk_replica;
+  const uint32_t* scan_chunk_first;
+  uint32_t* scan_chunk_sum;
+  uint32_t n_scan_chunks;
   // reorder scratch
   float4* pos2;
   float4* vel2;
@@ -193,6 +203,12 @@ struct DeviceView {
   const uint4* angles;       // (tag_i, tag_j, tag_k, type)
   const uint4* dihedrals;    // (tag_i, tag_j, tag_k, tag_l)
   const uint32_t* dihedral_type;
+  uint32_t n_bond_terms, n_angle_terms, n_dihedral_terms;
+  // term_mem: membership entry (index into term / term_off ranges) of every
+  // (term, member): bonds [2 nb], then angles [3 na], then dihedrals [4 nd].
+  const uint32_t* term_mem;
+  float4* bonded_contrib;    // per membership entry: force on the member, energy (first member)
+  float* bonded_vir;         // per membership entry: the term's virial (first member)
   const BondCoeff* bond_coeff;
   const AngleCoeff* angle_coeff;
   const DihedralCoeff* dihedral_coeff;

@@ -389,6 +389,26 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
     stage_cap_ = cap;
     staged_ = cap > 0;
   }
+  // List build form per replica: a thread per particle (k_build_sparse) when
+  // its cells hold fewer than kSparseOccupancy particles on average, else a
+  // warp per cell (k_build); both write the same lists.  BEADS_BUILD=dense or
+  // =sparse forces one form for every replica of the process.
+  {
+    constexpr double kSparseOccupancy = 8.0;
+    std::string force;
+    if (const char* e = std::getenv("BEADS_BUILD")) force = e;
+    any_sparse_ = any_dense_ = false;
+    for (uint32_t r = 0; r < n; ++r) {
+      const ReplicaHost& h = rep_[r];
+      const double occ = static_cast<double>(h.n_atoms) / std::max<uint32_t>(1, h.plan.n_cells);
+      bool sparse = occ < kSparseOccupancy;
+      if (force == "dense") sparse = false;
+      if (force == "sparse") sparse = true;
+      rp[r].sparse = sparse ? 1u : 0u;
+      any_sparse_ |= sparse;
+      any_dense_ |= !sparse;
+    }
+  }
   n_tags_ = tags;
   total_bond_types_ = static_cast<uint32_t>(bond_types);
   total_angle_types_ = static_cast<uint32_t>(angle_types);
@@ -530,6 +550,17 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   }
   term.reserve(term_off[T]);
   for (uint32_t t = 0; t < T; ++t) term.insert(term.end(), member[t].begin(), member[t].end());
+  // The membership entry of every (term, member), for k_bonded_terms.
+  const size_t nb_all = h_bonds.size(), na_all = h_angles.size(), nd_all = h_dihedrals.size();
+  std::vector<uint32_t> term_mem(2 * nb_all + 3 * na_all + 4 * nd_all, 0);
+  for (uint32_t e = 0; e < term.size(); ++e) {
+    const uint32_t m = term[e];
+    const uint32_t kind = m >> 30, role = (m >> 28) & 3u, idx = m & 0x0fffffffu;
+    const size_t at = kind == kTermBond    ? 2 * static_cast<size_t>(idx) + role
+                      : kind == kTermAngle ? 2 * nb_all + 3 * static_cast<size_t>(idx) + role
+                                           : 2 * nb_all + 3 * na_all + 4 * static_cast<size_t>(idx) + role;
+    term_mem[at] = e;
+  }
 
   // ---- LJ tables ----
   std::vector<LjCoeff> h_lj(lj_entries);
@@ -576,6 +607,24 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   v.ref_img = dalloc<int4>(S);
   v.cross = dalloc<uint32_t>(S);
   v.work_start = dalloc<uint32_t>(n + 1);
+  {
+    std::vector<uint32_t> chunk_replica, chunk_first(n + 1);
+    for (uint32_t r = 0; r < n; ++r) {
+      chunk_first[r] = static_cast<uint32_t>(chunk_replica.size());
+      const uint32_t chunks = std::max<uint32_t>(1, (rp[r].n_cells + kScanChunk - 1) / kScanChunk);
+      chunk_replica.insert(chunk_replica.end(), chunks, r);
+    }
+    chunk_first[n] = static_cast<uint32_t>(chunk_replica.size());
+    uint32_t* d_cr = dalloc<uint32_t>(chunk_replica.size());
+    uint32_t* d_cf = dalloc<uint32_t>(n + 1);
+    cuda_check(cudaMemcpy(d_cr, chunk_replica.data(), chunk_replica.size() * 4, cudaMemcpyHostToDevice),
+               "h2d");
+    cuda_check(cudaMemcpy(d_cf, chunk_first.data(), (n + 1) * 4ull, cudaMemcpyHostToDevice), "h2d");
+    v.scan_chunk_replica = d_cr;
+    v.scan_chunk_first = d_cf;
+    v.scan_chunk_sum = dalloc<uint32_t>(chunk_replica.size());
+    v.n_scan_chunks = static_cast<uint32_t>(chunk_replica.size());
+  }
   v.pos2 = dalloc<float4>(S);
   v.vel2 = dalloc<float4>(S);
   v.img2 = dalloc<int4>(S);
@@ -595,6 +644,9 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   uint32_t* d_excl_tag = dalloc<uint32_t>(excl_tag.size());
   uint32_t* d_term_off = dalloc<uint32_t>(T + 1);
   uint32_t* d_term = dalloc<uint32_t>(term.size());
+  uint32_t* d_term_mem = dalloc<uint32_t>(term_mem.size());
+  v.bonded_contrib = dalloc<float4>(term.size());
+  v.bonded_vir = dalloc<float>(term.size());
   uint4* d_bonds = dalloc<uint4>(h_bonds.size());
   uint4* d_angles = dalloc<uint4>(h_angles.size());
   uint4* d_dihedrals = dalloc<uint4>(h_dihedrals.size());
@@ -630,6 +682,7 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   up(d_excl_tag, excl_tag.data(), excl_tag.size() * sizeof(uint32_t));
   up(d_term_off, term_off.data(), term_off.size() * sizeof(uint32_t));
   up(d_term, term.data(), term.size() * sizeof(uint32_t));
+  up(d_term_mem, term_mem.data(), term_mem.size() * sizeof(uint32_t));
   up(d_bonds, h_bonds.data(), h_bonds.size() * sizeof(uint4));
   up(d_angles, h_angles.data(), h_angles.size() * sizeof(uint4));
   up(d_dihedrals, h_dihedrals.data(), h_dihedrals.size() * sizeof(uint4));
@@ -653,6 +706,10 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   v.angles = d_angles;
   v.dihedrals = d_dihedrals;
   v.dihedral_type = d_dih_type;
+  v.term_mem = d_term_mem;
+  v.n_bond_terms = static_cast<uint32_t>(nb_all);
+  v.n_angle_terms = static_cast<uint32_t>(na_all);
+  v.n_dihedral_terms = static_cast<uint32_t>(nd_all);
   v.bond_coeff = d_bc;
   v.angle_coeff = d_ac;
   v.dihedral_coeff = d_dc;
@@ -683,6 +740,8 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   launch_.max_atoms_per_replica = max_atoms;
   launch_.excl_cap = excl_cap;
   launch_.need_kinetic = any_thermostat ? 1 : 0;
+  launch_.any_dense = any_dense_ ? 1 : 0;
+  launch_.any_sparse = any_sparse_ ? 1 : 0;
   if (staged_) prepare_staged_kernels(static_cast<size_t>(stage_cap_ + 1) * sizeof(float4));
   // Initial slot-space exclusion rows (slot order = input order).
   launch_project_exclusions(launch_, true);

@@ -201,6 +201,7 @@ class Engine {
   uint32_t stage_cap_ = 0;             // stage entries per group (k_lj_staged)
   bool tuning_fixed_ = false;          // set_tuning() with an explicit choice
   bool layout_fixed_ = false;          // set_list_staged() called: the autotuner keeps the layout
+  bool any_sparse_ = false, any_dense_ = false;  // list build forms in use (k_build_sparse / k_build)
   bool tuned_ = false;                 // autotune() has run
   cudaStream_t side_stream_ = nullptr;
   std::map<std::pair<uint32_t, bool>, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs_;

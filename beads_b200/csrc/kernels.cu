@@ -196,16 +196,73 @@ __global__ void __launch_bounds__(kBlock) k_bin(DeviceView v) {
   atomicAdd(&v.cell_count[cell], 1u);
 }
 
-// rebuild 2: exclusive scan of the counts of one replica (one block per
-// replica); resets the counts for the next build.  Warp w owns a contiguous
-// range of cells: it sums the range (coalesced loads), the block scans the
-// 32 warp sums, then each warp rescans its range 32 cells at a time with
-// shuffles and writes the starts.
+// rebuild 2: exclusive scan of the cell counts (the cell starts), in three
+// kernels so that a replica with many cells is scanned by many blocks:
+// k_scan_sum (one block per chunk of kScanChunk cells: the chunk's total),
+// k_scan (one block per replica: the work list of the per-cell kernels and
+// the exclusive prefix of the replica's chunk totals) and k_scan_cells (one
+// block per chunk: the starts and cursors of its cells; the counts are reset
+// for the next build).
 constexpr int kScanThreads = 1024;
 constexpr int kScanWarps = kScanThreads / 32;
+constexpr uint32_t kScanPer = kScanChunk / kScanThreads;  // consecutive cells per thread
+
+// Exclusive prefix of x over the block (kScanThreads threads) and the total.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t& total) {
+  __shared__ uint32_t ws[kScanWarps + 1];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t inc = x;
+#pragma unroll
+  for (uint32_t o = 1; o < 32u; o <<= 1) {
+    const uint32_t up = __shfl_up_sync(kFull, inc, o);
+    if (lane >= o) inc += up;
+  }
+  if (lane == 31u) ws[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t t = ws[lane];
+    uint32_t wi = t;
+#pragma unroll
+    for (uint32_t o = 1; o < 32u; o <<= 1) {
+      const uint32_t up = __shfl_up_sync(kFull, wi, o);
+      if (lane >= o) wi += up;
+    }
+    ws[lane] = wi - t;                     // warps before this one
+    if (lane == 31u) ws[kScanWarps] = wi;  // the block total
+  }
+  __syncthreads();
+  const uint32_t out = ws[warp] + inc - x;
+  total = ws[kScanWarps];
+  __syncthreads();  // ws is reused by the next call
+  return out;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_sum(DeviceView v) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.scan_chunk_replica[b];
+  if (!v.rs[r].need_rebuild) return;
+  const ReplicaParams& p = v.rp[r];
+  const uint32_t c0 = (b - v.scan_chunk_first[r]) * kScanChunk;
+  const uint32_t* count = v.cell_count + p.cell_begin;
+  uint32_t s = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kScanPer; ++k) {
+    const uint32_t c = c0 + k * kScanThreads + threadIdx.x;
+    if (c < p.n_cells) s += count[c];
+  }
+  s = __reduce_add_sync(kFull, s);
+  __shared__ uint32_t part[kScanWarps];
+  if ((threadIdx.x & 31u) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < kScanWarps; ++w) t += part[w];
+    v.scan_chunk_sum[b] = t;
+  }
+}
+
 __global__ void __launch_bounds__(kScanThreads) k_scan(DeviceView v) {
   const uint32_t r = blockIdx.x;
-  __shared__ uint32_t warp_base[kScanWarps];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   {
     // Work list of the per-cell kernels (cell sort, list build): work item
@@ -237,50 +294,50 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(DeviceView v) {
       if (r == 0) v.work_start[v.n_replicas] = sa;
     }
   }
+  if (!v.rs[r].need_rebuild) return;  // block-uniform
+  const ReplicaParams& p = v.rp[r];
+  // Exclusive prefix of the replica's chunk totals, in place.
+  const uint32_t f0 = v.scan_chunk_first[r], f1 = v.scan_chunk_first[r + 1];
+  uint32_t run = 0;
+  for (uint32_t base = f0; base < f1; base += kScanThreads) {
+    const uint32_t at = base + threadIdx.x;
+    const uint32_t x = at < f1 ? v.scan_chunk_sum[at] : 0u;
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan(x, total);
+    if (at < f1) v.scan_chunk_sum[at] = run + ex;
+    run += total;
+  }
+  if (threadIdx.x == 0) v.cell_start[p.start_base + p.n_cells] = p.atom_begin + p.n_atoms;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_cells(DeviceView v) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.scan_chunk_replica[b];
   if (!v.rs[r].need_rebuild) return;
   const ReplicaParams& p = v.rp[r];
-  const uint32_t n = p.n_cells;
-  const uint32_t per = ((n + kScanWarps - 1) / kScanWarps + 31u) & ~31u;
-  const uint32_t begin = min(n, warp * per);
-  const uint32_t end = min(n, begin + per);
+  const uint32_t c0 = (b - v.scan_chunk_first[r]) * kScanChunk + threadIdx.x * kScanPer;
   uint32_t* count = v.cell_count + p.cell_begin;
-  uint32_t local = 0;
-#pragma unroll 8
-  for (uint32_t c = begin + lane; c < end; c += 32u) local += count[c];
-  const uint32_t total = __reduce_add_sync(kFull, local);
-  if (lane == 0) warp_base[warp] = total;
-  __syncthreads();
-  if (warp == 0) {
-    const uint32_t t = warp_base[lane];
-    uint32_t inc = t;
+  uint32_t cnt[kScanPer];
+  uint32_t s = 0;
 #pragma unroll
-    for (uint32_t o = 1; o < 32u; o <<= 1) {
-      const uint32_t up = __shfl_up_sync(kFull, inc, o);
-      if (lane >= o) inc += up;
-    }
-    warp_base[lane] = inc - t;
+  for (uint32_t k = 0; k < kScanPer; ++k) {
+    cnt[k] = c0 + k < p.n_cells ? count[c0 + k] : 0u;
+    s += cnt[k];
   }
-  __syncthreads();
-  uint32_t run = p.atom_begin + warp_base[warp];
+  uint32_t total;
+  uint32_t run = p.atom_begin + v.scan_chunk_sum[b] + block_exclusive_scan(s, total);
   uint32_t* start = v.cell_start + p.start_base;
   uint32_t* cursor = v.cell_cursor + p.cell_begin;
-  for (uint32_t c0 = begin; c0 < end; c0 += 32u) {
-    const uint32_t c = c0 + lane;
-    const uint32_t cnt = c < end ? count[c] : 0u;
-    uint32_t inc = cnt;
 #pragma unroll
-    for (uint32_t o = 1; o < 32u; o <<= 1) {
-      const uint32_t up = __shfl_up_sync(kFull, inc, o);
-      if (lane >= o) inc += up;
-    }
-    if (c < end) {
-      start[c] = run + inc - cnt;
-      cursor[c] = run + inc - cnt;
+  for (uint32_t k = 0; k < kScanPer; ++k) {
+    const uint32_t c = c0 + k;
+    if (c < p.n_cells) {
+      start[c] = run;
+      cursor[c] = run;
       count[c] = 0u;
     }
-    run += __shfl_sync(kFull, inc, 31);
+    run += cnt[k];
   }
-  if (threadIdx.x == 0) start[n] = p.atom_begin + p.n_atoms;
 }
 
 // rebuild 3: scatter slots into their cells (order inside a cell is fixed by
@@ -318,6 +375,7 @@ __device__ __forceinline__ uint32_t work_replica(const DeviceView& v, uint32_t w
 // list build reads its candidates with contiguous loads that do not wait on
 // the slot index; the reorder kernels find them there too.
 constexpr uint32_t kSortRankMax = 256;  // cells up to this size: rank sort in shared memory
+constexpr uint32_t kSortThreadMax = 8;  // sparse replicas: cells up to this size, one thread each
 // Sorts cell c of replica p (one warp; keys: this warp's shared scratch).
 __device__ __forceinline__ void sort_cell(const DeviceView& v, const ReplicaParams& p,
                                           uint32_t c, uint32_t lane, uint32_t* keys) {
@@ -325,6 +383,7 @@ __device__ __forceinline__ void sort_cell(const DeviceView& v, const ReplicaPara
     const uint32_t s0 = v.cell_start[p.start_base + c];
     const uint32_t s1 = v.cell_start[p.start_base + c + 1];
     const uint32_t n = s1 - s0;
+    if (p.sparse && n <= kSortThreadMax) return;  // sorted by k_cellsort_sparse
     if (n <= 32u) {
       uint32_t val = lane < n ? v.cell_atoms[s0 + lane] : 0xffffffffu;
       if (n > 1u) {
@@ -371,6 +430,42 @@ __device__ __forceinline__ void sort_cell(const DeviceView& v, const ReplicaPara
       }
       __syncwarp();
       for (uint32_t q = s0 + lane; q < s1; q += 32u) v.pos2[q] = v.pos[v.cell_atoms[q]];
+    }
+  }
+}
+
+// Cells of sparse replicas (k_build_sparse) with at most kSortThreadMax
+// members: one thread per work item sorts its cell's slots in registers
+// (insertion sort) and gathers their positions; k_cellsort sorts the rest.
+__global__ void __launch_bounds__(kBlock) k_cellsort_sparse(DeviceView v) {
+  const uint32_t w = blockIdx.x * kBlock + threadIdx.x;
+  if (w >= v.work_start[v.n_replicas]) return;
+  const uint32_t r = work_replica(v, w);
+  const ReplicaParams& p = v.rp[r];
+  if (!p.sparse) return;
+  const uint32_t c = w - v.work_start[r];
+  const uint32_t s0 = v.cell_start[p.start_base + c];
+  const uint32_t s1 = v.cell_start[p.start_base + c + 1];
+  const uint32_t n = s1 - s0;
+  if (n > kSortThreadMax) return;
+  uint32_t key[kSortThreadMax];
+#pragma unroll
+  for (uint32_t k = 0; k < kSortThreadMax; ++k) key[k] = k < n ? v.cell_atoms[s0 + k] : 0xffffffffu;
+  // Insertion sort of a fixed-size register array (compile-time indices).
+#pragma unroll
+  for (uint32_t a = 1; a < kSortThreadMax; ++a) {
+#pragma unroll
+    for (uint32_t b = a; b > 0; --b) {
+      const uint32_t lo = min(key[b - 1], key[b]), hi = max(key[b - 1], key[b]);
+      key[b - 1] = lo;
+      key[b] = hi;
+    }
+  }
+#pragma unroll
+  for (uint32_t k = 0; k < kSortThreadMax; ++k) {
+    if (k < n) {
+      v.cell_atoms[s0 + k] = key[k];
+      v.pos2[s0 + k] = v.pos[key[k]];
     }
   }
 }
@@ -695,6 +790,7 @@ template <int kCap>
 __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaParams& p,
                                            ReplicaState* st, uint32_t g, uint32_t lane,
                                            BuildShared& sh) {
+  if (p.sparse) return;  // built by k_build_sparse
   const uint32_t c = g - p.cell_begin;
   const uint32_t* start = v.cell_start + p.start_base;
   const uint32_t cs = start[c], ce = start[c + 1];
@@ -859,6 +955,138 @@ __global__ void __launch_bounds__(kBlock, 7) k_build(DeviceView v) {
   const uint32_t r = work_replica(v, w);
   const ReplicaParams& p = v.rp[r];
   build_cell<kCap>(v, p, &v.rs[r], p.cell_begin + (w - v.work_start[r]), lane, sh[warp]);
+}
+
+// The same lists, one thread per particle, for replicas whose cells hold a
+// few particles each (a bead-spring melt at WCA range: ~2.4 per cell), where
+// a warp per cell leaves most lanes idle and spends its time on the segment
+// table.  Thread q takes the particle at cell-order index q, walks the
+// stencil segments of its cell in build_cell's order (z, y rows; the x run
+// of a row, split in two where it wraps; ascending slot inside a cell) and
+// applies build_cell's float expressions, inclusion rule and entry encoding,
+// so the lists (order included) are the ones k_build writes.  A block is 128
+// consecutive cell-order rows: one stage group in a staged context.
+template <int kCap>
+__global__ void __launch_bounds__(kBlock) k_build_sparse(DeviceView v) {
+  __shared__ StageLayout lay;
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.block_replica[b];
+  const ReplicaParams& p = v.rp[r];
+  ReplicaState* st = &v.rs[r];
+  if (!p.sparse || !st->need_rebuild) return;  // block-uniform
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t nx = p.nc[0], ny = p.nc[1], nz = p.nc[2];
+  const bool regular = nx >= 4u && ny >= 4u && nz >= 4u;
+  const bool by_q = v.list_by_q != 0;
+  const bool staged_replica = by_q && p.staged != 0u && regular;
+  if (staged_replica) {
+    if (warp == 0) stage_layout(v, p, b, lane, v.stage_cap, lay);
+    __syncthreads();
+  }
+  const bool staged_group = staged_replica && lay.n_win != 0u;
+  const uint32_t q = b * kBlock + threadIdx.x;
+  if (q - p.atom_begin >= p.n_atoms) return;
+  const uint32_t i = v.cell_atoms[q];
+  const float4 xi = v.pos2[q];
+  const uint32_t c = v.cell_of_slot[i] - p.cell_begin;
+  const uint32_t cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+  const uint32_t* start = v.cell_start + p.start_base;
+  const int form = !regular ? kBuildMinImage
+                   : (cx == 0u || cy == 0u || cz == 0u || cx == nx - 1u || cy == ny - 1u ||
+                      cz == nz - 1u)
+                       ? kBuildShifted
+                       : kBuildInterior;
+  const float cut = p.search_cut_sq;
+  const uint32_t cap = p.max_neighbors;
+  uint32_t ex[kCap > 0 ? kCap : 1];
+  if (kCap > 0) {
+    const uint32_t* er = v.excl_slot + (size_t)i * v.excl_cap;
+#pragma unroll
+    for (int e = 0; e < kCap; ++e) ex[e] = er[e];
+  }
+  uint32_t* row = v.nbr + nbr_index(by_q ? q : i, 0, v.nbr_stride);
+  uint32_t cnt = 0u;
+  // One segment: cell-order run [q0, q1), periodic shift (sx, sy, sz) for the
+  // shifted form, entry offset `delta` (stage index = q + delta) in a staged
+  // group.
+  auto walk = [&](uint32_t q0, uint32_t q1, float sx, float sy, float sz, uint32_t delta) {
+    for (uint32_t qc = q0; qc < q1; ++qc) {
+      const uint32_t j = v.cell_atoms[qc];
+      const float4 x = v.pos2[qc];
+      float dx, dy, dz;
+      if (form == kBuildMinImage) {
+        dx = ref_delta(xi.x, x.x, p.len[0], p.half[0]);
+        dy = ref_delta(xi.y, x.y, p.len[1], p.half[1]);
+        dz = ref_delta(xi.z, x.z, p.len[2], p.half[2]);
+      } else {
+        dx = __fsub_rn(xi.x, x.x);
+        dy = __fsub_rn(xi.y, x.y);
+        dz = __fsub_rn(xi.z, x.z);
+        if (form == kBuildShifted) {
+          dx = __fadd_rn(dx, sx);
+          dy = __fadd_rn(dy, sy);
+          dz = __fadd_rn(dz, sz);
+        }
+      }
+      bool ok = !(norm2(dx, dy, dz) > cut) && j != i;
+      if (kCap > 0) {
+#pragma unroll
+        for (int e = 0; e < kCap; ++e) ok = ok && j != ex[e];
+      }
+      if (ok) {
+        if (cnt < cap) row[(size_t)cnt * kGroup] = staged_group ? qc + delta : j;
+        ++cnt;
+      }
+    }
+  };
+  if (regular) {
+    for (uint32_t a = 0; a < 3u; ++a) {
+      const uint32_t zc = stencil_cell(cz, nz, a);
+      const float shz = (cz == 0u && a == 0u) ? p.len[2] : (cz == nz - 1u && a == 2u) ? -p.len[2] : 0.0f;
+      for (uint32_t bb = 0; bb < 3u; ++bb) {
+        const uint32_t yc = stencil_cell(cy, ny, bb);
+        const float shy = (cy == 0u && bb == 0u) ? p.len[1] : (cy == ny - 1u && bb == 2u) ? -p.len[1] : 0.0f;
+        const uint32_t rowbase = nx * (yc + ny * zc);
+        const uint32_t k = 3u * a + bb;
+        for (uint32_t sg = 0; sg < 2u; ++sg) {
+          uint32_t lo = cx - 1u, hi = cx + 2u;
+          float shx = 0.0f;
+          bool used = sg == 0u;
+          if (cx == 0u) {
+            lo = sg == 0u ? nx - 1u : 0u, hi = sg == 0u ? nx : 2u, used = true;
+            shx = sg == 0u ? p.len[0] : 0.0f;
+          } else if (cx == nx - 1u) {
+            lo = sg == 0u ? nx - 2u : 0u, hi = sg == 0u ? nx : 1u, used = true;
+            shx = sg == 0u ? 0.0f : -p.len[0];
+          }
+          if (!used) continue;
+          uint32_t delta = 0u;
+          if (staged_group) {
+            const uint32_t w0 = 2u * (((cy + ny * cz) - lay.row_first) * 9u + k);
+            const uint32_t w = (lay.x0[w0] <= lo && lo < lay.x1[w0]) ? w0 : w0 + 1u;
+            delta = lay.base[w] - lay.qbeg[w];
+          }
+          walk(start[rowbase + lo], start[rowbase + hi], shx, shy, shz, delta);
+        }
+      }
+    }
+  } else {
+    const uint32_t sxn = min(nx, 3u), syn = min(ny, 3u), szn = min(nz, 3u);
+    for (uint32_t a = 0; a < szn; ++a) {
+      for (uint32_t bb = 0; bb < syn; ++bb) {
+        for (uint32_t k = 0; k < sxn; ++k) {
+          const uint32_t lc = stencil_cell(cx, nx, k) +
+                              nx * (stencil_cell(cy, ny, bb) + ny * stencil_cell(cz, nz, a));
+          walk(start[lc], start[lc + 1], 0.0f, 0.0f, 0.0f, 0u);
+        }
+      }
+    }
+  }
+  v.nbr_count[by_q ? q : i] = min(cnt, p.max_neighbors);
+  v.ref_pos[i] = xi;
+  v.ref_img[i] = v.img[i];
+  v.cross[i] = 0u;
+  if (cnt > p.max_neighbors) atomicOr(&st->status, kStatusNeighborOverflow);
 }
 
 // ---------------------------------------------------------------------------
@@ -1523,9 +1751,8 @@ __device__ __forceinline__ float bond_length(V3 d, float r0, float& stretch) {
 
 // Force on member `role` of a harmonic bond; energy and virial of the whole
 // term.  U = 0.5 k (r - r0)^2.
-__device__ V3 bond_term(const DeviceView& v, const ReplicaParams& p,
-                        uint32_t idx, uint32_t role, float& energy,
-                        float& virial) {
+__device__ void bond_forces(const DeviceView& v, const ReplicaParams& p, uint32_t idx,
+                            V3 (&f)[4], float& energy, float& virial) {
   const uint4 t = v.bonds[idx];
   const BondCoeff c = v.bond_coeff[t.z];
   const V3 d = arm(v, p, t.x, t.y);
@@ -1534,12 +1761,13 @@ __device__ V3 bond_term(const DeviceView& v, const ReplicaParams& p,
   energy = 0.5f * c.k * s * s;
   if (r == 0.0f) {
     virial = 0.f;
-    return v3(0.f, 0.f, 0.f);
+    f[0] = f[1] = v3(0.f, 0.f, 0.f);
+    return;
   }
   const float sc = -c.k * s / r;
   virial = -c.k * s * r;
-  const float sign = role == 0u ? 1.0f : -1.0f;
-  return scal(sc * sign, d);
+  f[0] = scal(sc, d);
+  f[1] = scal(-sc, d);
 }
 
 // U = 0.5 k (theta - theta0)^2 with the reference's conventions: sin(theta)
@@ -1551,9 +1779,8 @@ __device__ V3 bond_term(const DeviceView& v, const ReplicaParams& p,
 // and the force on i, a (cos a1 / r1^2 - a2 / (r1 r2)) with a = -k dtheta /
 // sin, is evaluated as a (a1 x n) / (r1^2 r1 r2) = -k dtheta (a1 x n) /
 // (r1^2 |n|) (likewise for k); the same quantities in exact arithmetic.
-__device__ V3 angle_term(const DeviceView& v, const ReplicaParams& p,
-                         uint32_t idx, uint32_t role, float& energy,
-                         float& virial) {
+__device__ void angle_forces(const DeviceView& v, const ReplicaParams& p, uint32_t idx,
+                             V3 (&f)[4], float& energy, float& virial) {
   const uint4 t = v.angles[idx];
   const AngleCoeff c = v.angle_coeff[t.w];
   const V3 a1 = arm(v, p, t.x, t.y);   // i - j
@@ -1563,7 +1790,8 @@ __device__ V3 angle_term(const DeviceView& v, const ReplicaParams& p,
   if (q1 == 0.0f || q2 == 0.0f) {
     energy = 0.5f * c.k * c.theta0 * c.theta0;
     virial = 0.f;
-    return v3(0.f, 0.f, 0.f);
+    f[0] = f[1] = f[2] = v3(0.f, 0.f, 0.f);
+    return;
   }
   const V3 n = cross3(a1, a2);
   const float qn = dot3(n, n);
@@ -1589,9 +1817,9 @@ __device__ V3 angle_term(const DeviceView& v, const ReplicaParams& p,
     fk = scal(g / q2, cross3(n, a2));
   }
   virial = dot3(a1, fi) + dot3(a2, fk);
-  if (role == 0u) return fi;
-  if (role == 2u) return fk;
-  return v3(-(fi.x + fk.x), -(fi.y + fk.y), -(fi.z + fk.z));
+  f[0] = fi;
+  f[1] = v3(-(fi.x + fk.x), -(fi.y + fk.y), -(fi.z + fk.z));
+  f[2] = fk;
 }
 
 // U = k (1 + d cos(n phi)), signed phi; singular geometry contributes energy
@@ -1599,9 +1827,8 @@ __device__ V3 angle_term(const DeviceView& v, const ReplicaParams& p,
 // (b0 x b1).(b1 x b2)): the reference's acos of the normalised cosine with
 // the sign of b0.(b1 x b2), in a form that keeps float accuracy near
 // phi = 0 and pi (cis and trans), where acos loses digits.
-__device__ V3 dihedral_term(const DeviceView& v, const ReplicaParams& p,
-                            uint32_t idx, uint32_t role, float& energy,
-                            float& virial) {
+__device__ void dihedral_forces(const DeviceView& v, const ReplicaParams& p, uint32_t idx,
+                                V3 (&f)[4], float& energy, float& virial) {
   const uint4 t = v.dihedrals[idx];
   const DihedralCoeff c = v.dihedral_coeff[v.dihedral_type[idx]];
   const V3 b0 = arm(v, p, t.x, t.y);   // i - j
@@ -1615,7 +1842,8 @@ __device__ V3 dihedral_term(const DeviceView& v, const ReplicaParams& p,
   if (q1 == 0.0f || qm == 0.0f || qn == 0.0f) {
     energy = c.n == 0 ? c.k * (1.0f + (float)c.d) : c.k;
     virial = 0.f;
-    return v3(0.f, 0.f, 0.f);
+    f[0] = f[1] = f[2] = f[3] = v3(0.f, 0.f, 0.f);
+    return;
   }
   const float l1 = sqrtf(q1);
   const float phi = atan2f(l1 * dot3(b0, n), dot3(m, n));
@@ -1634,14 +1862,52 @@ __device__ V3 dihedral_term(const DeviceView& v, const ReplicaParams& p,
   const V3 fk = v3(-(s.x + fl.x), -(s.y + fl.y), -(s.z + fl.z));
   const V3 lj = v3(b1.x - b2.x, b1.y - b2.y, b1.z - b2.z);
   virial = dot3(b0, fi) + dot3(b1, fk) + dot3(lj, fl);
-  switch (role) {
-    case 0u: return fi;
-    case 1u: return fj;
-    case 2u: return fk;
-    default: return fl;
+  f[0] = fi;
+  f[1] = fj;
+  f[2] = fk;
+  f[3] = fl;
+}
+
+// Bonded terms, one thread per term (bonds, then angles, then dihedrals in
+// one index space): the term is evaluated once and the force on each member
+// goes to that member's membership entry (term_mem), with the term's energy
+// in the first member's entry (.w) and, for observables, its virial
+// beside it.  k_bonded then sums each particle's entries in membership
+// order, so the sum order is fixed and no force atomics exist.
+template <bool kObs>
+__global__ void __launch_bounds__(kBlock) k_bonded_terms(DeviceView v) {
+  const uint32_t t = blockIdx.x * kBlock + threadIdx.x;
+  const uint32_t nb = v.n_bond_terms, na = v.n_angle_terms, nd = v.n_dihedral_terms;
+  if (t >= nb + na + nd) return;
+  uint32_t kind, idx, first_tag, nm, mem;
+  if (t < nb) {
+    kind = kTermBond, idx = t, first_tag = v.bonds[idx].x, nm = 2u, mem = 2u * idx;
+  } else if (t < nb + na) {
+    kind = kTermAngle, idx = t - nb, first_tag = v.angles[idx].x, nm = 3u;
+    mem = 2u * nb + 3u * idx;
+  } else {
+    kind = kTermDihedral, idx = t - nb - na, first_tag = v.dihedrals[idx].x, nm = 4u;
+    mem = 2u * nb + 3u * na + 4u * idx;
+  }
+  const ReplicaParams& p = v.rp[v.block_replica[v.slot_of_tag[first_tag] / (uint32_t)kBlock]];
+  V3 f[4];
+  float en = 0.f, vir = 0.f;
+  if (kind == kTermBond) {
+    bond_forces(v, p, idx, f, en, vir);
+  } else if (kind == kTermAngle) {
+    angle_forces(v, p, idx, f, en, vir);
+  } else {
+    dihedral_forces(v, p, idx, f, en, vir);
+  }
+  for (uint32_t m = 0; m < nm; ++m) {
+    const uint32_t e = v.term_mem[mem + m];
+    v.bonded_contrib[e] = make_float4(f[m].x, f[m].y, f[m].z, m == 0u ? en : 0.f);
+    if (kObs && m == 0u) v.bonded_vir[e] = vir;
   }
 }
 
+// Per particle: the bonded force from its membership entries (in membership
+// order) added to the pair force, then (post modes) the second half-kick.
 template <bool kObs, int kMode>
 __global__ void __launch_bounds__(kBlock) k_bonded(DeviceView v) {
   constexpr bool kPost = kMode >= kForcePost;
@@ -1660,31 +1926,25 @@ __global__ void __launch_bounds__(kBlock) k_bonded(DeviceView v) {
     if (e1 > e0) {
       V3 f = v3(0.f, 0.f, 0.f);
       for (uint32_t e = e0; e < e1; ++e) {
-        const uint32_t m = v.term[e];
-        const uint32_t kind = m >> 30;
-        const uint32_t role = (m >> 28) & 3u;
-        const uint32_t idx = m & 0x0fffffffu;
-        float en = 0.f, vir = 0.f;
-        V3 g;
-        if (kind == kTermBond) {
-          g = bond_term(v, p, idx, role, en, vir);
-          if (role == 0u) eb += en;
-        } else if (kind == kTermAngle) {
-          g = angle_term(v, p, idx, role, en, vir);
-          if (role == 0u) ea += en;
-        } else {
-          g = dihedral_term(v, p, idx, role, en, vir);
-          if (role == 0u) ed += en;
+        const float4 c = v.bonded_contrib[e];
+        f.x = __fadd_rn(f.x, c.x);
+        f.y = __fadd_rn(f.y, c.y);
+        f.z = __fadd_rn(f.z, c.z);
+        if (kObs) {
+          const uint32_t m = v.term[e];
+          if (((m >> 28) & 3u) == 0u) {
+            const uint32_t kind = m >> 30;
+            if (kind == kTermBond) eb += c.w;
+            else if (kind == kTermAngle) ea += c.w;
+            else ed += c.w;
+            w += v.bonded_vir[e];
+          }
         }
-        if (role == 0u) w += vir;
-        f.x += g.x;
-        f.y += g.y;
-        f.z += g.z;
       }
       fo = v.force[i];
-      fo.x += f.x;
-      fo.y += f.y;
-      fo.z += f.z;
+      fo.x = __fadd_rn(fo.x, f.x);
+      fo.y = __fadd_rn(fo.y, f.y);
+      fo.z = __fadd_rn(fo.z, f.z);
       v.force[i] = fo;
     } else if (kPost) {
       fo = v.force[i];
@@ -1850,10 +2110,18 @@ void launch_rebuild(const StepLaunch& l, bool force_all, bool count_build) {
   }
   k_bin<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
   check_launch("bin");
+  k_scan_sum<<<l.v.n_scan_chunks, kScanThreads, 0, l.stream>>>(l.v);
+  check_launch("scan sum");
   k_scan<<<l.v.n_replicas, kScanThreads, 0, l.stream>>>(l.v);
   check_launch("scan");
+  k_scan_cells<<<l.v.n_scan_chunks, kScanThreads, 0, l.stream>>>(l.v);
+  check_launch("scan cells");
   k_scatter<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
   check_launch("scatter");
+  if (l.any_sparse) {
+    k_cellsort_sparse<<<(l.v.total_cells + kBlock - 1) / kBlock, kBlock, 0, l.stream>>>(l.v);
+    check_launch("cellsort sparse");
+  }
   k_cellsort<<<(l.v.total_cells + kBlock / 32 - 1) / (kBlock / 32), kBlock, 0, l.stream>>>(l.v);
   check_launch("cellsort");
   k_reorder_gather<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
@@ -1865,7 +2133,11 @@ void launch_rebuild(const StepLaunch& l, bool force_all, bool count_build) {
     check_launch("project_exclusions");
   }
   const uint32_t bg = (l.v.total_cells + kBuildWarps - 1) / kBuildWarps;
-#define BB_BUILD(cap) k_build<cap><<<bg, kBlock, 0, l.stream>>>(l.v)
+#define BB_BUILD(cap)                                                              \
+  do {                                                                              \
+    if (l.any_dense) k_build<cap><<<bg, kBlock, 0, l.stream>>>(l.v);                \
+    if (l.any_sparse) k_build_sparse<cap><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); \
+  } while (0)
   switch (l.excl_cap) {
     case 0: BB_BUILD(0); break;
     case 4: BB_BUILD(4); break;
@@ -2051,6 +2323,16 @@ void launch_forces(const StepLaunch& l, bool observables, bool clamp, bool post,
   }
   if (parts & kForcePair) check_launch("lj");
   if (bonded) {
+    const uint32_t n_terms = l.v.n_bond_terms + l.v.n_angle_terms + l.v.n_dihedral_terms;
+    const uint32_t tg = (n_terms + kBlock - 1) / kBlock;
+    if (tg > 0) {
+      if (observables) {
+        k_bonded_terms<true><<<tg, kBlock, 0, l.stream>>>(l.v);
+      } else {
+        k_bonded_terms<false><<<tg, kBlock, 0, l.stream>>>(l.v);
+      }
+      check_launch("bonded terms");
+    }
 #define BB_BONDED(obs, mode) k_bonded<obs, mode><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v)
     if (observables) {
       if (fin == kForcePlain) BB_BONDED(true, kForcePlain);

@@ -23,6 +23,8 @@ struct StepLaunch {
   int lj_types;           // largest LJ table side over the batch (1, 2: specialised)
   int fuse_post;          // second half-kick inside the last force kernel
   int need_kinetic;       // a thermostat is active in some replica
+  int any_dense;          // some replica builds its lists a warp per cell (k_build)
+  int any_sparse;         // some replica builds them a thread per particle
   float sd_dmax;          // descent: displacement cap
   float sd_fref;          // descent: force floor
 };
