@@ -854,17 +854,20 @@ def run_chains(args) -> None:
 
 
 def _bonded_bytes_per_bead(spec) -> float:
-    """Algorithmic bytes per bead of the bonded kernel, each array element
-    counted once: the bead's tag, its two term offsets and force (read and
-    written), one 4-byte membership word per term it belongs to, the 16-byte
-    term records (and 4-byte dihedral types) once each, the tag-to-slot map
-    and the positions the terms read."""
+    """Algorithmic bytes per bead of the bonded stage (k_bonded_terms, then
+    k_bonded), each array element counted once.  Terms: the 16-byte records
+    (and 4-byte dihedral types), one 4-byte membership index per member, the
+    tag-to-slot map and positions of the beads, one 16-byte contribution
+    written per membership.  Gather: the bead's tag and two term offsets,
+    the contributions read back, the force read and written."""
     n = spec.n
     nb = 0 if spec.bonds is None else len(spec.bonds)
     na = 0 if spec.angles is None else len(spec.angles)
     nd = 0 if spec.dihedrals is None else len(spec.dihedrals)
     memberships = 2 * nb + 3 * na + 4 * nd
-    return (4 + 8 + 32 + 4 + 16) + (4.0 * memberships + 16.0 * (nb + na + nd) + 4.0 * nd) / n
+    per_term = 16.0 * (nb + na + nd) + 4.0 * nd + 4.0 * memberships + 16.0 * memberships
+    per_gather = 16.0 * memberships
+    return (4 + 16) + (4 + 8 + 32) + (per_term + per_gather) / n
 
 
 def adjoint_metric(world: int) -> str:
