@@ -170,24 +170,30 @@ void Engine::autotune() {
       chosen = l;
     }
   };
-  // The pair-force shape first (second half-kick as its own kernel), then
-  // the best shape with the kick fused.  The staged kernel has no L1 policy
-  // choice (its neighbour positions are in shared memory).
+  // One coordinate at a time, each from the best so far: threads per
+  // particle {1, 2, 4} at batch depth 4 with list loads bypassing L1, then
+  // depth 8, then list loads through L1 (the staged kernel reads its
+  // neighbour positions from shared memory and has no L1 choice), then the
+  // second half-kick fused into the force kernel: six trials per layout
+  // instead of the full grid of thirteen, which a short run pays for.
   auto tune_layout = [&]() {
     best = 0.f;
     const bool staged_now = v_.list_by_q != 0;
     for (int tpa : {1, 2, 4}) {
-      for (int unroll : {8, 4}) {
-        for (int no_l1 : {0, 1}) {
-          if (staged_now && no_l1 == 0) continue;
-          StepLaunch l = launch_;
-          l.lj_tpa = tpa;
-          l.lj_unroll = unroll;
-          l.lj_no_l1 = no_l1;
-          l.fuse_post = 0;
-          trial(l);
-        }
-      }
+      StepLaunch l = launch_;
+      l.lj_tpa = tpa;
+      l.lj_unroll = 4;
+      l.lj_no_l1 = 1;
+      l.fuse_post = 0;
+      trial(l);
+    }
+    StepLaunch deeper = chosen;
+    deeper.lj_unroll = 8;
+    trial(deeper);
+    if (!staged_now) {
+      StepLaunch l1 = chosen;
+      l1.lj_no_l1 = 0;
+      trial(l1);
     }
     StepLaunch fused = chosen;
     fused.fuse_post = 1;
@@ -1248,42 +1254,31 @@ void Engine::set_list_staged(bool staged) {
 // bit as they would have without the change.
 void Engine::relayout_list() {
   const size_t S = v_.n_slots;
-  float4* save_pos = nullptr;
-  int4* save_img = nullptr;
-  uint32_t* save_cross = nullptr;
-  cuda_check(cudaMalloc(&save_pos, S * sizeof(float4)), "cudaMalloc");
-  cudaError_t e1 = cudaMalloc(&save_img, S * sizeof(int4));
-  cudaError_t e2 = cudaMalloc(&save_cross, S * sizeof(uint32_t));
-  try {
-    cuda_check(e1, "cudaMalloc");
-    cuda_check(e2, "cudaMalloc");
-    auto d2d = [&](void* dst, const void* src, size_t bytes) {
-      cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream_), "copy");
-    };
-    d2d(save_pos, v_.pos, S * sizeof(float4));
-    d2d(save_img, v_.ref_img, S * sizeof(int4));
-    d2d(save_cross, v_.cross, S * sizeof(uint32_t));
-    d2d(v_.pos, v_.ref_pos, S * sizeof(float4));
-    std::vector<ReplicaState> saved(rep_.size());
-    sync();
-    cuda_check(cudaMemcpy(saved.data(), v_.rs, saved.size() * sizeof(ReplicaState),
-                          cudaMemcpyDeviceToHost), "state save");
-    launch_rebuild(launch_, true, false);
-    d2d(v_.pos, save_pos, S * sizeof(float4));
-    d2d(v_.ref_img, save_img, S * sizeof(int4));
-    d2d(v_.cross, save_cross, S * sizeof(uint32_t));
-    cuda_check(cudaMemcpyAsync(v_.rs, saved.data(), saved.size() * sizeof(ReplicaState),
-                               cudaMemcpyHostToDevice, stream_), "state restore");
-    sync();
-  } catch (...) {
-    cudaFree(save_pos);
-    if (save_img) cudaFree(save_img);
-    if (save_cross) cudaFree(save_cross);
-    throw;
+  // Save buffers kept for the context's life (allocated at the first call):
+  // a layout change, the autotuner's included, then costs no allocation.
+  if (!relayout_pos_) {
+    relayout_pos_ = dalloc<float4>(S);
+    relayout_img_ = dalloc<int4>(S);
+    relayout_cross_ = dalloc<uint32_t>(S);
   }
-  cudaFree(save_pos);
-  cudaFree(save_img);
-  cudaFree(save_cross);
+  auto d2d = [&](void* dst, const void* src, size_t bytes) {
+    cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, stream_), "copy");
+  };
+  d2d(relayout_pos_, v_.pos, S * sizeof(float4));
+  d2d(relayout_img_, v_.ref_img, S * sizeof(int4));
+  d2d(relayout_cross_, v_.cross, S * sizeof(uint32_t));
+  d2d(v_.pos, v_.ref_pos, S * sizeof(float4));
+  std::vector<ReplicaState> saved(rep_.size());
+  sync();
+  cuda_check(cudaMemcpy(saved.data(), v_.rs, saved.size() * sizeof(ReplicaState),
+                        cudaMemcpyDeviceToHost), "state save");
+  launch_rebuild(launch_, true, false);
+  d2d(v_.pos, relayout_pos_, S * sizeof(float4));
+  d2d(v_.ref_img, relayout_img_, S * sizeof(int4));
+  d2d(v_.cross, relayout_cross_, S * sizeof(uint32_t));
+  cuda_check(cudaMemcpyAsync(v_.rs, saved.data(), saved.size() * sizeof(ReplicaState),
+                             cudaMemcpyHostToDevice, stream_), "state restore");
+  sync();
 }
 
 void Engine::debug_neighbors(uint32_t r, uint32_t cap, uint32_t* counts, uint32_t* partners) {

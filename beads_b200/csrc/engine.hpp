@@ -202,6 +202,9 @@ class Engine {
   bool tuning_fixed_ = false;          // set_tuning() with an explicit choice
   bool layout_fixed_ = false;          // set_list_staged() called: the autotuner keeps the layout
   bool any_sparse_ = false, any_dense_ = false;  // list build forms in use (k_build_sparse / k_build)
+  float4* relayout_pos_ = nullptr;     // relayout_list save buffers (allocated at first use)
+  int4* relayout_img_ = nullptr;
+  uint32_t* relayout_cross_ = nullptr;
   bool tuned_ = false;                 // autotune() has run
   cudaStream_t side_stream_ = nullptr;
   std::map<std::pair<uint32_t, bool>, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs_;
