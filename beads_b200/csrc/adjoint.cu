@@ -49,7 +49,8 @@ T* AdjointStore::alloc(size_t count) {
   void* p = nullptr;
   cuda_check(cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(T)), "cudaMalloc (adjoint)");
   allocations.push_back(p);
-  cuda_check(cudaMemset(p, 0, std::max<size_t>(1, count) * sizeof(T)), "cudaMemset (adjoint)");
+  cuda_check(cudaMemsetAsync(p, 0, std::max<size_t>(1, count) * sizeof(T), stream),
+             "cudaMemset (adjoint)");
   return static_cast<T*>(p);
 }
 
@@ -626,9 +627,8 @@ void Engine::set_lj(uint32_t replica, const double* eps, const double* sigma) {
     }
   }
   sync();
-  cuda_check(cudaMemcpy(const_cast<LjCoeff*>(v_.lj) + h.lj_offset, table.data(),
-                        table.size() * sizeof(LjCoeff), cudaMemcpyHostToDevice),
-             "LJ table upload");
+  h2d(const_cast<LjCoeff*>(v_.lj) + h.lj_offset, table.data(), table.size() * sizeof(LjCoeff),
+      "LJ table upload");
   initialized_ = false;  // forces of the current state are stale
 }
 
@@ -756,6 +756,7 @@ void Engine::adjoint_forward(uint64_t steps, uint64_t record_from, uint32_t ever
 
   if (!adj_) adj_ = std::make_unique<AdjointStore>();
   AdjointStore& A = *adj_;
+  A.stream = stream_;
   const uint32_t R = n_replicas();
   const size_t S = v_.n_slots;
   // every == 0: keep every step's state from this forward pass (one segment,
@@ -799,9 +800,7 @@ void Engine::adjoint_forward(uint64_t steps, uint64_t record_from, uint32_t ever
     d2d(A.ck_ref_pos + c * S, v_.ref_pos, S * sizeof(float4));
     d2d(A.ck_ref_img + c * S, v_.ref_img, S * sizeof(int4));
     sync();
-    cuda_check(cudaMemcpy(A.ck_state.data() + static_cast<size_t>(c) * R, v_.rs,
-                          R * sizeof(ReplicaState), cudaMemcpyDeviceToHost),
-               "checkpoint");
+    d2h(A.ck_state.data() + static_cast<size_t>(c) * R, v_.rs, R * sizeof(ReplicaState), "checkpoint");
   };
   std::vector<beads_observables> o;
   auto put_obs = [&](uint64_t n) {
@@ -903,24 +902,26 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
     std::vector<double> g((T + 1) * R * 3, 0.0);
     std::copy(obs_grad, obs_grad + (T + 1 - A.record_from) * R * 3,
               g.begin() + A.record_from * R * 3);
-    cuda_check(cudaMemcpy(A.obs_grad, g.data(), g.size() * sizeof(double),
-                          cudaMemcpyHostToDevice), "adjoint upload");
+    h2d(A.obs_grad, g.data(), g.size() * sizeof(double), "adjoint upload");
     std::vector<int> sh(R);
     for (uint32_t r = 0; r < R; ++r) sh[r] = rep_[r].lj_shift ? 1 : 0;
-    cuda_check(cudaMemcpy(d_shift, sh.data(), R * sizeof(int), cudaMemcpyHostToDevice),
-               "adjoint upload");
+    h2d(d_shift, sh.data(), R * sizeof(int), "adjoint upload");
   }
   sync();
-  cuda_check(cudaMemset(A.xbar, 0, S * sizeof(float4)), "memset");
-  cuda_check(cudaMemset(A.ubar, 0, S * sizeof(float4)), "memset");
-  cuda_check(cudaMemset(A.vbar, 0, S * sizeof(float4)), "memset");
-  cuda_check(cudaMemset(A.theta, 0, static_cast<size_t>(R) * kAdjTypes * kAdjTypes * 4 * 8),
+  cuda_check(cudaMemsetAsync(A.xbar, 0, S * sizeof(float4), stream_), "memset");
+  cuda_check(cudaMemsetAsync(A.ubar, 0, S * sizeof(float4), stream_), "memset");
+  cuda_check(cudaMemsetAsync(A.vbar, 0, S * sizeof(float4), stream_), "memset");
+  cuda_check(cudaMemsetAsync(A.theta, 0, static_cast<size_t>(R) * kAdjTypes * kAdjTypes * 4 * 8,
+             stream_),
              "memset");
-  cuda_check(cudaMemset(A.dot, 0, static_cast<size_t>(R) * 4 * sizeof(long long)), "memset");
-  cuda_check(cudaMemset(A.theta_bond, 0, std::max<size_t>(1, total_bond_types_) * 4 * 8), "memset");
-  cuda_check(cudaMemset(A.theta_angle, 0, std::max<size_t>(1, total_angle_types_) * 4 * 8),
+  cuda_check(cudaMemsetAsync(A.dot, 0, static_cast<size_t>(R) * 4 * sizeof(long long), stream_),
              "memset");
-  cuda_check(cudaMemset(A.theta_dihedral, 0, std::max<size_t>(1, total_dihedral_types_) * 2 * 8),
+  cuda_check(cudaMemsetAsync(A.theta_bond, 0, std::max<size_t>(1, total_bond_types_) * 4 * 8,
+             stream_), "memset");
+  cuda_check(cudaMemsetAsync(A.theta_angle, 0, std::max<size_t>(1, total_angle_types_) * 4 * 8, stream_),
+             "memset");
+  cuda_check(cudaMemsetAsync(A.theta_dihedral, 0, std::max<size_t>(1,
+             total_dihedral_types_) * 2 * 8, stream_),
              "memset");
 
   AdjView av{};
@@ -973,8 +974,7 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
     }
     sync();
     flags.resize(static_cast<size_t>(b - a + 1) * R);
-    cuda_check(cudaMemcpy(flags.data(), A.seg_flags, flags.size() * sizeof(uint32_t),
-                          cudaMemcpyDeviceToHost), "flags");
+    d2h(flags.data(), A.seg_flags, flags.size() * sizeof(uint32_t), "flags");
     // The list each forward step m used: built at the replica's last rebuild
     // at or before m inside this segment, else the checkpoint's.  Walking
     // backwards, a replica's list is rebuilt when that source changes; the
@@ -1003,10 +1003,8 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
         }
       }
     }
-    cuda_check(cudaMemcpy(A.seg_src, src_all.data(), nk * R * sizeof(int), cudaMemcpyHostToDevice),
-               "adjoint list sources");
-    cuda_check(cudaMemcpy(A.seg_changed, chg_all.data(), nk * R * sizeof(uint32_t),
-                          cudaMemcpyHostToDevice), "adjoint list sources");
+    h2d(A.seg_src, src_all.data(), nk * R * sizeof(int), "adjoint list sources");
+    h2d(A.seg_changed, chg_all.data(), nk * R * sizeof(uint32_t), "adjoint list sources");
     for (uint64_t m = b + 1; m-- > m_lo;) {
       const uint32_t k = static_cast<uint32_t>(m - a);
       AdjView lv = av;
@@ -1061,8 +1059,7 @@ void Engine::adjoint_backward(const double* obs_grad, double* grad_eps, double* 
                              cudaMemcpyDeviceToHost, stream_), "adjoint download");
   std::vector<long long> th(static_cast<size_t>(R) * kAdjTypes * kAdjTypes * 4);
   sync();
-  cuda_check(cudaMemcpy(th.data(), A.theta, th.size() * sizeof(long long), cudaMemcpyDeviceToHost),
-             "adjoint download");
+  d2h(th.data(), A.theta, th.size() * sizeof(long long), "adjoint download");
   size_t out = 0;
   for (uint32_t r = 0; r < R; ++r) {
     const int nt = rep_[r].n_types;
@@ -1089,8 +1086,7 @@ void Engine::adjoint_bonded_grads(double* grad_bond, double* grad_angle, double*
   sync();
   auto read = [&](const long long* src, size_t n_pairs, std::vector<double>& out) {
     std::vector<long long> raw(2 * std::max<size_t>(1, n_pairs));
-    cuda_check(cudaMemcpy(raw.data(), src, raw.size() * sizeof(long long), cudaMemcpyDeviceToHost),
-               "adjoint download");
+    d2h(raw.data(), src, raw.size() * sizeof(long long), "adjoint download");
     out.resize(n_pairs);
     for (size_t q = 0; q < n_pairs; ++q) {
       out[q] = static_cast<double>(raw[2 * q]) + static_cast<double>(raw[2 * q + 1]) / kFixFrac;
@@ -1118,36 +1114,32 @@ void Engine::set_bonded(uint32_t replica, const double* bond_k, const double* bo
   sync();
   if (h.n_bond_types > 0 && (bond_k || bond_r0)) {
     std::vector<BondCoeff> c(h.n_bond_types);
-    cuda_check(cudaMemcpy(c.data(), v_.bond_coeff + h.bond_type_base,
-                          c.size() * sizeof(BondCoeff), cudaMemcpyDeviceToHost), "bonded");
+    d2h(c.data(), v_.bond_coeff + h.bond_type_base, c.size() * sizeof(BondCoeff), "bonded");
     for (int t = 0; t < h.n_bond_types; ++t) {
       if (bond_k) c[t].k = static_cast<float>(bond_k[t]);
       if (bond_r0) c[t].r0 = static_cast<float>(bond_r0[t]);
     }
-    cuda_check(cudaMemcpy(const_cast<BondCoeff*>(v_.bond_coeff) + h.bond_type_base, c.data(),
-                          c.size() * sizeof(BondCoeff), cudaMemcpyHostToDevice), "bonded");
+    h2d(const_cast<BondCoeff*>(v_.bond_coeff) + h.bond_type_base, c.data(),
+        c.size() * sizeof(BondCoeff), "bonded");
   }
   if (h.n_angle_types > 0 && (angle_k || angle_theta0_deg)) {
     std::vector<AngleCoeff> c(h.n_angle_types);
-    cuda_check(cudaMemcpy(c.data(), v_.angle_coeff + h.angle_type_base,
-                          c.size() * sizeof(AngleCoeff), cudaMemcpyDeviceToHost), "bonded");
+    d2h(c.data(), v_.angle_coeff + h.angle_type_base, c.size() * sizeof(AngleCoeff), "bonded");
     for (int t = 0; t < h.n_angle_types; ++t) {
       if (angle_k) c[t].k = static_cast<float>(angle_k[t]);
       if (angle_theta0_deg) {
         c[t].theta0 = static_cast<float>(angle_theta0_deg[t]) * 3.14159265358979323846f / 180.0f;
       }
     }
-    cuda_check(cudaMemcpy(const_cast<AngleCoeff*>(v_.angle_coeff) + h.angle_type_base, c.data(),
-                          c.size() * sizeof(AngleCoeff), cudaMemcpyHostToDevice), "bonded");
+    h2d(const_cast<AngleCoeff*>(v_.angle_coeff) + h.angle_type_base, c.data(),
+        c.size() * sizeof(AngleCoeff), "bonded");
   }
   if (h.n_dihedral_types > 0 && dihedral_k) {
     std::vector<DihedralCoeff> c(h.n_dihedral_types);
-    cuda_check(cudaMemcpy(c.data(), v_.dihedral_coeff + h.dihedral_type_base,
-                          c.size() * sizeof(DihedralCoeff), cudaMemcpyDeviceToHost), "bonded");
+    d2h(c.data(), v_.dihedral_coeff + h.dihedral_type_base, c.size() * sizeof(DihedralCoeff), "bonded");
     for (int t = 0; t < h.n_dihedral_types; ++t) c[t].k = static_cast<float>(dihedral_k[t]);
-    cuda_check(cudaMemcpy(const_cast<DihedralCoeff*>(v_.dihedral_coeff) + h.dihedral_type_base,
-                          c.data(), c.size() * sizeof(DihedralCoeff), cudaMemcpyHostToDevice),
-               "bonded");
+    h2d(const_cast<DihedralCoeff*>(v_.dihedral_coeff) + h.dihedral_type_base, c.data(),
+        c.size() * sizeof(DihedralCoeff), "bonded");
   }
   initialized_ = false;
 }

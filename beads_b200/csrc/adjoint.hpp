@@ -29,6 +29,7 @@ struct AdjointStore {
   int max_types = 0;          // LJ table side of the largest replica table
   bool forward_done = false;
   bool store_all = false;     // every step kept by the forward pass (no replay)
+  cudaStream_t stream = nullptr;  // the engine stream: zero fills are ordered on it
 
   // checkpoints: segment starts 0..segments-1, then the final state
   float4* ck_pos = nullptr;

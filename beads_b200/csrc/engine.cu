@@ -82,8 +82,7 @@ void Engine::set_sort_enabled(bool on) {
   for (uint32_t r = 0; r < rep_.size(); ++r) {
     const uint32_t value = on ? rep_[r].sort_every : 0u;
     ReplicaParams* dst = const_cast<ReplicaParams*>(v_.rp) + r;
-    cuda_check(cudaMemcpy(&dst->sort_every, &value, sizeof(value), cudaMemcpyHostToDevice),
-               "sort cadence");
+    h2d(&dst->sort_every, &value, sizeof(value), "sort cadence");
   }
 }
 
@@ -144,8 +143,7 @@ void Engine::autotune() {
   }();
   std::vector<ReplicaState> saved(rep_.size());
   sync();
-  cuda_check(cudaMemcpy(saved.data(), v_.rs, saved.size() * sizeof(ReplicaState),
-                        cudaMemcpyDeviceToHost), "state save");
+  d2h(saved.data(), v_.rs, saved.size() * sizeof(ReplicaState), "state save");
   cuda_check(cudaMemcpyAsync(v_.vel2, v_.vel, v_.n_slots * sizeof(float4),
                              cudaMemcpyDeviceToDevice, stream_), "velocity save");
   cudaEvent_t a = nullptr, b = nullptr;
@@ -623,9 +621,8 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
     chunk_first[n] = static_cast<uint32_t>(chunk_replica.size());
     uint32_t* d_cr = dalloc<uint32_t>(chunk_replica.size());
     uint32_t* d_cf = dalloc<uint32_t>(n + 1);
-    cuda_check(cudaMemcpy(d_cr, chunk_replica.data(), chunk_replica.size() * 4, cudaMemcpyHostToDevice),
-               "h2d");
-    cuda_check(cudaMemcpy(d_cf, chunk_first.data(), (n + 1) * 4ull, cudaMemcpyHostToDevice), "h2d");
+    h2d(d_cr, chunk_replica.data(), chunk_replica.size() * 4, "h2d");
+    h2d(d_cf, chunk_first.data(), (n + 1) * 4ull, "h2d");
     v.scan_chunk_replica = d_cr;
     v.scan_chunk_first = d_cf;
     v.scan_chunk_sum = dalloc<uint32_t>(chunk_replica.size());
@@ -757,11 +754,19 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
 
 void Engine::sync() { cuda_check(cudaStreamSynchronize(stream_), "stream synchronize"); }
 
+void Engine::h2d(void* dst, const void* src, size_t bytes, const char* what) {
+  cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_), what);
+  sync();
+}
+
+void Engine::d2h(void* dst, const void* src, size_t bytes, const char* what) {
+  cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream_), what);
+  sync();
+}
+
 void Engine::check_status() {
   sync();
-  cuda_check(cudaMemcpy(h_state_, v_.rs, rep_.size() * sizeof(ReplicaState),
-                        cudaMemcpyDeviceToHost),
-             "status download");
+  d2h(h_state_, v_.rs, rep_.size() * sizeof(ReplicaState), "status download");
   for (uint32_t r = 0; r < rep_.size(); ++r) {
     const unsigned s = h_state_[r].status;
     if (s & kStatusNeighborOverflow) {
@@ -991,9 +996,7 @@ void Engine::minimize(uint32_t iterations, float dmax, float fref) {
     h_state_[r].step = 0;
     h_state_[r].lambda = 1.0;
   }
-  cuda_check(cudaMemcpy(v_.rs, h_state_, rep_.size() * sizeof(ReplicaState),
-                        cudaMemcpyHostToDevice),
-             "state reset");
+  h2d(v_.rs, h_state_, rep_.size() * sizeof(ReplicaState), "state reset");
   initialized_ = false;
   step_ = 0;
 }
@@ -1013,8 +1016,7 @@ double Engine::profile(int stage, uint32_t reps) {
     // keep copies and put them back after timing.
     saved.resize(rep_.size());
     sync();
-    cuda_check(cudaMemcpy(saved.data(), v_.rs, saved.size() * sizeof(ReplicaState),
-                          cudaMemcpyDeviceToHost), "state save");
+    d2h(saved.data(), v_.rs, saved.size() * sizeof(ReplicaState), "state save");
     cuda_check(cudaMemcpyAsync(v_.vel2, v_.vel, v_.n_slots * sizeof(float4),
                                cudaMemcpyDeviceToDevice, stream_), "velocity save");
   }
@@ -1066,19 +1068,17 @@ double Engine::profile(int stage, uint32_t reps) {
 void Engine::counters(uint32_t replica, uint64_t out[4]) {
   sync();
   ReplicaState st;
-  cuda_check(cudaMemcpy(&st, v_.rs + replica, sizeof(ReplicaState), cudaMemcpyDeviceToHost),
-             "counters download");
+  d2h(&st, v_.rs + replica, sizeof(ReplicaState), "counters download");
   out[0] = st.step;
   out[1] = st.builds;
   out[2] = st.dangerous;
-  cuda_check(cudaMemcpy(&out[3], v_.chain_launches, sizeof(unsigned long long),
-                        cudaMemcpyDeviceToHost), "counters download");
+  d2h(&out[3], v_.chain_launches, sizeof(unsigned long long), "counters download");
 }
 
 void Engine::list_stats(uint64_t* total, uint32_t* max_count) {
   sync();
   std::vector<uint32_t> cnt(v_.n_slots);
-  cuda_check(cudaMemcpy(cnt.data(), v_.nbr_count, cnt.size() * 4ull, cudaMemcpyDeviceToHost), "d2h");
+  d2h(cnt.data(), v_.nbr_count, cnt.size() * 4ull, "d2h");
   uint64_t t = 0;
   uint32_t m = 0;
   for (uint32_t c : cnt) {
@@ -1091,8 +1091,7 @@ void Engine::list_stats(uint64_t* total, uint32_t* max_count) {
 
 void Engine::observables(std::vector<beads_observables>& out) {
   sync();
-  cuda_check(cudaMemcpy(h_obs_, v_.obs, rep_.size() * sizeof(ReplicaObs), cudaMemcpyDeviceToHost),
-             "observables download");
+  d2h(h_obs_, v_.obs, rep_.size() * sizeof(ReplicaObs), "observables download");
   out.resize(rep_.size());
   for (uint32_t r = 0; r < rep_.size(); ++r) {
     const ReplicaObs& o = h_obs_[r];
@@ -1131,12 +1130,12 @@ void Engine::slot_view(uint32_t r, SlotView& out) {
   out.tag.resize(n);
   out.mol.resize(n);
   const size_t b = h.atom_begin;
-  cuda_check(cudaMemcpy(out.pos.data(), v_.pos + b, n * sizeof(float4), cudaMemcpyDeviceToHost), "d2h");
-  cuda_check(cudaMemcpy(out.vel.data(), v_.vel + b, n * sizeof(float4), cudaMemcpyDeviceToHost), "d2h");
-  cuda_check(cudaMemcpy(out.force.data(), v_.force + b, n * sizeof(float4), cudaMemcpyDeviceToHost), "d2h");
-  cuda_check(cudaMemcpy(out.img.data(), v_.img + b, n * sizeof(int4), cudaMemcpyDeviceToHost), "d2h");
-  cuda_check(cudaMemcpy(out.tag.data(), v_.tag + b, n * sizeof(uint32_t), cudaMemcpyDeviceToHost), "d2h");
-  cuda_check(cudaMemcpy(out.mol.data(), v_.mol + b, n * sizeof(uint32_t), cudaMemcpyDeviceToHost), "d2h");
+  d2h(out.pos.data(), v_.pos + b, n * sizeof(float4), "d2h");
+  d2h(out.vel.data(), v_.vel + b, n * sizeof(float4), "d2h");
+  d2h(out.force.data(), v_.force + b, n * sizeof(float4), "d2h");
+  d2h(out.img.data(), v_.img + b, n * sizeof(int4), "d2h");
+  d2h(out.tag.data(), v_.tag + b, n * sizeof(uint32_t), "d2h");
+  d2h(out.mol.data(), v_.mol + b, n * sizeof(uint32_t), "d2h");
   for (auto& t : out.tag) t = t - h.tag_base + 1;  // 1-based local tags
 }
 
@@ -1227,10 +1226,10 @@ void Engine::debug_cells(uint32_t r, uint32_t* cell_by_tag) {
   const ReplicaHost& h = rep_.at(r);
   sync();
   std::vector<uint32_t> cell(h.n_atoms), tag(h.n_atoms);
-  cuda_check(cudaMemcpy(cell.data(), v_.cell_of_slot + h.atom_begin, h.n_atoms * 4, cudaMemcpyDeviceToHost), "d2h");
-  cuda_check(cudaMemcpy(tag.data(), v_.tag + h.atom_begin, h.n_atoms * 4, cudaMemcpyDeviceToHost), "d2h");
+  d2h(cell.data(), v_.cell_of_slot + h.atom_begin, h.n_atoms * 4, "d2h");
+  d2h(tag.data(), v_.tag + h.atom_begin, h.n_atoms * 4, "d2h");
   std::vector<ReplicaParams> rp(1);
-  cuda_check(cudaMemcpy(rp.data(), v_.rp + r, sizeof(ReplicaParams), cudaMemcpyDeviceToHost), "d2h");
+  d2h(rp.data(), v_.rp + r, sizeof(ReplicaParams), "d2h");
   for (uint32_t k = 0; k < h.n_atoms; ++k) {
     cell_by_tag[tag[k] - h.tag_base] = cell[k] - rp[0].cell_begin;
   }
@@ -1270,8 +1269,7 @@ void Engine::relayout_list() {
   d2d(v_.pos, v_.ref_pos, S * sizeof(float4));
   std::vector<ReplicaState> saved(rep_.size());
   sync();
-  cuda_check(cudaMemcpy(saved.data(), v_.rs, saved.size() * sizeof(ReplicaState),
-                        cudaMemcpyDeviceToHost), "state save");
+  d2h(saved.data(), v_.rs, saved.size() * sizeof(ReplicaState), "state save");
   launch_rebuild(launch_, true, false);
   d2d(v_.pos, relayout_pos_, S * sizeof(float4));
   d2d(v_.ref_img, relayout_img_, S * sizeof(int4));
@@ -1290,13 +1288,13 @@ void Engine::debug_neighbors(uint32_t r, uint32_t cap, uint32_t* counts, uint32_
   sync();
   const uint32_t S = v_.n_slots;
   std::vector<uint32_t> cnt(S), tag(S);
-  cuda_check(cudaMemcpy(cnt.data(), v_.nbr_count, S * 4ull, cudaMemcpyDeviceToHost), "d2h");
-  cuda_check(cudaMemcpy(tag.data(), v_.tag, S * 4ull, cudaMemcpyDeviceToHost), "d2h");
+  d2h(cnt.data(), v_.nbr_count, S * 4ull, "d2h");
+  d2h(tag.data(), v_.tag, S * 4ull, "d2h");
   // Only the groups of this replica's slots are copied.
   const uint64_t g0 = h.atom_begin / kGroup, g1 = (h.atom_begin + h.n_pad) / kGroup;
   const uint64_t per_group = static_cast<uint64_t>(v_.nbr_stride) * kGroup;
   std::vector<uint32_t> list((g1 - g0) * per_group);
-  cuda_check(cudaMemcpy(list.data(), v_.nbr + g0 * per_group, list.size() * 4ull, cudaMemcpyDeviceToHost), "d2h");
+  d2h(list.data(), v_.nbr + g0 * per_group, list.size() * 4ull, "d2h");
   for (uint32_t k = 0; k < h.n_atoms; ++k) {
     const uint32_t slot = h.atom_begin + k;
     const uint32_t t = tag[slot] - h.tag_base;  // 0-based local
@@ -1326,10 +1324,9 @@ void Engine::debug_neighbors_staged(uint32_t r, uint32_t cap, uint32_t* counts,
     cuda_check(cudaMemsetAsync(d_count, 0, S * 4ull, stream_), "memset");
     launch_list_to_slots(launch_, cap, d_count, d_list);
     sync();
-    cuda_check(cudaMemcpy(cnt.data(), d_count, S * 4ull, cudaMemcpyDeviceToHost), "d2h");
-    cuda_check(cudaMemcpy(list.data(), d_list + static_cast<size_t>(h.atom_begin) * cap,
-                          list.size() * 4ull, cudaMemcpyDeviceToHost), "d2h");
-    cuda_check(cudaMemcpy(tag.data(), v_.tag, S * 4ull, cudaMemcpyDeviceToHost), "d2h");
+    d2h(cnt.data(), d_count, S * 4ull, "d2h");
+    d2h(list.data(), d_list + static_cast<size_t>(h.atom_begin) * cap, list.size() * 4ull, "d2h");
+    d2h(tag.data(), v_.tag, S * 4ull, "d2h");
   } catch (...) {
     cudaFree(d_count);
     cudaFree(d_list);

@@ -185,6 +185,11 @@ class Engine {
   void clear_replay_graphs();
   void launch_chunk(uint32_t steps, bool obs_last);
   void sync();
+  // Host<->device copies ordered on stream_ and complete on return.  The
+  // engine stream is non-blocking, so a plain cudaMemcpy (legacy stream) is
+  // not ordered against its kernels or its zero fills.
+  void h2d(void* dst, const void* src, size_t bytes, const char* what);
+  void d2h(void* dst, const void* src, size_t bytes, const char* what);
 
   std::vector<ReplicaHost> rep_;
   std::vector<void*> allocations_;
