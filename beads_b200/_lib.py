@@ -158,6 +158,7 @@ EXPORTED = (
     "beads_profile",
     "beads_list_stats",
     "beads_counters",
+    "beads_launch_counts",
     "beads_set_tuning",
     "beads_get_tuning",
     "beads_set_list_layout",
@@ -211,6 +212,8 @@ def load():
     L.beads_profile.argtypes = [vp, ctypes.c_int32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]
     L.beads_list_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint32)]
     L.beads_counters.argtypes = [vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)]
+    L.beads_launch_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32),
+                                      ctypes.POINTER(ctypes.c_uint32)]
     L.beads_set_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
     L.beads_get_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
     L.beads_set_list_layout.argtypes = [vp, ctypes.c_int32]

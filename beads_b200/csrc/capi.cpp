@@ -467,6 +467,13 @@ int beads_counters(beads_ctx* ctx, uint32_t replica, uint64_t* counters) {
   });
 }
 
+int beads_launch_counts(beads_ctx* ctx, uint32_t* per_step, uint32_t* per_rebuild_chain) {
+  return guarded([&] {
+    require(ctx && ctx->engine && per_step && per_rebuild_chain, "NULL argument.");
+    ctx->engine->launch_counts(*per_step, *per_rebuild_chain);
+  });
+}
+
 int beads_debug_cells(beads_ctx* ctx, uint32_t replica, uint32_t* cell_by_tag) {
   return guarded([&] {
     require(ctx && ctx->engine && cell_by_tag, "NULL argument.");

@@ -22,6 +22,22 @@ void cuda_check(cudaError_t e, const char* what) {
 
 namespace {
 
+// Kernel nodes at the top level of a captured graph (a conditional node's
+// body is a graph of its own).
+uint32_t kernel_nodes(cudaGraph_t graph) {
+  size_t n = 0;
+  cuda_check(cudaGraphGetNodes(graph, nullptr, &n), "graph nodes");
+  std::vector<cudaGraphNode_t> nodes(n);
+  cuda_check(cudaGraphGetNodes(graph, nodes.data(), &n), "graph nodes");
+  uint32_t kernels = 0;
+  for (cudaGraphNode_t node : nodes) {
+    cudaGraphNodeType type;
+    cuda_check(cudaGraphNodeGetType(node, &type), "graph node type");
+    kernels += type == cudaGraphNodeTypeKernel ? 1u : 0u;
+  }
+  return kernels;
+}
+
 constexpr uint32_t kChunkMax = 16;     // steps per captured graph
 constexpr double kKbNmKjMol = 0.00831446261815324;
 constexpr double kPressNmKjMol = 16.60539067;
@@ -852,6 +868,7 @@ void Engine::record_step_conditional(bool observables) {
     throw;
   }
   cuda_check(cudaStreamEndCapture(side_stream_, &body), "body capture end");
+  chain_kernels_ = kernel_nodes(body);
   launch_forces(launch_, observables, false, true);
 }
 
@@ -896,6 +913,29 @@ cudaGraphExec_t Engine::graph_for(uint32_t steps, bool obs_last) {
   }
   graphs_[key] = std::make_pair(graph, exec);
   return exec;
+}
+
+void Engine::launch_counts(uint32_t& per_step, uint32_t& per_chain) {
+  const bool conditional = use_graphs_ && use_conditional_;
+  sync();
+  cudaGraph_t graph = nullptr;
+  cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+  try {
+    if (conditional) {
+      record_step_conditional(false);
+    } else {
+      record_step(false);
+    }
+  } catch (...) {
+    cudaGraph_t discard = nullptr;
+    cudaStreamEndCapture(stream_, &discard);
+    if (discard) cudaGraphDestroy(discard);
+    throw;
+  }
+  cuda_check(cudaStreamEndCapture(stream_, &graph), "end capture");
+  per_step = kernel_nodes(graph);
+  per_chain = conditional ? chain_kernels_ : 0u;
+  cudaGraphDestroy(graph);
 }
 
 void Engine::launch_chunk(uint32_t steps, bool obs_last) {
@@ -1206,6 +1246,9 @@ void Engine::upload_all(const float* pos, const float* vel) {
   if (vel) cuda_check(cudaMemcpyAsync(d_xfer_vel_, vel, bytes, cudaMemcpyHostToDevice, stream_), "h2d");
   launch_scatter_state(launch_, pos ? d_xfer_pos_ : nullptr, vel ? d_xfer_vel_ : nullptr,
                        static_cast<uint32_t>(n_tags_));
+  // From pinned host memory the copies are asynchronous: the caller may reuse
+  // its buffers as soon as this returns.
+  sync();
   initialized_ = false;
 }
 

@@ -118,6 +118,11 @@ class Engine {
   // Completed steps, neighbour builds and dangerous rebuilds of one replica,
   // and the launches of the rebuild chain so far (whole batch).
   void counters(uint32_t replica, uint64_t out[4]);
+  // Kernels one MD step launches under the current schedule, and the
+  // kernels of one rebuild chain when that chain runs only on rebuild steps
+  // (0 when every step launches it: no conditional graph node).  Counted
+  // as the kernel nodes of one captured step; nothing is executed.
+  void launch_counts(uint32_t& per_step, uint32_t& per_chain);
   void check_status();
   // Kernel schedule of the step: threads per particle of the pair-force
   // kernel (1, 2 or 4), its batch depth (4 or 8 list entries in flight per
@@ -201,6 +206,7 @@ class Engine {
   bool initialized_ = false;
   bool use_graphs_ = true;
   bool use_conditional_ = true;
+  uint32_t chain_kernels_ = 0;  // kernel nodes of the last captured rebuild-chain body
   uint32_t total_bond_types_ = 0, total_angle_types_ = 0, total_dihedral_types_ = 0;
   bool staged_ = false;                // some replica stages its pair forces
   uint32_t stage_cap_ = 0;             // stage entries per group (k_lj_staged)

@@ -388,6 +388,16 @@ class Engine:
         return {"steps": int(out[0]), "builds": int(out[1]), "dangerous": int(out[2]),
                 "chain_launches": int(out[3])}
 
+    def launch_counts(self) -> dict:
+        """Kernels per MD step and per rebuild chain under the current
+        schedule (see beads_launch_counts); per_rebuild_chain is 0 when every
+        step launches the chain."""
+        per_step = ctypes.c_uint32()
+        per_chain = ctypes.c_uint32()
+        _lib.check(self._lib.beads_launch_counts(self._h, ctypes.byref(per_step),
+                                                 ctypes.byref(per_chain)))
+        return {"per_step": per_step.value, "per_rebuild_chain": per_chain.value}
+
     def list_stats(self) -> dict:
         total = ctypes.c_uint64()
         mx = ctypes.c_uint32()

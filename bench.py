@@ -474,6 +474,14 @@ def run_ours(args) -> None:
     achieved = spec.n * bytes_per_atom / (force_ms / 1e3) / 1e9
     peak, peak_kind = _peaks()
     traffic = _traffic_from_profile()
+    # Secondary figure: FP32 work of the pair kernel per atom-step, 9 per
+    # listed pair (difference, r^2, test) + 23 per pair inside rc (force,
+    # energy, virial); pairs inside rc estimated from the list at uniform
+    # density, n_c = n_l (rc / (rc + skin))^3.  Peak: SMs x 128 FP32 lanes x
+    # 2 FLOP (FMA) x the SM clock sampled during the timed steps.
+    n_inside = mean_nbr * (spec.cutoff / (spec.cutoff + spec.cutoff_buffer)) ** 3
+    flop_per_atom = 9.0 * mean_nbr + 23.0 * n_inside
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
 
     # End-to-end through the C ABI with host buffers: upload positions and
     # velocities, run E2E_STEPS steps (the call rebuilds the list and forces
@@ -514,9 +522,21 @@ def run_ours(args) -> None:
     # Every step launches pre, the per-replica rebuild decision, the
     # pair-force kernel, post (unless the schedule fuses the kick into the
     # force kernel) and the per-replica finish kernel; a step that rebuilds
-    # also runs the 7 kernels of the rebuild chain (conditional graph node).
-    per_step = 4 if eng.tuning()["fuse_post"] else 5
-    gpu_launches = per_step * args.steps + 7 * int(timed_chains)
+    # also runs the rebuild chain (conditional graph node).  The engine counts
+    # both as kernel nodes of a captured step.
+    launches = eng.launch_counts()
+    gpu_launches = (launches["per_step"] * args.steps
+                    + launches["per_rebuild_chain"] * int(timed_chains))
+    clock_mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
+    flops = None
+    if clock_mhz:
+        flop_achieved = spec.n * flop_per_atom / (force_ms / 1e3) / 1e12
+        flop_peak = sms * 128 * 2 * clock_mhz * 1e6 / 1e12
+        flops = {"kernel": "k_lj (pair forces)", "per_atom_step": flop_per_atom,
+                 "pairs_inside_rc_per_atom": n_inside, "achieved": flop_achieved,
+                 "peak": flop_peak, "unit": "TFLOP/s", "frac": flop_achieved / flop_peak,
+                 "peak_kind": f"FP32 FMA pipe, {sms} SMs x 128 lanes x 2 at {clock_mhz:.0f} MHz "
+                              "(SM clock sampled during the timed steps)"}
     line = {
         "metric": metric(world),
         "value": value,
@@ -536,6 +556,9 @@ def run_ours(args) -> None:
             "mean_neighbors": round(mean_nbr, 2),
             "max_neighbors_seen": stats["max"],
             "neighbor_builds_timed": int(timed_builds),
+            "rebuild_chain_launches_timed": int(timed_chains),
+            "kernels_per_step": launches["per_step"],
+            "kernels_per_rebuild_chain": launches["per_rebuild_chain"],
             "graph_warmup_steps": GRAPH_WARMUP,
             "schedule": eng.tuning(),
         },
@@ -559,6 +582,8 @@ def run_ours(args) -> None:
         "gpu_launches": gpu_launches,
         "clocks": clocks,
     }
+    if flops is not None:
+        line["flops"] = flops
     if drift is not None:
         line["energy_drift"] = drift
     if cpu is not None:
@@ -638,6 +663,7 @@ def run_replicas(args) -> None:
     batch_ms = max_over_ranks(start.elapsed_time(stop), dev)
     builds = int(sum_over_ranks(builds, dev))
     schedule = eng.tuning()
+    launches = eng.launch_counts()
     value = total_atoms * args.steps / (batch_ms / 1e3)
     eng.close()
 
@@ -690,7 +716,8 @@ def run_replicas(args) -> None:
             "graph_warmup_steps": GRAPH_WARMUP,
             "schedule": schedule,
         },
-        "gpu_launches": (4 if schedule["fuse_post"] else 5) * args.steps + 7 * int(chains),
+        "gpu_launches": (launches["per_step"] * args.steps
+                         + launches["per_rebuild_chain"] * int(chains)),
         "clocks": clocks,
     }
     if rank == 0:
@@ -755,6 +782,7 @@ def run_chains(args) -> None:
     builds = eng.counters(0)["builds"] - builds_before
     chains = eng.counters()["chain_launches"] - chains_before
     schedule = eng.tuning()
+    launches = eng.launch_counts()
     stats = eng.list_stats()
     mean_nbr = stats["entries"] / spec.n
 
@@ -817,10 +845,12 @@ def run_chains(args) -> None:
             "graph_warmup_steps": GRAPH_WARMUP,
             "schedule": schedule,
         },
-        # pre, decide, pair forces, bonded forces (+ half-kick), [post,] post finish
-        # per step; bin, scan, scatter, cellsort, two reorder passes, exclusion
-        # projection and list build per rebuild chain.
-        "gpu_launches": (5 if schedule["fuse_post"] else 6) * args.steps + 8 * int(chains),
+        # pre, decide, pair forces, bonded terms and their gather (+ half-kick),
+        # [post,] post finish per step; the rebuild chain (bin, three scan
+        # kernels, scatter, cell sorts, two reorder passes, exclusion
+        # projection, list build) per rebuild; counted by the engine.
+        "gpu_launches": (launches["per_step"] * args.steps
+                         + launches["per_rebuild_chain"] * int(chains)),
         "clocks": clocks,
         "roofline": {
             "bound": "hbm",

@@ -240,7 +240,9 @@ BEADS_API int beads_set_state(beads_ctx* ctx, uint32_t replica, const float* pos
 /* Whole-batch host transfers in TAG order, replica after replica (replica r's
  * block starts at the sum of the previous replicas' particle counts).  These
  * are one H2D / D2H copy each plus a device scatter/gather, used by callers
- * that stream the state every call.  Any pointer may be NULL. */
+ * that stream the state every call.  Both return once their copies are
+ * complete, so the host buffers (pinned or not) may be reused at once.  Any
+ * pointer may be NULL. */
 BEADS_API int beads_upload_all(beads_ctx* ctx, const float* positions,
                      const float* velocities);
 BEADS_API int beads_download_all(beads_ctx* ctx, float* positions, float* velocities);
@@ -345,6 +347,16 @@ BEADS_API int beads_adjoint_bonded_grads(beads_ctx* ctx, double* grad_bond, doub
  * rebuild chain so far for the whole context (a captured step launches the
  * chain only when some replica rebuilds).  counters has 4 entries. */
 BEADS_API int beads_counters(beads_ctx* ctx, uint32_t replica, uint64_t* counters);
+
+/* Kernel launches of the current schedule: *per_step kernels every MD step
+ * launches, and *per_rebuild_chain kernels each time the rebuild chain runs
+ * (counters[3] of beads_counters counts those runs).  *per_rebuild_chain is 0
+ * when every step launches the chain itself (no conditional graph node, or
+ * graphs switched off with BEADS_GRAPHS=0); *per_step then includes it.
+ * Counted as the kernel nodes of one captured step; nothing runs.  No
+ * counterpart in the reference (measurement). */
+BEADS_API int beads_launch_counts(beads_ctx* ctx, uint32_t* per_step,
+                                  uint32_t* per_rebuild_chain);
 
 /* Steepest descent with a per-particle displacement cap, used to relax
  * random initial configurations: x += dmax * F / max(|F|, fref), with the LJ

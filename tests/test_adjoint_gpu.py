@@ -113,11 +113,12 @@ def _fit_loss(obs, volumes, pe_target, p_target):
 
 def test_parameter_gradients_match_central_differences():
     """d loss / d(eps_ab, sigma_ab) of the fit loss against central finite
-    differences of the FP64 restatement.  The step is 1e-6 relative: the
-    truncated LJ force jumps at the cutoff, so a step of 1e-3 moves pairs
-    across it and the difference quotient then differs from the derivative
-    by about 1% on this run (the FP64 restatement's own autograd gradient
-    shows the same gap)."""
+    differences of the FP64 restatement, at relative steps 1e-6 and 1e-3.
+    At 1e-6 they agree to 1e-4.  The truncated LJ force jumps at the cutoff,
+    so a step of 1e-3 moves pairs across it and the difference quotient then
+    differs from the derivative by 0.7% on this run; the FP64 restatement's
+    own autograd gradient shows the same gap (6.7e-3), so the bound there is
+    3%."""
     specs = _small(seed=9)
     steps, rec = 40, 25
     vols = torch.tensor([float(np.prod(np.asarray(s.box_bound[1], np.float64) - s.box_bound[0]))
@@ -149,24 +150,25 @@ def test_parameter_gradients_match_central_differences():
             at += n
         return float(_fit_loss(torch.stack(rows, dim=1), vols, pe_t, p_t))
 
-    ours, fd = [], []
-    for which, base, grad in (("eps", eps0, eps.grad), ("sig", sig0, sig.grad)):
-        for a, b in ((0, 0), (0, 1), (1, 1)):
-            h = 1e-6 * float(base[a, b])
-            plus, minus = base.clone(), base.clone()
-            plus[a, b] += h
-            minus[a, b] -= h
-            if a != b:  # the symmetric table entry moves with it
-                plus[b, a] += h
-                minus[b, a] -= h
-            if which == "eps":
-                d = (loss_fp64(plus, sig0) - loss_fp64(minus, sig0)) / (2 * h)
-            else:
-                d = (loss_fp64(eps0, plus) - loss_fp64(eps0, minus)) / (2 * h)
-            fd.append(d)
-            ours.append(float(grad[a, b] + (grad[b, a] if a != b else 0.0)))
-    ours, fd = np.array(ours), np.array(fd)
-    assert np.linalg.norm(ours - fd) / np.linalg.norm(fd) < 1e-4, (ours, fd)
+    for rel, bound in ((1e-6, 1e-4), (1e-3, 3e-2)):
+        ours, fd = [], []
+        for which, base, grad in (("eps", eps0, eps.grad), ("sig", sig0, sig.grad)):
+            for a, b in ((0, 0), (0, 1), (1, 1)):
+                h = rel * float(base[a, b])
+                plus, minus = base.clone(), base.clone()
+                plus[a, b] += h
+                minus[a, b] -= h
+                if a != b:  # the symmetric table entry moves with it
+                    plus[b, a] += h
+                    minus[b, a] -= h
+                if which == "eps":
+                    d = (loss_fp64(plus, sig0) - loss_fp64(minus, sig0)) / (2 * h)
+                else:
+                    d = (loss_fp64(eps0, plus) - loss_fp64(eps0, minus)) / (2 * h)
+                fd.append(d)
+                ours.append(float(grad[a, b] + (grad[b, a] if a != b else 0.0)))
+        ours, fd = np.array(ours), np.array(fd)
+        assert np.linalg.norm(ours - fd) / np.linalg.norm(fd) < bound, (rel, ours, fd)
 
 
 def test_bonded_adjoint_matches_fp64_autograd():
