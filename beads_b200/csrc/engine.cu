@@ -22,22 +22,6 @@ void cuda_check(cudaError_t e, const char* what) {
 
 namespace {
 
-// Kernel nodes at the top level of a captured graph (a conditional node's
-// body is a graph of its own).
-uint32_t kernel_nodes(cudaGraph_t graph) {
-  size_t n = 0;
-  cuda_check(cudaGraphGetNodes(graph, nullptr, &n), "graph nodes");
-  std::vector<cudaGraphNode_t> nodes(n);
-  cuda_check(cudaGraphGetNodes(graph, nodes.data(), &n), "graph nodes");
-  uint32_t kernels = 0;
-  for (cudaGraphNode_t node : nodes) {
-    cudaGraphNodeType type;
-    cuda_check(cudaGraphNodeGetType(node, &type), "graph node type");
-    kernels += type == cudaGraphNodeTypeKernel ? 1u : 0u;
-  }
-  return kernels;
-}
-
 constexpr uint32_t kChunkMax = 16;     // steps per captured graph
 constexpr double kKbNmKjMol = 0.00831446261815324;
 constexpr double kPressNmKjMol = 16.60539067;
@@ -868,7 +852,7 @@ void Engine::record_step_conditional(bool observables) {
     throw;
   }
   cuda_check(cudaStreamEndCapture(side_stream_, &body), "body capture end");
-  chain_kernels_ = kernel_nodes(body);
+  last_chain_body_ = body;
   launch_forces(launch_, observables, false, true);
 }
 
@@ -933,9 +917,17 @@ void Engine::launch_counts(uint32_t& per_step, uint32_t& per_chain) {
     throw;
   }
   cuda_check(cudaStreamEndCapture(stream_, &graph), "end capture");
-  per_step = kernel_nodes(graph);
-  per_chain = conditional ? chain_kernels_ : 0u;
+  // Every node a step records is a kernel launch, except the conditional
+  // node that holds the rebuild chain (whose body holds only kernels).  The
+  // graphs are only queried once the capture has ended.
+  size_t top = 0, body = 0;
+  cudaError_t e = cudaGraphGetNodes(graph, nullptr, &top);
+  if (e == cudaSuccess && conditional) e = cudaGraphGetNodes(last_chain_body_, nullptr, &body);
+  last_chain_body_ = nullptr;
   cudaGraphDestroy(graph);
+  cuda_check(e, "graph nodes");
+  per_step = static_cast<uint32_t>(conditional ? top - 1 : top);
+  per_chain = static_cast<uint32_t>(body);
 }
 
 void Engine::launch_chunk(uint32_t steps, bool obs_last) {

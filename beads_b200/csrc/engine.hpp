@@ -206,7 +206,7 @@ class Engine {
   bool initialized_ = false;
   bool use_graphs_ = true;
   bool use_conditional_ = true;
-  uint32_t chain_kernels_ = 0;  // kernel nodes of the last captured rebuild-chain body
+  cudaGraph_t last_chain_body_ = nullptr;  // body of the last recorded conditional node
   uint32_t total_bond_types_ = 0, total_angle_types_ = 0, total_dihedral_types_ = 0;
   bool staged_ = false;                // some replica stages its pair forces
   uint32_t stage_cap_ = 0;             // stage entries per group (k_lj_staged)
