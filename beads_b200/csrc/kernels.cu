@@ -785,8 +785,10 @@ __device__ __forceinline__ void build_chunk(const DeviceView& v, const ReplicaPa
   }
 }
 
-// The list rows of the particles of global cell g (one warp).
-template <int kCap>
+// The list rows of the particles of global cell g (one warp).  kByQ: the
+// context lists rows by cell-order index (staged layout); a compile-time
+// flag so that the slot-layout build carries none of the staging code.
+template <int kCap, bool kByQ>
 __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaParams& p,
                                            ReplicaState* st, uint32_t g, uint32_t lane,
                                            BuildShared& sh) {
@@ -859,7 +861,7 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
                        : kBuildInterior;
   const uint32_t nseg = regular ? 18u : kMaxSegments;
   bool any_overflow = false;
-  const bool by_q = v.list_by_q != 0;
+  constexpr bool by_q = kByQ;
   const bool staged_replica = by_q && p.staged != 0u && regular;
 
   // In a staged context the home particles in flight never span two groups
@@ -946,7 +948,7 @@ __device__ __forceinline__ void build_cell(const DeviceView& v, const ReplicaPar
 
 // Warp w builds the lists of work item w (k_scan): the warps past the cells
 // of the rebuilding replicas return after one load.
-template <int kCap>
+template <int kCap, bool kByQ>
 __global__ void __launch_bounds__(kBlock, 7) k_build(DeviceView v) {
   __shared__ BuildShared sh[kBuildWarps];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -954,7 +956,7 @@ __global__ void __launch_bounds__(kBlock, 7) k_build(DeviceView v) {
   if (w >= v.work_start[v.n_replicas]) return;  // warp-uniform
   const uint32_t r = work_replica(v, w);
   const ReplicaParams& p = v.rp[r];
-  build_cell<kCap>(v, p, &v.rs[r], p.cell_begin + (w - v.work_start[r]), lane, sh[warp]);
+  build_cell<kCap, kByQ>(v, p, &v.rs[r], p.cell_begin + (w - v.work_start[r]), lane, sh[warp]);
 }
 
 // The same lists, one thread per particle, for replicas whose cells hold a
@@ -965,8 +967,9 @@ __global__ void __launch_bounds__(kBlock, 7) k_build(DeviceView v) {
 // of a row, split in two where it wraps; ascending slot inside a cell) and
 // applies build_cell's float expressions, inclusion rule and entry encoding,
 // so the lists (order included) are the ones k_build writes.  A block is 128
-// consecutive cell-order rows: one stage group in a staged context.
-template <int kCap>
+// consecutive cell-order rows: one stage group in a staged context.  kByQ
+// as for k_build.
+template <int kCap, bool kByQ>
 __global__ void __launch_bounds__(kBlock) k_build_sparse(DeviceView v) {
   __shared__ StageLayout lay;
   const uint32_t b = blockIdx.x;
@@ -977,7 +980,7 @@ __global__ void __launch_bounds__(kBlock) k_build_sparse(DeviceView v) {
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t nx = p.nc[0], ny = p.nc[1], nz = p.nc[2];
   const bool regular = nx >= 4u && ny >= 4u && nz >= 4u;
-  const bool by_q = v.list_by_q != 0;
+  constexpr bool by_q = kByQ;
   const bool staged_replica = by_q && p.staged != 0u && regular;
   if (staged_replica) {
     if (warp == 0) stage_layout(v, p, b, lane, v.stage_cap, lay);
@@ -2133,10 +2136,18 @@ void launch_rebuild(const StepLaunch& l, bool force_all, bool count_build) {
     check_launch("project_exclusions");
   }
   const uint32_t bg = (l.v.total_cells + kBuildWarps - 1) / kBuildWarps;
-#define BB_BUILD(cap)                                                              \
-  do {                                                                              \
-    if (l.any_dense) k_build<cap><<<bg, kBlock, 0, l.stream>>>(l.v);                \
-    if (l.any_sparse) k_build_sparse<cap><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); \
+#define BB_BUILD_Q(cap, q)                                                             \
+  do {                                                                                  \
+    if (l.any_dense) k_build<cap, q><<<bg, kBlock, 0, l.stream>>>(l.v);                 \
+    if (l.any_sparse) k_build_sparse<cap, q><<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v); \
+  } while (0)
+#define BB_BUILD(cap)           \
+  do {                          \
+    if (l.v.list_by_q) {        \
+      BB_BUILD_Q(cap, true);    \
+    } else {                    \
+      BB_BUILD_Q(cap, false);   \
+    }                           \
   } while (0)
   switch (l.excl_cap) {
     case 0: BB_BUILD(0); break;
@@ -2148,6 +2159,7 @@ void launch_rebuild(const StepLaunch& l, bool force_all, bool count_build) {
     default: throw std::runtime_error("unsupported exclusion capacity");
   }
 #undef BB_BUILD
+#undef BB_BUILD_Q
   check_launch("build");
 }
 
