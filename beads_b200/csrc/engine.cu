@@ -900,6 +900,9 @@ cudaGraphExec_t Engine::graph_for(uint32_t steps, bool obs_last) {
 }
 
 void Engine::launch_counts(uint32_t& per_step, uint32_t& per_chain) {
+  // The cached one-step graph settles whether this driver takes conditional
+  // nodes (graph_for falls back to recording the chain in every step).
+  if (use_graphs_) graph_for(1, false);
   const bool conditional = use_graphs_ && use_conditional_;
   sync();
   cudaGraph_t graph = nullptr;
