@@ -723,7 +723,8 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
 
   cuda_check(cudaMallocHost(&h_obs_, n * sizeof(ReplicaObs)), "cudaMallocHost");
   cuda_check(cudaMallocHost(&h_state_, n * sizeof(ReplicaState)), "cudaMallocHost");
-  cuda_check(cudaMallocHost(&h_chunk_status_, 2 * n * sizeof(unsigned)), "cudaMallocHost");
+  cuda_check(cudaMallocHost(&h_chunk_status_, kStatusRing * n * sizeof(unsigned)),
+             "cudaMallocHost");
   for (cudaEvent_t& e : chunk_event_) {
     cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event create");
   }
@@ -954,7 +955,7 @@ bool Engine::run(uint64_t steps, uint64_t obs_every, const std::function<bool()>
   // Status words of a finished chunk: any bit set means the step that set it
   // failed; check_status() (full download, reference message) then throws.
   auto chunk_failed = [&](uint64_t k) {
-    const unsigned* w = h_chunk_status_ + (k & 1u) * n;
+    const unsigned* w = h_chunk_status_ + (k % kStatusRing) * n;
     for (uint32_t r = 0; r < n; ++r) {
       if (w[r] != 0u) return true;
     }
@@ -980,19 +981,25 @@ bool Engine::run(uint64_t steps, uint64_t obs_every, const std::function<bool()>
     }
     launch_chunk(static_cast<uint32_t>(chunk), obs);
     // This chunk's status words, gathered from the replica states (one
-    // strided copy), land in its half of the pinned ring.
+    // strided copy), land in its slot of the pinned ring.
     const uint64_t k = chunks++;
-    cuda_check(cudaMemcpy2DAsync(h_chunk_status_ + (k & 1u) * n, sizeof(unsigned), &v_.rs->status,
+    cuda_check(cudaMemcpy2DAsync(h_chunk_status_ + (k % kStatusRing) * n, sizeof(unsigned),
+                                 &v_.rs->status,
                                  sizeof(ReplicaState), sizeof(unsigned), n,
                                  cudaMemcpyDeviceToHost, stream_),
                "status copy");
-    cuda_check(cudaEventRecord(chunk_event_[k & 1u], stream_), "event record");
+    cuda_check(cudaEventRecord(chunk_event_[k % kStatusRing], stream_), "event record");
     step_ += chunk;
     remaining -= chunk;
     last_obs = obs;
-    if (k > 0) {
-      cuda_check(cudaEventSynchronize(chunk_event_[(k - 1) & 1u]), "status wait");
-      if (chunk_failed(k - 1)) check_status();
+    // Check the chunk two before this one: the GPU still holds the last two
+    // chunks while the host waits, so a host stall of up to a chunk's length
+    // leaves it no idle gap.  A failure is raised at most two chunks after
+    // the chunk that set it (every chunk left is checked at the end).
+    constexpr uint64_t kLag = kStatusRing - 1;
+    if (k >= kLag) {
+      cuda_check(cudaEventSynchronize(chunk_event_[(k - kLag) % kStatusRing]), "status wait");
+      if (chunk_failed(k - kLag)) check_status();
     }
     if (poll != nullptr && remaining > 0 && step_ - last_poll >= poll_every) {
       last_poll = step_;

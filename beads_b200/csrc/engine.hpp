@@ -222,8 +222,12 @@ class Engine {
   std::map<uint32_t, std::pair<cudaGraph_t, cudaGraphExec_t>> replay_graphs_;
   ReplicaObs* h_obs_ = nullptr;        // pinned
   ReplicaState* h_state_ = nullptr;    // pinned
-  unsigned* h_chunk_status_ = nullptr; // pinned, [2][n_replicas]: status words after a chunk
-  cudaEvent_t chunk_event_[2] = {nullptr, nullptr};
+  // Status words of the last kStatusRing chunks (pinned, [kStatusRing][n_replicas]).
+  // The run loop checks a chunk's words once the two chunks after it are
+  // queued, so the GPU keeps two chunks of work while the host waits.
+  static constexpr uint32_t kStatusRing = 3;
+  unsigned* h_chunk_status_ = nullptr;
+  cudaEvent_t chunk_event_[kStatusRing] = {};
   float* d_xfer_pos_ = nullptr;        // tag-order staging (lazily allocated)
   float* d_xfer_vel_ = nullptr;
   std::vector<uint32_t> host_row_tag_;  // per replica concatenated (global tag idx)

@@ -1,8 +1,9 @@
 """Run-loop failure semantics on the GPU, without faulting it.
 
   * A neighbour list that overflows in the middle of a run is raised within
-    one captured chunk (16 steps) of the chunk whose build overflowed: the
-    engine reads each chunk's status words while the next chunk runs.  (The
+    two captured chunks (16 steps each) of the chunk whose build overflowed:
+    the engine reads each chunk's status words while the next two chunks
+    run, so the GPU always has queued work while the host waits.  (The
     reference raises right after the overflowing build,
     native/src/simulation/neighbor/neighbor_system.cpp:143.)  The overflow
     itself is an ordinary status bit: the build clamps its writes at the
@@ -56,14 +57,14 @@ def test_overflow_mid_run_raises_within_a_chunk():
                 first = s
                 break
     assert first is not None and first > 1, "the lattice never overflowed its list"
-    # The same dynamics in one long call: the error arrives at most one chunk
-    # after the chunk holding the overflowing build.
+    # The same dynamics in one long call: the error arrives at most two
+    # chunks after the chunk holding the overflowing build.
     with Engine(spec) as eng:
         eng.eval()
         with pytest.raises(RuntimeError, match="NeighborList overflow"):
             eng.run(limit)
         done = eng.counters()["steps"]
-    assert first <= done <= first + 2 * CHUNK, (first, done)
+    assert first <= done <= first + 3 * CHUNK, (first, done)
 
 
 def test_interrupt_stops_execute_simulation(tmp_path, monkeypatch):
@@ -115,8 +116,8 @@ def test_failed_state_stops_list_builds():
             eng.run(4 * CHUNK)
         c = eng.counters()
     # Step 1 may rebuild (its decision comes before the failing kick); none of
-    # the later steps of the chunk does, and the error arrives within two
-    # chunks.
+    # the later steps does, and the error arrives while at most two more
+    # chunks run.
     assert c["steps"] >= 2, c
     assert c["builds"] <= builds0 + 1, (builds0, c)
-    assert c["steps"] <= 2 * CHUNK, c
+    assert c["steps"] <= 3 * CHUNK, c
