@@ -202,7 +202,8 @@ __global__ void __launch_bounds__(kBlock) k_bin(DeviceView v) {
 // k_scan (one block per replica: the work list of the per-cell kernels and
 // the exclusive prefix of the replica's chunk totals) and k_scan_cells (one
 // block per chunk: the starts and cursors of its cells; the counts are reset
-// for the next build).
+// for the next build).  When every replica fits one chunk, k_scan_single
+// does all three in one launch.
 constexpr int kScanThreads = 1024;
 constexpr int kScanWarps = kScanThreads / 32;
 constexpr uint32_t kScanPer = kScanChunk / kScanThreads;  // consecutive cells per thread
@@ -261,15 +262,13 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_sum(DeviceView v) {
   }
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan(DeviceView v) {
-  const uint32_t r = blockIdx.x;
+// Work list of the per-cell kernels (cell sort, list build): work item w is
+// cell w - work_start[q] of the rebuilding replica q with work_start[q] <= w
+// < work_start[q + 1].  Block r (one per replica) writes entry r (the cells
+// of the rebuilding replicas before it), block 0 also the total.
+__device__ __forceinline__ void write_work_start(const DeviceView& v, uint32_t r) {
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   {
-    // Work list of the per-cell kernels (cell sort, list build): work item
-    // w is cell w - work_start[q] of the rebuilding replica q with
-    // work_start[q] <= w < work_start[q + 1].  Every block writes its own
-    // entry (the cells of the rebuilding replicas before it), block 0 also
-    // the total.
     uint32_t before = 0, all = 0;
     for (uint32_t q = threadIdx.x; q < v.n_replicas; q += kScanThreads) {
       const uint32_t c = v.rs[q].need_rebuild ? v.rp[q].n_cells : 0u;
@@ -294,6 +293,11 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(DeviceView v) {
       if (r == 0) v.work_start[v.n_replicas] = sa;
     }
   }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan(DeviceView v) {
+  const uint32_t r = blockIdx.x;
+  write_work_start(v, r);
   if (!v.rs[r].need_rebuild) return;  // block-uniform
   const ReplicaParams& p = v.rp[r];
   // Exclusive prefix of the replica's chunk totals, in place.
@@ -310,12 +314,12 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(DeviceView v) {
   if (threadIdx.x == 0) v.cell_start[p.start_base + p.n_cells] = p.atom_begin + p.n_atoms;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_cells(DeviceView v) {
-  const uint32_t b = blockIdx.x;
-  const uint32_t r = v.scan_chunk_replica[b];
-  if (!v.rs[r].need_rebuild) return;
-  const ReplicaParams& p = v.rp[r];
-  const uint32_t c0 = (b - v.scan_chunk_first[r]) * kScanChunk + threadIdx.x * kScanPer;
+// Starts and cursors of the cells of chunk `chunk` of replica p (the counts
+// are reset for the next build); `prefix` is the count total of the
+// replica's chunks before it.
+__device__ __forceinline__ void scan_chunk_cells(const DeviceView& v, const ReplicaParams& p,
+                                                 uint32_t chunk, uint32_t prefix) {
+  const uint32_t c0 = chunk * kScanChunk + threadIdx.x * kScanPer;
   uint32_t* count = v.cell_count + p.cell_begin;
   uint32_t cnt[kScanPer];
   uint32_t s = 0;
@@ -325,7 +329,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_cells(DeviceView v) {
     s += cnt[k];
   }
   uint32_t total;
-  uint32_t run = p.atom_begin + v.scan_chunk_sum[b] + block_exclusive_scan(s, total);
+  uint32_t run = p.atom_begin + prefix + block_exclusive_scan(s, total);
   uint32_t* start = v.cell_start + p.start_base;
   uint32_t* cursor = v.cell_cursor + p.cell_begin;
 #pragma unroll
@@ -338,6 +342,25 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_cells(DeviceView v) {
     }
     run += cnt[k];
   }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_cells(DeviceView v) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t r = v.scan_chunk_replica[b];
+  if (!v.rs[r].need_rebuild) return;
+  scan_chunk_cells(v, v.rp[r], b - v.scan_chunk_first[r], v.scan_chunk_sum[b]);
+}
+
+// The same scan when every replica's cells fit one chunk (a batch of small
+// replicas): the work list, then the replica's starts and cursors with a
+// zero chunk prefix, in one launch instead of three.
+__global__ void __launch_bounds__(kScanThreads) k_scan_single(DeviceView v) {
+  const uint32_t r = blockIdx.x;
+  write_work_start(v, r);
+  if (!v.rs[r].need_rebuild) return;  // block-uniform
+  const ReplicaParams& p = v.rp[r];
+  scan_chunk_cells(v, p, 0u, 0u);
+  if (threadIdx.x == 0) v.cell_start[p.start_base + p.n_cells] = p.atom_begin + p.n_atoms;
 }
 
 // rebuild 3: scatter slots into their cells (order inside a cell is fixed by
@@ -2113,12 +2136,17 @@ void launch_rebuild(const StepLaunch& l, bool force_all, bool count_build) {
   }
   k_bin<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
   check_launch("bin");
-  k_scan_sum<<<l.v.n_scan_chunks, kScanThreads, 0, l.stream>>>(l.v);
-  check_launch("scan sum");
-  k_scan<<<l.v.n_replicas, kScanThreads, 0, l.stream>>>(l.v);
-  check_launch("scan");
-  k_scan_cells<<<l.v.n_scan_chunks, kScanThreads, 0, l.stream>>>(l.v);
-  check_launch("scan cells");
+  if (l.v.n_scan_chunks == l.v.n_replicas) {  // every replica fits one chunk
+    k_scan_single<<<l.v.n_replicas, kScanThreads, 0, l.stream>>>(l.v);
+    check_launch("scan");
+  } else {
+    k_scan_sum<<<l.v.n_scan_chunks, kScanThreads, 0, l.stream>>>(l.v);
+    check_launch("scan sum");
+    k_scan<<<l.v.n_replicas, kScanThreads, 0, l.stream>>>(l.v);
+    check_launch("scan");
+    k_scan_cells<<<l.v.n_scan_chunks, kScanThreads, 0, l.stream>>>(l.v);
+    check_launch("scan cells");
+  }
   k_scatter<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
   check_launch("scatter");
   if (l.any_sparse) {

@@ -27,9 +27,10 @@ def test_lattice_step_and_chain_kernels():
     # pre, decide, pair forces, post, post finish; the fused schedule drops post
     assert plain["per_step"] == 5, plain
     assert fused["per_step"] == 4, fused
-    # bin, three scan kernels, scatter, cell sort, two reorder kernels, build
-    assert plain["per_rebuild_chain"] == 9, plain
-    assert fused["per_rebuild_chain"] == 9, fused
+    # bin, scan (64 cells: one chunk, one scan kernel), scatter, cell sort,
+    # two reorder kernels, build
+    assert plain["per_rebuild_chain"] == 7, plain
+    assert fused["per_rebuild_chain"] == 7, fused
 
 
 def test_melt_adds_bonded_kernels_and_chain_stages():
@@ -39,4 +40,13 @@ def test_melt_adds_bonded_kernels_and_chain_stages():
     assert counts["per_step"] == 7, counts
     # the sparse cell sort, the exclusion projection and the sparse build
     # (in place of the dense one) join the chain
-    assert counts["per_rebuild_chain"] == 11, counts
+    assert counts["per_rebuild_chain"] == 9, counts
+
+
+def test_replicas_beyond_one_scan_chunk_take_the_three_kernel_scan():
+    # A scan chunk holds 4,096 cells: a 46^3-site lattice (97,336 beads)
+    # has 17^3 = 4,913 cells, two chunks.
+    big = workloads.lj_lattice(n_side=46)
+    counts = _counts(big, False)
+    # bin, three scan kernels, scatter, cell sort, two reorder kernels, build
+    assert counts["per_rebuild_chain"] == 9, counts
