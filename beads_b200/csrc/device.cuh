@@ -217,6 +217,11 @@ struct DeviceView {
   ReplicaState* rs;
   ReplicaObs* obs;
   const uint32_t* block_replica;
+  // Rebuild chain over the rebuilding replicas' slot blocks (batches):
+  // chain_block_start[q] = blocks of the rebuilding replicas before q
+  // ([n_replicas + 1], laid out by k_chain_blocks).
+  uint32_t* chain_block_start;
+  uint32_t chain_block_list;
   const uint32_t* cell_replica;  // replica of each global cell
   unsigned long long* chain_launches;  // launches of the rebuild chain so far
   long long* ke_part;            // [replica][kKeBuckets][whole, frac] kinetic-energy buckets

@@ -611,6 +611,8 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   v.ref_img = dalloc<int4>(S);
   v.cross = dalloc<uint32_t>(S);
   v.work_start = dalloc<uint32_t>(n + 1);
+  v.chain_block_start = dalloc<uint32_t>(n + 1);
+  v.chain_block_list = n > 1 ? 1u : 0u;
   {
     std::vector<uint32_t> chunk_replica, chunk_first(n + 1);
     for (uint32_t r = 0; r < n; ++r) {
@@ -746,6 +748,14 @@ void Engine::upload_static(uint32_t n, const beads_system_desc* systems,
   launch_.need_kinetic = any_thermostat ? 1 : 0;
   launch_.any_dense = any_dense_ ? 1 : 0;
   launch_.any_sparse = any_sparse_ ? 1 : 0;
+  {
+    // One wave of 128-thread blocks (16 per SM) for the chain's per-slot
+    // kernels when they walk the block list.
+    int device = 0, sms = 0;
+    cuda_check(cudaGetDevice(&device), "device");
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+    launch_.chain_grid = std::max<uint32_t>(1u, std::min<uint32_t>(v.n_blocks, 16u * sms));
+  }
   if (staged_) prepare_staged_kernels(static_cast<size_t>(stage_cap_ + 1) * sizeof(float4));
   // Initial slot-space exclusion rows (slot order = input order).
   launch_project_exclusions(launch_, true);

@@ -176,26 +176,6 @@ __global__ void k_force_rebuild_flags(DeviceView v, int count_build) {
   st->checks_since_build = 0u;
 }
 
-// ---------------------------------------------------------------------------
-// rebuild 1: cell id and per-cell count.
-__global__ void __launch_bounds__(kBlock) k_bin(DeviceView v) {
-  const uint32_t b = blockIdx.x;
-  if (b == 0 && threadIdx.x == 0) *v.chain_launches += 1ull;  // launches of the chain
-  const uint32_t r = v.block_replica[b];
-  if (!v.rs[r].need_rebuild) return;
-  const ReplicaParams& p = v.rp[r];
-  const uint32_t slot = b * kBlock + threadIdx.x;
-  const uint32_t local = slot - p.atom_begin;
-  if (local >= p.n_atoms) return;
-  const float4 x = v.pos[slot];
-  const uint32_t ix = axis_cell(x.x, p.lo[0], p.inv_cell[0], p.nc[0]);
-  const uint32_t iy = axis_cell(x.y, p.lo[1], p.inv_cell[1], p.nc[1]);
-  const uint32_t iz = axis_cell(x.z, p.lo[2], p.inv_cell[2], p.nc[2]);
-  const uint32_t cell = p.cell_begin + ix + p.nc[0] * (iy + p.nc[1] * iz);
-  v.cell_of_slot[slot] = cell;
-  atomicAdd(&v.cell_count[cell], 1u);
-}
-
 // rebuild 2: exclusive scan of the cell counts (the cell starts), in three
 // kernels so that a replica with many cells is scanned by many blocks:
 // k_scan_sum (one block per chunk of kScanChunk cells: the chunk's total),
@@ -236,6 +216,72 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t& t
   total = ws[kScanWarps];
   __syncthreads();  // ws is reused by the next call
   return out;
+}
+
+// ---------------------------------------------------------------------------
+// The per-slot kernels of the rebuild chain (bin, scatter, reorder) touch
+// only the replicas that rebuild.  In a batch, where a step typically
+// rebuilds a fifth of the replicas, they walk a list of those replicas'
+// 128-slot blocks with a grid of about one wave, instead of launching one
+// block per slot block of the batch that mostly returns at once.  Block item
+// w is block w - chain_block_start[q] of the rebuilding replica q with
+// chain_block_start[q] <= w < chain_block_start[q + 1]; k_chain_blocks (one
+// block) lays the list out at the head of the chain.
+__global__ void __launch_bounds__(kScanThreads) k_chain_blocks(DeviceView v) {
+  uint32_t run = 0;
+  for (uint32_t base = 0; base < v.n_replicas; base += kScanThreads) {
+    const uint32_t q = base + threadIdx.x;
+    const uint32_t x = (q < v.n_replicas && v.rs[q].need_rebuild) ? v.rp[q].n_pad / kBlock : 0u;
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan(x, total);
+    if (q < v.n_replicas) v.chain_block_start[q] = run + ex;
+    run += total;
+  }
+  if (threadIdx.x == 0) v.chain_block_start[v.n_replicas] = run;
+}
+
+// Runs F(v, b) for every slot block b this launch covers: the listed blocks
+// of the rebuilding replicas (grid-stride over the list) or, without the
+// list, block blockIdx.x of the batch.  F returns early for blocks of
+// replicas that do not rebuild; it holds no barrier.
+template <void (*F)(const DeviceView&, uint32_t)>
+__device__ __forceinline__ void for_chain_blocks(const DeviceView& v) {
+  if (v.chain_block_list) {
+    const uint32_t* start = v.chain_block_start;
+    const uint32_t total = start[v.n_replicas];
+    for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
+      uint32_t lo = 0, hi = v.n_replicas;  // start[lo] <= w < start[hi]
+      while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (start[mid] <= w) lo = mid; else hi = mid;
+      }
+      F(v, v.rp[lo].block_begin + (w - start[lo]));
+    }
+  } else {
+    F(v, blockIdx.x);
+  }
+}
+
+// rebuild 1: cell id and per-cell count.
+__device__ __forceinline__ void bin_block(const DeviceView& v, uint32_t b) {
+  const uint32_t r = v.block_replica[b];
+  if (!v.rs[r].need_rebuild) return;
+  const ReplicaParams& p = v.rp[r];
+  const uint32_t slot = b * kBlock + threadIdx.x;
+  const uint32_t local = slot - p.atom_begin;
+  if (local >= p.n_atoms) return;
+  const float4 x = v.pos[slot];
+  const uint32_t ix = axis_cell(x.x, p.lo[0], p.inv_cell[0], p.nc[0]);
+  const uint32_t iy = axis_cell(x.y, p.lo[1], p.inv_cell[1], p.nc[1]);
+  const uint32_t iz = axis_cell(x.z, p.lo[2], p.inv_cell[2], p.nc[2]);
+  const uint32_t cell = p.cell_begin + ix + p.nc[0] * (iy + p.nc[1] * iz);
+  v.cell_of_slot[slot] = cell;
+  atomicAdd(&v.cell_count[cell], 1u);
+}
+
+__global__ void __launch_bounds__(kBlock) k_bin(DeviceView v) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *v.chain_launches += 1ull;  // launches of the chain
+  for_chain_blocks<bin_block>(v);
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_sum(DeviceView v) {
@@ -365,8 +411,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_single(DeviceView v) {
 
 // rebuild 3: scatter slots into their cells (order inside a cell is fixed by
 // the next kernel).
-__global__ void __launch_bounds__(kBlock) k_scatter(DeviceView v) {
-  const uint32_t b = blockIdx.x;
+__device__ __forceinline__ void scatter_block(const DeviceView& v, uint32_t b) {
   const uint32_t r = v.block_replica[b];
   if (!v.rs[r].need_rebuild) return;
   const ReplicaParams& p = v.rp[r];
@@ -374,6 +419,10 @@ __global__ void __launch_bounds__(kBlock) k_scatter(DeviceView v) {
   if (slot - p.atom_begin >= p.n_atoms) return;
   const uint32_t at = atomicAdd(&v.cell_cursor[v.cell_of_slot[slot]], 1u);
   v.cell_atoms[at] = slot;
+}
+
+__global__ void __launch_bounds__(kBlock) k_scatter(DeviceView v) {
+  for_chain_blocks<scatter_block>(v);
 }
 
 // The replica of work item w (see k_scan); w is warp-uniform.
@@ -505,8 +554,7 @@ __global__ void __launch_bounds__(kBlock) k_cellsort(DeviceView v) {
 }
 
 // rebuild 5/6: physical reorder into cell order (every sort_every builds).
-__global__ void __launch_bounds__(kBlock) k_reorder_gather(DeviceView v) {
-  const uint32_t b = blockIdx.x;
+__device__ __forceinline__ void reorder_gather_block(const DeviceView& v, uint32_t b) {
   const uint32_t r = v.block_replica[b];
   const ReplicaState& st = v.rs[r];
   if (!st.need_rebuild || !st.reorder_now) return;
@@ -521,8 +569,11 @@ __global__ void __launch_bounds__(kBlock) k_reorder_gather(DeviceView v) {
   v.cell2[k] = v.cell_of_slot[old];
 }
 
-__global__ void __launch_bounds__(kBlock) k_reorder_commit(DeviceView v) {
-  const uint32_t b = blockIdx.x;
+__global__ void __launch_bounds__(kBlock) k_reorder_gather(DeviceView v) {
+  for_chain_blocks<reorder_gather_block>(v);
+}
+
+__device__ __forceinline__ void reorder_commit_block(const DeviceView& v, uint32_t b) {
   const uint32_t r = v.block_replica[b];
   const ReplicaState& st = v.rs[r];
   if (!st.need_rebuild || !st.reorder_now) return;
@@ -538,6 +589,10 @@ __global__ void __launch_bounds__(kBlock) k_reorder_commit(DeviceView v) {
   v.cell_of_slot[k] = v.cell2[k];
   v.cell_atoms[k] = k;
   v.slot_of_tag[t] = k;
+}
+
+__global__ void __launch_bounds__(kBlock) k_reorder_commit(DeviceView v) {
+  for_chain_blocks<reorder_commit_block>(v);
 }
 
 // Exclusion partners of every slot, projected from tag space to slot space
@@ -2134,7 +2189,14 @@ void launch_rebuild(const StepLaunch& l, bool force_all, bool count_build) {
         l.v, count_build ? 1 : 0);
     check_launch("force_rebuild_flags");
   }
-  k_bin<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  // With the block list, the per-slot kernels of the chain walk the
+  // rebuilding replicas' blocks with a grid of chain_grid blocks.
+  const uint32_t sg = l.v.chain_block_list ? l.chain_grid : l.v.n_blocks;
+  if (l.v.chain_block_list) {
+    k_chain_blocks<<<1, kScanThreads, 0, l.stream>>>(l.v);
+    check_launch("chain blocks");
+  }
+  k_bin<<<sg, kBlock, 0, l.stream>>>(l.v);
   check_launch("bin");
   if (l.v.n_scan_chunks == l.v.n_replicas) {  // every replica fits one chunk
     k_scan_single<<<l.v.n_replicas, kScanThreads, 0, l.stream>>>(l.v);
@@ -2147,7 +2209,7 @@ void launch_rebuild(const StepLaunch& l, bool force_all, bool count_build) {
     k_scan_cells<<<l.v.n_scan_chunks, kScanThreads, 0, l.stream>>>(l.v);
     check_launch("scan cells");
   }
-  k_scatter<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  k_scatter<<<sg, kBlock, 0, l.stream>>>(l.v);
   check_launch("scatter");
   if (l.any_sparse) {
     k_cellsort_sparse<<<(l.v.total_cells + kBlock - 1) / kBlock, kBlock, 0, l.stream>>>(l.v);
@@ -2155,9 +2217,9 @@ void launch_rebuild(const StepLaunch& l, bool force_all, bool count_build) {
   }
   k_cellsort<<<(l.v.total_cells + kBlock / 32 - 1) / (kBlock / 32), kBlock, 0, l.stream>>>(l.v);
   check_launch("cellsort");
-  k_reorder_gather<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  k_reorder_gather<<<sg, kBlock, 0, l.stream>>>(l.v);
   check_launch("reorder_gather");
-  k_reorder_commit<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v);
+  k_reorder_commit<<<sg, kBlock, 0, l.stream>>>(l.v);
   check_launch("reorder_commit");
   if (l.excl_cap > 0) {
     k_project_exclusions<<<l.v.n_blocks, kBlock, 0, l.stream>>>(l.v, 0);

@@ -25,6 +25,7 @@ struct StepLaunch {
   int need_kinetic;       // a thermostat is active in some replica
   int any_dense;          // some replica builds its lists a warp per cell (k_build)
   int any_sparse;         // some replica builds them a thread per particle
+  uint32_t chain_grid;    // blocks of the chain's per-slot kernels with the block list
   float sd_dmax;          // descent: displacement cap
   float sd_fref;          // descent: force floor
 };
