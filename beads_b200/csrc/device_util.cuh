@@ -107,6 +107,22 @@ __device__ __forceinline__ float acc_delta(float xi, float xj, float len,
   return d;
 }
 
+// acc_delta of two pairs on one axis in packed FP32x2 arithmetic: d = xi - xj
+// as already rounded, nxj = -xj.  Every lane rounds exactly as acc_delta
+// does (each packed operation rounds its halves as the scalar one would); a
+// lane whose pair is not `far` keeps d.
+__device__ __forceinline__ float2 acc_delta2(float2 d, float2 xi, float2 nxj, float len,
+                                             float half, bool far0, bool far1) {
+  const float2 bp = __fadd2_rn(d, make_float2(-xi.x, -xi.y));
+  const float2 ap = __fadd2_rn(d, make_float2(-bp.x, -bp.y));
+  const float2 err = __fadd2_rn(__fadd2_rn(xi, make_float2(-ap.x, -ap.y)),
+                                __fadd2_rn(nxj, make_float2(-bp.x, -bp.y)));
+  const float2 shift = make_float2(d.x > 0.0f ? -len : len, d.y > 0.0f ? -len : len);
+  const float2 img = __fadd2_rn(__fadd2_rn(d, shift), err);
+  return make_float2(far0 && fabsf(d.x) > half ? img.x : d.x,
+                     far1 && fabsf(d.y) > half ? img.y : d.y);
+}
+
 // Net periodic-boundary crossings of a slot since its last list build
 // (img - ref_img), three signed 10-bit fields in one word, so the
 // displacement check reads 4 bytes per slot instead of both image vectors.

@@ -1526,18 +1526,17 @@ __device__ __forceinline__ void lj_pairs(const DeviceView& v, const ReplicaParam
       const bool far0 = r2.x >= half_min_sq && r2.x < kFarR2;
       const bool far1 = r2.y >= half_min_sq && r2.y < kFarR2;
       if (kFar && __any_sync(kFull, far0 || far1)) {
-        if (far0) {
-          dx.x = acc_delta(xi.x, xj[u0].x, p.len[0], p.half[0]);
-          dy.x = acc_delta(xi.y, xj[u0].y, p.len[1], p.half[1]);
-          dz.x = acc_delta(xi.z, xj[u0].z, p.len[2], p.half[2]);
-          r2.x = norm2(dx.x, dy.x, dz.x);
-        }
-        if (far1) {
-          dx.y = acc_delta(xi.x, xj[u1].x, p.len[0], p.half[0]);
-          dy.y = acc_delta(xi.y, xj[u1].y, p.len[1], p.half[1]);
-          dz.y = acc_delta(xi.z, xj[u1].z, p.len[2], p.half[2]);
-          r2.y = norm2(dx.y, dy.y, dz.y);
-        }
+        // Both pairs at once through the packed pipe, each lane rounded
+        // exactly as acc_delta / norm2 round it; pairs that are not far keep
+        // their plain differences.
+        dx = acc_delta2(dx, xi2x, make_float2(-xj[u0].x, -xj[u1].x), p.len[0], p.half[0],
+                        far0, far1);
+        dy = acc_delta2(dy, xi2y, make_float2(-xj[u0].y, -xj[u1].y), p.len[1], p.half[1],
+                        far0, far1);
+        dz = acc_delta2(dz, xi2z, make_float2(-xj[u0].z, -xj[u1].z), p.len[2], p.half[2],
+                        far0, far1);
+        const float2 r2f = __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
+        r2 = make_float2(far0 ? r2f.x : r2.x, far1 ? r2f.y : r2.y);
       }
       // Entries past the particle's count are the far particle: r^2 > rc^2.
       const bool in0 = r2.x < rc2;
